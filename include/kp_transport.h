@@ -1,0 +1,174 @@
+/* kratos_polrad_b200 — C ABI of the B200 photon-packet transport path.
+ *
+ * Plain C: pointers, sizes and POD structs; no C++ or torch types.  Every
+ * entry point returns an int status (KP_OK = 0); kp_last_error() gives the
+ * calling thread's last message.  "device pointer" arguments are CUDA
+ * global-memory addresses on the current device; "host pointer" arguments
+ * are ordinary (pageable or pinned) host memory.  Streams and events are
+ * passed as opaque `void *` holding a cudaStream_t / cudaEvent_t (NULL is
+ * the legacy default stream).
+ *
+ * Each declaration names the reference interface it replaces
+ * (paths relative to the reference project's tree).
+ */
+#ifndef KP_TRANSPORT_H
+#define KP_TRANSPORT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KP_ABI_VERSION 1
+
+enum kp_status
+{
+    KP_OK           = 0,
+    KP_ERR_ARG      = 1,   /* invalid argument                         */
+    KP_ERR_CUDA     = 2,   /* CUDA runtime error                        */
+    KP_ERR_CONFIG   = 3,   /* bad mesh / transport configuration        */
+    KP_ERR_CAPACITY = 4,   /* a size exceeds a documented maximum       */
+    KP_ERR_DEVICE   = 5,   /* a kernel reported an error status word    */
+    KP_ERR_ALLOC    = 6    /* allocation refused                        */
+};
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char * kp_last_error( void );
+int          kp_abi_version( void );
+
+/* ------------------------------------------------------------------ */
+/* Device layer.  Replaces device::base_t's function objects and       */
+/* virtuals (src/device/device.h:37-50,66-186) and their CUDA backend   */
+/* (src/device/cuda/cuda.cpp:31-130,164-176).                           */
+
+int kp_device_init( int idx_device );            /* cuda_t::init, cuda.cpp:108-130          */
+int kp_device_count( int * n );
+int kp_malloc( void ** p, size_t bytes );        /* f_malloc, device.h:37-50                */
+int kp_malloc_host( void ** p, size_t bytes );   /* f_malloc_host (pinned), cuda.cpp:39-44  */
+int kp_free( void * p );                         /* f_free                                  */
+int kp_free_host( void * p );                    /* f_free_host                             */
+int kp_memset_async( void * p, int value, size_t bytes, void * stream );  /* f_mset      */
+int kp_memcpy( void * dst, const void * src, size_t bytes );              /* f_cp        */
+int kp_memcpy_async( void * dst, const void * src, size_t bytes,
+                     void * stream );                                     /* a_cp        */
+int kp_stream_create( void ** stream );          /* yield_stream, cuda.cpp:164-176          */
+int kp_stream_destroy( void * stream );
+int kp_stream_sync( void * stream );             /* sync_stream, device.cpp:124-151         */
+int kp_event_create( void ** event );            /* event_create                            */
+int kp_event_destroy( void * event );            /* event_destroy                           */
+int kp_event_record( void * event, void * stream );   /* event_record                       */
+int kp_event_wait( void * stream, void * event );     /* event_wait                         */
+int kp_event_sync( void * event );                    /* event_sync                         */
+int kp_event_elapsed( float * ms, void * start, void * stop );
+/* f_launch_host (device.cpp:101-119), without the reference's shared
+ * static callback vector: each call carries its own (fn, arg). */
+int kp_launch_host( void * stream, void ( * fn )( void * ), void * arg );
+
+/* ------------------------------------------------------------------ */
+/* Mesh.  Replaces meshgen::base_t (mesh/meshgen/meshgen.cpp:13-163,    */
+/* 286-432), tree_t (mesh/tree/tree.cpp:177-230) and the proxy table    */
+/* of particle::block_map_t (modules/particle/types/block_map.h:53-103, */
+/* types/proxy.h:22-62).  Building a mesh needs no GPU; the tables are  */
+/* copied to the current device on first use or by kp_mesh_upload.     */
+
+typedef struct kp_mesh kp_mesh_t;
+
+typedef struct kp_refine_box
+{
+    int    level;          /* [refine_region*] level                   */
+    double x_min[ 3 ];     /* [refine_region*] x_min (or loc)           */
+    double x_max[ 3 ];     /* [refine_region*] x_max                    */
+} kp_refine_box_t;
+
+typedef struct kp_mesh_desc
+{
+    double x_min[ 3 ];            /* [mesh] x_min                       */
+    double x_max[ 3 ];            /* [mesh] x_max                       */
+    int    n_cell_global[ 3 ];    /* [mesh] n_cell_global               */
+    int    n_cell_block[ 3 ];     /* [mesh] n_cell_block                */
+    int    periodic[ 3 ];         /* [boundary] kinds "per..." per axis */
+    int    n_refine;
+    const kp_refine_box_t * refine;
+} kp_mesh_desc_t;
+
+typedef struct kp_mesh_info
+{
+    int       n_blocks;
+    int       n_cell_block[ 3 ];
+    int       cells_per_block;
+    int       max_level;
+    long long n_cells;
+    int       periodic[ 3 ];
+    double    x_min[ 3 ];
+    double    x_max[ 3 ];
+} kp_mesh_info_t;
+
+int kp_mesh_create( const kp_mesh_desc_t * desc, kp_mesh_t ** mesh );
+/* Same, from an INI file with the reference's [mesh], [boundary] and
+ * [refine_region*] keys (io/args/input.cpp:72-108). */
+int kp_mesh_create_ini( const char * path, kp_mesh_t ** mesh );
+int kp_mesh_destroy( kp_mesh_t * mesh );
+int kp_mesh_info( const kp_mesh_t * mesh, kp_mesh_info_t * info );
+/* Region key (level, logical block index) per block id; host arrays of
+ * n_blocks and 3*n_blocks ints. */
+int kp_mesh_blocks( const kp_mesh_t * mesh, int * level, int * reg3 );
+/* Block geometry as the reference's geo_t holds it for float_t of
+ * `precision` bytes (4 or 8), widened to double: face origin xf0[3],
+ * spacing dx0[3], cell volume vol0, physical-boundary flags [6]. */
+int kp_mesh_geometry( const kp_mesh_t * mesh, int precision, double * xf0,
+                      double * dx0, double * vol0, int * phybnd );
+/* Face-neighbour table per block, slot (((a*2+side)*2+j0)*2+j1):
+ * ids [24], shift bits [48] (two per slot) and level deltas [6], with
+ * proxy_base_t's layout (types/proxy.h:13-19). */
+int kp_mesh_neighbors( const kp_mesh_t * mesh, int * nb_id, int * nb_shift,
+                       int * d_lvl );
+/* Host point location: block id and cell index of each of n points
+ * (x: host, 3n doubles).  Points outside the domain get ib = -1. */
+int kp_mesh_locate( const kp_mesh_t * mesh, long long n, const double * x,
+                    int * ib, int * cell3 );
+/* Copies the tables to the current device (idempotent). */
+int kp_mesh_upload( kp_mesh_t * mesh );
+/* Per-cell coefficients (sigma_sca, sigma_abs) as 2*n_cells floats in
+ * block-id order, x-fastest within a block.  `src` is a host pointer, or a
+ * device pointer when on_device != 0.  Replaces the per-block rad_t
+ * inverse-mean-free-path field (modules/particle/radiation/rad_data.cpp:
+ * 13-25). */
+int kp_mesh_set_sigma( kp_mesh_t * mesh, const float * src, long long n_values,
+                       int on_device, void * stream );
+/* Device pointer of the mesh's coefficient array (2*n_cells floats). */
+int kp_mesh_sigma_ptr( kp_mesh_t * mesh, float ** sigma );
+/* Synchronizes `stream`, returns and clears the mesh's device error status
+ * bits (out-of-range block or cell index, queue overflow, bad source); a
+ * kernel that sets one skips the offending access instead of faulting.
+ * Replaces the reference's debug flag (src/device/device.cpp:12-22,124-151). */
+int kp_mesh_status( kp_mesh_t * mesh, void * stream, unsigned * flags );
+
+/* ------------------------------------------------------------------ */
+/* Geometric walk with the path-length flux estimator.  Replaces        */
+/* integrate::base_t::intg / ker_itg (modules/particle/evolve/          */
+/* integrator.h:11-17,47-63,80-106) running photon::cart_t::proc        */
+/* (modules/particle/radiation/photon.h:20-125) over the packet pool,   */
+/* with the same per-step arithmetic.  Packet state is structure-of-    */
+/* arrays in device memory and is updated in place, as the pool is:   */
+/*   x[3n], dir[3n]  float_t (float if precision == 4, double if 8)     */
+/*   cell[3n], ib[n], step[n]  int;  todo[n]  int8 (to_keep -2,         */
+/*   to_rm -3, as particle::todo_t, types/particle_base.h:12)           */
+/*   proper[n] float_t                                                  */
+/* flux_mode 0: `flux` is float_t[n_cells] summed with float atomics,   */
+/* as the reference does (photon.h:81); 1: `flux` is int64[n_cells]     */
+/* holding round(deposit * 2^fx_shift), order independent.              */
+
+enum kp_flux_mode { KP_FLUX_FLOAT = 0, KP_FLUX_FIXED = 1 };
+
+int kp_trace( kp_mesh_t * mesh, int precision, long long n,
+              void * x, const void * dir, int * cell, int * ib,
+              const void * proper, int * step, int8_t * todo,
+              int flux_mode, int fx_shift, void * flux, void * stream );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KP_TRANSPORT_H */

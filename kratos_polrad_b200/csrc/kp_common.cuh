@@ -1,0 +1,129 @@
+// Internal types shared by the C-ABI translation units.
+#pragma once
+
+#include "../../include/kp_transport.h"
+#include "host/block_tree.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+namespace kp
+{
+
+////////////////////////////////////////////////////////////
+// Error handling: every entry point converts exceptions to a status and
+// records the message for kp_last_error() (replaces cuda_api's throw,
+// device/cuda/cuda.cpp:16-26, with a C-friendly status).
+
+struct error_t : std::runtime_error
+{
+    int code;
+    error_t( int c, const std::string & m ) : std::runtime_error( m ), code( c ) {}
+};
+
+void set_last_error( const std::string & msg );
+void clear_last_error(  );
+
+inline void cuda_check( cudaError_t e, const char * what )
+{
+    if( e != cudaSuccess )
+        throw error_t( KP_ERR_CUDA, std::string( what ) + ": "
+                                    + cudaGetErrorString( e ) );
+}
+#define KP_CUDA( call ) ::kp::cuda_check( ( call ), #call )
+
+template< class F >
+int guarded( const char * fn, F && f )
+{
+    try
+    {
+        clear_last_error(  );
+        f(  );
+        return KP_OK;
+    }
+    catch( const error_t & e )
+    {
+        set_last_error( std::string( fn ) + ": " + e.what(  ) );
+        return e.code;
+    }
+    catch( const std::bad_alloc & )
+    {
+        set_last_error( std::string( fn ) + ": host allocation failed" );
+        return KP_ERR_ALLOC;
+    }
+    catch( const std::exception & e )
+    {
+        set_last_error( std::string( fn ) + ": " + e.what(  ) );
+        return KP_ERR_CONFIG;
+    }
+}
+
+inline void require( bool ok, const char * msg, int code = KP_ERR_ARG )
+{
+    if( ! ok ) throw error_t( code, msg );
+}
+
+////////////////////////////////////////////////////////////
+// Device error status word bits (set by kernels, read by kp_mesh_status).
+
+enum status_bits : unsigned
+{
+    ST_BAD_BLOCK   = 1u << 0,   // packet block id out of range
+    ST_BAD_CELL    = 1u << 1,   // cell index out of range at a deposit
+    ST_QUEUE_FULL  = 1u << 2,   // a device queue overflowed
+    ST_BAD_SOURCE  = 1u << 3,   // a source lies outside the mesh
+};
+
+////////////////////////////////////////////////////////////
+// Device view of a mesh: passed by value to kernels.
+
+struct alignas( 16 ) blk_meta_t
+{
+    int8_t  d_lvl[ 6 ];       // level delta per face (2a+side)
+    uint8_t shift[ 6 ];       // shift bits of slot [a][side][0][0]
+    uint8_t phybnd;           // bit (2a+side): physical boundary
+    uint8_t pad[ 3 ];
+};
+static_assert( sizeof( blk_meta_t ) == 16, "meta record" );
+
+struct mesh_view_t
+{
+    int n_blocks;
+    int nc[ 3 ];
+    int cpb;                              // cells per block
+    const int        * __restrict__ nb;   // [n_blocks][24]
+    const blk_meta_t * __restrict__ meta; // [n_blocks]
+    const double     * __restrict__ geo_d;// [n_blocks][8]: xf0[3] dx0[3] vol0 -
+    const float      * __restrict__ geo_f;// [n_blocks][8]
+    const float2     * __restrict__ sigma;// [n_blocks * cpb] (sca, abs)
+    unsigned periodic;                    // bit a
+    double xlim_d[ 2 ][ 3 ];
+    double lbox_d[ 3 ];
+    float  xlim_f[ 2 ][ 3 ];
+    float  lbox_f[ 3 ];
+    unsigned * status;
+};
+
+}   // namespace kp
+
+// The opaque mesh handle of the C ABI.
+struct kp_mesh
+{
+    std::unique_ptr< kp::block_tree_t > tree;
+    int          device   = -1;
+    bool         uploaded = false;
+    int        * d_nb     = nullptr;
+    kp::blk_meta_t * d_meta = nullptr;
+    double     * d_geo_d  = nullptr;
+    float      * d_geo_f  = nullptr;
+    float2     * d_sigma  = nullptr;
+    unsigned   * d_status = nullptr;
+
+    kp::mesh_view_t view(  ) const;
+    void upload(  );
+    void release(  );
+};

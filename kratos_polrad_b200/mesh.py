@@ -1,0 +1,143 @@
+"""Block-structured AMR mesh handle (host mirror of the reference's mesh set-up).
+
+Mirrors what the reference's ``mesh_t::init`` + ``meshgen::base_t`` +
+``particle::block_map_t::update`` produce for the transport path
+(mesh/meshgen/meshgen.cpp:44-106, modules/particle/types/block_map.h:53-103):
+a static 2:1-balanced block tree, per-block geometry and the face-neighbour
+table, built by the C++ host code behind ``kp_mesh_create``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, ptr
+
+
+@dataclass
+class RefineRegion:
+    """One ``[refine_region*]`` section (meshgen.cpp:111-142)."""
+    level: int
+    x_min: tuple
+    x_max: tuple
+
+
+@dataclass
+class MeshConfig:
+    """The ``[mesh]`` / ``[boundary]`` / ``[refine_region*]`` keys."""
+    x_min: tuple
+    x_max: tuple
+    n_cell_global: tuple
+    n_cell_block: tuple = (16, 16, 16)
+    periodic: tuple = (False, False, False)
+    refine: list = field(default_factory=list)
+
+    def to_ini(self) -> str:
+        """INI text with the reference's section and key names."""
+        f = lambda v: " ".join(repr(float(t)) for t in v)
+        kinds = []
+        for a in range(3):
+            kinds += ["periodic", "periodic"] if self.periodic[a] else ["outflow", "outflow"]
+        lines = ["[mesh]", f"x_min = {f(self.x_min)}", f"x_max = {f(self.x_max)}",
+                 "n_cell_global = " + " ".join(str(int(v)) for v in self.n_cell_global),
+                 "n_cell_block = " + " ".join(str(int(v)) for v in self.n_cell_block),
+                 "", "[boundary]", "kinds = " + " ".join(kinds)]
+        for k, r in enumerate(self.refine):
+            lines += ["", f"[refine_region_{k:05d}]", f"level = {int(r.level)}",
+                      f"x_min = {f(r.x_min)}", f"x_max = {f(r.x_max)}"]
+        return "\n".join(lines) + "\n"
+
+
+class Mesh:
+    """Owns a ``kp_mesh_t``; building needs no GPU."""
+
+    def __init__(self, cfg: MeshConfig | None = None, ini_path: str | None = None):
+        h = ctypes.c_void_p()
+        if ini_path is not None:
+            call("kp_mesh_create_ini", ini_path.encode(), ctypes.byref(h))
+        else:
+            d = _lib.MeshDesc()
+            for a in range(3):
+                d.x_min[a], d.x_max[a] = cfg.x_min[a], cfg.x_max[a]
+                d.n_cell_global[a] = int(cfg.n_cell_global[a])
+                d.n_cell_block[a] = int(cfg.n_cell_block[a])
+                d.periodic[a] = int(bool(cfg.periodic[a]))
+            boxes = (_lib.RefineBox * max(1, len(cfg.refine)))()
+            for k, r in enumerate(cfg.refine):
+                boxes[k].level = int(r.level)
+                for a in range(3):
+                    boxes[k].x_min[a], boxes[k].x_max[a] = r.x_min[a], r.x_max[a]
+            d.n_refine = len(cfg.refine)
+            d.refine = ctypes.cast(boxes, ctypes.POINTER(_lib.RefineBox))
+            call("kp_mesh_create", ctypes.byref(d), ctypes.byref(h))
+        self.handle = h
+        info = _lib.MeshInfo()
+        call("kp_mesh_info", h, ctypes.byref(info))
+        self.n_blocks = info.n_blocks
+        self.nc = tuple(info.n_cell_block)
+        self.cells_per_block = info.cells_per_block
+        self.n_cells = info.n_cells
+        self.max_level = info.max_level
+        self.periodic = tuple(bool(v) for v in info.periodic)
+        self.x_min = tuple(info.x_min)
+        self.x_max = tuple(info.x_max)
+
+    def close(self):
+        if self.handle:
+            call("kp_mesh_destroy", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- tables (host) ----
+    def blocks(self):
+        lev = np.zeros(self.n_blocks, np.int32)
+        reg = np.zeros((self.n_blocks, 3), np.int32)
+        call("kp_mesh_blocks", self.handle, ptr(lev), ptr(reg))
+        return lev, reg
+
+    def geometry(self, precision: int = 8):
+        nb = self.n_blocks
+        xf0, dx0 = np.zeros((nb, 3)), np.zeros((nb, 3))
+        vol0, pb = np.zeros(nb), np.zeros((nb, 6), np.int32)
+        call("kp_mesh_geometry", self.handle, precision, ptr(xf0), ptr(dx0), ptr(vol0), ptr(pb))
+        return xf0, dx0, vol0, pb
+
+    def neighbors(self):
+        nb = self.n_blocks
+        ids = np.zeros((nb, 24), np.int32)
+        sh = np.zeros((nb, 48), np.int32)
+        dl = np.zeros((nb, 6), np.int32)
+        call("kp_mesh_neighbors", self.handle, ptr(ids), ptr(sh), ptr(dl))
+        return ids, sh, dl
+
+    def locate(self, x):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        ib = np.zeros(len(x), np.int32)
+        cell = np.zeros((len(x), 3), np.int32)
+        call("kp_mesh_locate", self.handle, len(x), ptr(x), ptr(ib), ptr(cell))
+        return ib, cell
+
+    # ---- device ----
+    def upload(self):
+        call("kp_mesh_upload", self.handle)
+
+    def set_sigma(self, sigma2):
+        """Per-cell (sigma_sca, sigma_abs), shape (n_cells, 2), host or torch CUDA."""
+        on_dev = int(hasattr(sigma2, "is_cuda") and sigma2.is_cuda)
+        if not on_dev:
+            sigma2 = np.ascontiguousarray(sigma2, np.float32)
+        n = int(np.prod(sigma2.shape))
+        call("kp_mesh_set_sigma", self.handle, ptr(sigma2), n, on_dev, None)
+
+    def status(self, stream=None) -> int:
+        flags = ctypes.c_uint()
+        call("kp_mesh_status", self.handle, stream, ctypes.byref(flags))
+        return flags.value
