@@ -1,0 +1,53 @@
+/* Oracle: plain-C restatement of the transport path (test infrastructure).
+ *
+ * Only the tests, the smoke check and the bench's CPU-baseline leg use this
+ * library (oracle/_ref/libkporacle.so); the product never links it.
+ *
+ * Geometric walk: restates photon::cart_t::proc and what it calls
+ * (reference files modules/particle/radiation/photon.h:20-125,
+ * types/particle_base.h:37-56,86-126, types/proxy.h:64-121,
+ * mesh/geometry/geometry.h:206-256) over flat block tables, in float
+ * (PRECISION=1) or double (PRECISION=2) arithmetic with the reference's
+ * operation order.  Pinned bit-for-bit against the reference's own code
+ * compiled on the host (oracle/ref_harness.cpp).
+ */
+#ifndef KP_ORACLE_H
+#define KP_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Flat mesh tables, block-id order (see kp_mesh_geometry/_neighbors). */
+typedef struct kpo_mesh
+{
+    int            n_blocks;
+    int            nc[ 3 ];
+    const double * xf0;       /* [nb][3] (float_t values widened)   */
+    const double * dx0;       /* [nb][3]                             */
+    const double * vol0;      /* [nb]                                */
+    const int    * phybnd;    /* [nb][6]                             */
+    const int    * nb_id;     /* [nb][24] slot ((a*2+s)*2+j0)*2+j1   */
+    const int    * nb_shift;  /* [nb][48]                            */
+    const int    * d_lvl;     /* [nb][6]                             */
+    int            periodic[ 3 ];
+    double         xlim[ 2 ][ 3 ];
+    double         lbox[ 3 ];
+} kpo_mesh_t;
+
+/* Walks n packets in place (x, dir: 3n; cell: 3n; ib, step, todo: n).
+ * precision 4: float_t = float, 8: double.  Deposits go to flux_f (float_t
+ * sums in packet order, widened) and flux_fx (int64 round(v*2^fx_shift)),
+ * both [n_blocks * cells_per_block]. */
+int kpo_trace( const kpo_mesh_t * m, int precision, long n, double * x,
+               const double * dir, int * cell, int * ib, const double * proper,
+               int * step, int * todo, int fx_shift, double * flux_f,
+               long long * flux_fx );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

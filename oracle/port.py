@@ -1,0 +1,110 @@
+"""ctypes driver of the C restatement (oracle/_ref/libkporacle.so).
+
+Test infrastructure only.  The walk consumes flat block tables, either the
+reference harness's (refharness.RefMesh) or the product's (kp_mesh_*).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "_ref", "libkporacle.so")
+
+
+class _Mesh(ctypes.Structure):
+    _fields_ = [("n_blocks", ctypes.c_int), ("nc", ctypes.c_int * 3),
+                ("xf0", ctypes.c_void_p), ("dx0", ctypes.c_void_p), ("vol0", ctypes.c_void_p),
+                ("phybnd", ctypes.c_void_p), ("nb_id", ctypes.c_void_p),
+                ("nb_shift", ctypes.c_void_p), ("d_lvl", ctypes.c_void_p),
+                ("periodic", ctypes.c_int * 3), ("xlim", ctypes.c_double * 6),
+                ("lbox", ctypes.c_double * 3)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise FileNotFoundError(f"{LIB} missing: run `make -C oracle`")
+        _lib = ctypes.CDLL(LIB)
+    return _lib
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+class Tables:
+    """Flat tables (block-id order) of a mesh for one float_t precision."""
+
+    def __init__(self, nc, xf0, dx0, vol0, phybnd, nb_id, nb_shift, d_lvl, periodic, xlim, lbox):
+        c = lambda a, t: np.ascontiguousarray(a, t)
+        self.nc = tuple(int(v) for v in nc)
+        self.xf0, self.dx0, self.vol0 = c(xf0, np.float64), c(dx0, np.float64), c(vol0, np.float64)
+        self.phybnd, self.nb_id = c(phybnd, np.int32), c(nb_id, np.int32)
+        self.nb_shift, self.d_lvl = c(nb_shift, np.int32), c(d_lvl, np.int32)
+        self.periodic = [int(v) for v in periodic]
+        self.xlim = np.asarray(xlim, np.float64).reshape(2, 3)
+        self.lbox = np.asarray(lbox, np.float64)
+        self.n_blocks = len(self.vol0)
+        self.cells_per_block = int(np.prod(self.nc))
+
+    @classmethod
+    def from_ref(cls, ref):
+        xf0, dx0, vol0, pb = ref.geometry()
+        ids, sh, dl = ref.neighbors()
+        xlim, lbox, per = ref.box()
+        return cls(ref.nc, xf0, dx0, vol0, pb, ids, sh, dl, per, xlim, lbox)
+
+    @classmethod
+    def from_mesh(cls, mesh, precision):
+        xf0, dx0, vol0, pb = mesh.geometry(precision)
+        ids, sh, dl = mesh.neighbors()
+        xlim = np.array([mesh.x_min, mesh.x_max])
+        lbox = xlim[1] - xlim[0]
+        if precision == 4:
+            xlim = xlim.astype(np.float32).astype(np.float64)
+            lbox = lbox.astype(np.float32).astype(np.float64)
+        return cls(mesh.nc, xf0, dx0, vol0, pb, ids, sh, dl, mesh.periodic, xlim, lbox)
+
+    def _struct(self):
+        s = _Mesh()
+        s.n_blocks = self.n_blocks
+        for a in range(3):
+            s.nc[a] = self.nc[a]
+            s.periodic[a] = self.periodic[a]
+            s.lbox[a] = self.lbox[a]
+        for k, v in enumerate(self.xlim.reshape(-1)):
+            s.xlim[k] = v
+        for f in ("xf0", "dx0", "vol0", "phybnd", "nb_id", "nb_shift", "d_lvl"):
+            setattr(s, f, getattr(self, f).ctypes.data)
+        return s
+
+
+def trace(tab: Tables, precision: int, x, dir, cell, ib, proper, steps, fx_shift=32, todo=None):
+    """Restated cart_t::proc walk; returns final state and both flux sums."""
+    n = len(ib)
+    x = np.array(x, np.float64).reshape(n, 3)
+    dir = np.ascontiguousarray(dir, np.float64).reshape(n, 3)
+    cell = np.array(cell, np.int32).reshape(n, 3)
+    ib = np.array(ib, np.int32)
+    proper = np.ascontiguousarray(proper, np.float64)
+    steps = np.array(steps, np.int32)
+    todo = np.full(n, -2, np.int32) if todo is None else np.array(todo, np.int32)
+    ncell = tab.n_blocks * tab.cells_per_block
+    flux_f, flux_fx = np.zeros(ncell), np.zeros(ncell, np.int64)
+    s = tab._struct()
+    L = lib()
+    L.kpo_trace.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_long] + [ctypes.c_void_p] * 7 + \
+        [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    p = lambda a: a.ctypes.data
+    st = L.kpo_trace(ctypes.byref(s), precision, n, p(x), p(dir), p(cell), p(ib), p(proper),
+                     p(steps), p(todo), fx_shift, p(flux_f), p(flux_fx))
+    if st != 0:
+        raise RuntimeError("kpo_trace: bad block id")
+    return dict(x=x, cell=cell, ib=ib, step=steps, todo=todo, flux=flux_f, flux_fx=flux_fx)
