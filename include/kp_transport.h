@@ -167,6 +167,113 @@ int kp_trace( kp_mesh_t * mesh, int precision, long long n,
               const void * proper, int * step, int8_t * todo,
               int flux_mode, int fx_shift, void * flux, void * stream );
 
+/* ------------------------------------------------------------------ */
+/* Polarized Monte-Carlo transport.  Replaces one cycle of the particle */
+/* module (particle::base_t::integrate, modules/particle/driver.h:      */
+/* 59-79): the generator launch (evolve/generate_par.h:51-62, ker_gen)  */
+/* and the integrator launch running the packet walk (evolve/           */
+/* integrator.h:47-63; radiation/photon.h:104-125), extended with the   */
+/* physics the reference leaves to user hooks (photon.h:73-102,         */
+/* proc_phys/proc_step): optical-depth sampling, albedo weighting,      */
+/* Rayleigh or HG+polarization scattering of the Stokes vector,         */
+/* peel-off imaging and escape tallies.  Packets have counter-based     */
+/* Philox streams keyed by (seed, stream_id) and their global id, so a  */
+/* packet's history does not depend on the launch, the GPU count or the */
+/* thread that runs it.                                                 */
+
+#define KP_MAX_SOURCES 64
+#define KP_MAX_BATCHES 64
+
+enum kp_phase       { KP_PHASE_RAYLEIGH = 0, KP_PHASE_HG_POL = 1 };
+enum kp_source_kind { KP_SOURCE_POINT = 0, KP_SOURCE_PLANE_BASE = 1 };
+enum kp_emit        { KP_EMIT_ISOTROPIC = 0, KP_EMIT_UP_UNIFORM = 1 };
+enum kp_tally_mode  { KP_TALLY_FIXED = 0, KP_TALLY_FLOAT = 1 };
+enum kp_counter
+{
+    KP_CNT_STEPS = 0,       /* packet-steps of the walk (segments)        */
+    KP_CNT_PEEL_STEPS,      /* segments of peel-off rays                  */
+    KP_CNT_SCATTER,         /* interactions                               */
+    KP_CNT_ESCAPED,
+    KP_CNT_ABSORBED,        /* ended by Russian roulette                  */
+    KP_CNT_CAPPED,          /* ended by max_scatter or max_steps          */
+    KP_CNT_LOST,            /* no neighbour across an inner face          */
+    KP_CNT_EMITTED,
+    KP_NCOUNTERS
+};
+
+typedef struct kp_source
+{
+    int    kind;     /* KP_SOURCE_POINT at pos, or KP_SOURCE_PLANE_BASE:
+                        uniform over the domain's lower z face            */
+    int    emit;     /* KP_EMIT_ISOTROPIC, or KP_EMIT_UP_UNIFORM (mu = d.z
+                        uniform in (0,1))                                  */
+    double pos[ 3 ];
+} kp_source_t;
+
+typedef struct kp_transport_cfg
+{
+    long long n_packets;       /* packets of this call                         */
+    long long packet_offset;   /* global id of its first packet               */
+    uint32_t  seed;
+    uint32_t  stream_id;       /* second Philox key word (e.g. scene id)       */
+    int       phase;           /* enum kp_phase                                */
+    float     hg_g;            /* HG asymmetry (KP_PHASE_HG_POL)               */
+    float     pol_max;         /* peak linear polarization at 90 deg (HG)      */
+    int       n_sources;       /* 1..KP_MAX_SOURCES; packet p uses p % n       */
+    const kp_source_t * sources;   /* host pointer                             */
+    int       n_mu_bins;       /* escape tally bins in mu = d.z (0: off)       */
+    float     mu_lo, mu_hi;
+    int       image_n;         /* peel-off image side in pixels (0: off)       */
+    double    inclination_deg; /* observer direction from +z                   */
+    double    azimuth_deg;     /* ... and about +z from +x                     */
+    double    image_center[ 3 ];
+    double    image_half_width;
+    float     tau_peel_max;    /* peel-off rays stop beyond this depth (<=0: 40) */
+    int       tally_mode;      /* enum kp_tally_mode                           */
+    int       fx_shift;        /* fixed point: round(value * 2^fx_shift)       */
+    int       n_batches;       /* batch-means tallies: packet p -> p % n       */
+    float     w_min;           /* Russian roulette below this weight (0: off)  */
+    float     rr_survive;      /* roulette survival probability (<=0: 0.1)     */
+    int       max_scatter;     /* interactions per packet before it is ended   */
+    long long max_steps;       /* segments per packet before it is ended       */
+    long long n_record;        /* final-state records for the first n packets  */
+} kp_transport_cfg_t;
+
+typedef struct kp_packet_record
+{
+    double    x[ 3 ];
+    float     d[ 3 ];
+    float     stokes[ 3 ];     /* q, u, v relative to I (frame vector below)   */
+    float     w;
+    int       ib;
+    int       cell[ 3 ];
+    int       n_scatter;
+    int       status;          /* 1 escaped, 2 absorbed, 3/4 capped, 5 lost    */
+    uint32_t  rng_draws;       /* Philox blocks consumed                       */
+    long long n_steps;
+} kp_packet_record_t;
+
+/* Output buffers (device pointers), accumulated into: zero them before the
+ * first call.  Element type int64 (KP_TALLY_FIXED) or float (KP_TALLY_FLOAT).
+ *   mu          [n_batches][n_mu_bins][4]  escaping I,Q,U,V (meridian frame)
+ *   image       [image_n][image_n][4]      peel-off I,Q,U,V (Q>0 vertical)
+ *   image_batch [n_batches][4]             image sums per batch
+ *   counters    [KP_NCOUNTERS] uint64 (optional)
+ *   records     [n_record] (optional) */
+typedef struct kp_tallies
+{
+    void * mu;
+    void * image;
+    void * image_batch;
+    unsigned long long * counters;
+    kp_packet_record_t * records;
+} kp_tallies_t;
+
+/* Asynchronous on `stream`.  Calls that share a mesh handle must not
+ * overlap on the GPU (they share the mesh's packet counter). */
+int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                          const kp_tallies_t * tallies, void * stream );
+
 #ifdef __cplusplus
 }
 #endif

@@ -298,6 +298,24 @@ void block_tree_t::build_tables(  )
             }
         }
     }
+    const int L = t.max_level;
+    for( int a = 0; a < 3; ++ a )
+        t.lookup_n[ a ] = blocks_at( L, a );
+    t.lookup.assign( ( size_t ) t.lookup_n[ 0 ] * t.lookup_n[ 1 ] * t.lookup_n[ 2 ], -1 );
+    for( const auto & [ k, n ] : nodes_ )
+    {
+        if( n.refined )
+            continue;
+        const int f = 1 << ( L - k.level );
+        for( int dz = 0; dz < f; ++ dz )
+            for( int dy = 0; dy < f; ++ dy )
+                for( int dx = 0; dx < f; ++ dx )
+                {
+                    const size_t i = k.i[ 0 ] * f + dx, j = k.i[ 1 ] * f + dy,
+                                 l = k.i[ 2 ] * f + dz;
+                    t.lookup[ ( l * t.lookup_n[ 1 ] + j ) * t.lookup_n[ 0 ] + i ] = n.id;
+                }
+    }
     for( int a = 0; a < 3; ++ a )
     {
         t.periodic[ a ]  = desc_.periodic[ a ];

@@ -77,6 +77,11 @@ struct block_tables_t
     std::vector< int8_t >   d_lvl;         // [nb][6]
     std::vector< uint8_t >  nb_shift;      // [nb][24] bit0: shift[0], bit1: shift[1]
 
+    // Finest-level lookup grid: leaf block id of every finest-level block
+    // position, x fastest (device-side point location of plane sources).
+    int lookup_n[ 3 ] = { 0, 0, 0 };
+    std::vector< int >      lookup;
+
     double xlim_d[ 2 ][ 3 ];
     double l_box_d[ 3 ];
     float  xlim_f[ 2 ][ 3 ];

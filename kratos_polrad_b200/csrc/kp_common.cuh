@@ -6,7 +6,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -97,9 +99,13 @@ struct mesh_view_t
     int cpb;                              // cells per block
     const int        * __restrict__ nb;   // [n_blocks][24]
     const blk_meta_t * __restrict__ meta; // [n_blocks]
-    const double     * __restrict__ geo_d;// [n_blocks][8]: xf0[3] dx0[3] vol0 -
+    const double     * __restrict__ geo_d;// [n_blocks][16]: xf0[3] dx0[3] vol0 -
+                                          //   inv_dx[3] - ...
     const float      * __restrict__ geo_f;// [n_blocks][8]
     const float2     * __restrict__ sigma;// [n_blocks * cpb] (sca, abs)
+    const int        * __restrict__ lookup;// finest-level block grid
+    int lookup_n[ 3 ];
+    int max_level;
     unsigned periodic;                    // bit a
     double xlim_d[ 2 ][ 3 ];
     double lbox_d[ 3 ];
@@ -121,9 +127,13 @@ struct kp_mesh
     double     * d_geo_d  = nullptr;
     float      * d_geo_f  = nullptr;
     float2     * d_sigma  = nullptr;
+    int        * d_lookup = nullptr;
     unsigned   * d_status = nullptr;
 
+    unsigned long long * d_work = nullptr;   // scratch: packet counters
+
     kp::mesh_view_t view(  ) const;
+    unsigned long long * workspace(  ) { upload(  ); return d_work; }
     void upload(  );
     void release(  );
 };

@@ -20,6 +20,9 @@ kp::mesh_view_t kp_mesh::view(  ) const
     v.geo_d = d_geo_d;
     v.geo_f = d_geo_f;
     v.sigma = d_sigma;
+    v.lookup = d_lookup;
+    for( int a = 0; a < 3; ++ a ) v.lookup_n[ a ] = t.lookup_n[ a ];
+    v.max_level = t.max_level;
     v.periodic = 0;
     for( int a = 0; a < 3; ++ a )
     {
@@ -49,7 +52,7 @@ void kp_mesh::upload(  )
     const auto & t = tree->tables(  );
     const size_t nb = t.n_blocks;
     std::vector< kp::blk_meta_t > meta( nb );
-    std::vector< double > gd( nb * 8, 0. );
+    std::vector< double > gd( nb * 16, 0. );
     std::vector< float  > gf( nb * 8, 0.f );
     for( size_t b = 0; b < nb; ++ b )
     {
@@ -63,12 +66,13 @@ void kp_mesh::upload(  )
         m.phybnd = t.phybnd[ b ];
         for( int a = 0; a < 3; ++ a )
         {
-            gd[ 8 * b + a ]     = t.xf0_d[ 3 * b + a ];
-            gd[ 8 * b + 3 + a ] = t.dx0_d[ 3 * b + a ];
+            gd[ 16 * b + a ]     = t.xf0_d[ 3 * b + a ];
+            gd[ 16 * b + 3 + a ] = t.dx0_d[ 3 * b + a ];
+            gd[ 16 * b + 8 + a ] = 1.0 / t.dx0_d[ 3 * b + a ];
             gf[ 8 * b + a ]     = t.xf0_f[ 3 * b + a ];
             gf[ 8 * b + 3 + a ] = t.dx0_f[ 3 * b + a ];
         }
-        gd[ 8 * b + 6 ] = t.vol0_d[ b ];
+        gd[ 16 * b + 6 ] = t.vol0_d[ b ];
         gf[ 8 * b + 6 ] = t.vol0_f[ b ];
     }
     const size_t n_cells = nb * ( size_t ) t.cells_per_block;
@@ -76,10 +80,15 @@ void kp_mesh::upload(  )
     {
         KP_CUDA( cudaMalloc( & d_nb,     nb * 24 * sizeof( int ) ) );
         KP_CUDA( cudaMalloc( & d_meta,   nb * sizeof( kp::blk_meta_t ) ) );
-        KP_CUDA( cudaMalloc( & d_geo_d,  nb * 8 * sizeof( double ) ) );
+        KP_CUDA( cudaMalloc( & d_geo_d,  nb * 16 * sizeof( double ) ) );
+        KP_CUDA( cudaMalloc( & d_lookup, t.lookup.size(  ) * sizeof( int ) ) );
+        KP_CUDA( cudaMemcpy( d_lookup, t.lookup.data(  ), t.lookup.size(  ) * sizeof( int ),
+                             cudaMemcpyHostToDevice ) );
         KP_CUDA( cudaMalloc( & d_geo_f,  nb * 8 * sizeof( float ) ) );
         KP_CUDA( cudaMalloc( & d_sigma,  n_cells * sizeof( float2 ) ) );
         KP_CUDA( cudaMalloc( & d_status, 4 * sizeof( unsigned ) ) );
+        KP_CUDA( cudaMalloc( & d_work, 32 * sizeof( unsigned long long ) ) );
+        KP_CUDA( cudaMemset( d_work, 0, 32 * sizeof( unsigned long long ) ) );
         KP_CUDA( cudaMemcpy( d_nb, t.nb_id.data(  ), nb * 24 * sizeof( int ),
                              cudaMemcpyHostToDevice ) );
         KP_CUDA( cudaMemcpy( d_meta, meta.data(  ), nb * sizeof( kp::blk_meta_t ),
@@ -107,7 +116,9 @@ void kp_mesh::release(  )
     cudaFree( d_geo_d );  d_geo_d  = nullptr;
     cudaFree( d_geo_f );  d_geo_f  = nullptr;
     cudaFree( d_sigma );  d_sigma  = nullptr;
+    cudaFree( d_lookup ); d_lookup = nullptr;
     cudaFree( d_status ); d_status = nullptr;
+    cudaFree( d_work );   d_work   = nullptr;
     uploaded = false;
 }
 

@@ -37,6 +37,9 @@ template<> struct geo_ptr< float >
 template<> struct geo_ptr< double >
 { static __device__ const double * get( const mesh_view_t & m ) { return m.geo_d; } };
 
+template< class f_t > __device__ __forceinline__ int geo_stride(  );
+template<> __device__ __forceinline__ int geo_stride< float  >(  ) { return 8; }
+template<> __device__ __forceinline__ int geo_stride< double >(  ) { return 16; }
 template< class f_t > __device__ __forceinline__ f_t xlim( const mesh_view_t & m, int l, int a );
 template<> __device__ __forceinline__ float  xlim< float  >( const mesh_view_t & m, int l, int a ) { return m.xlim_f[ l ][ a ]; }
 template<> __device__ __forceinline__ double xlim< double >( const mesh_view_t & m, int l, int a ) { return m.xlim_d[ l ][ a ]; }
@@ -51,7 +54,7 @@ struct blk_geo_t
     f_t xf0[ 3 ], dx0[ 3 ], vol0;
     __device__ void load( const mesh_view_t & m, int b )
     {
-        const f_t * g = geo_ptr< f_t >::get( m ) + 8 * ( size_t ) b;
+        const f_t * g = geo_ptr< f_t >::get( m ) + geo_stride< f_t >(  ) * ( size_t ) b;
         #pragma unroll
         for( int a = 0; a < 3; ++ a ) { xf0[ a ] = g[ a ]; dx0[ a ] = g[ 3 + a ]; }
         vol0 = g[ 6 ];

@@ -1,0 +1,290 @@
+// Forward polarized transport: persistent kernel with packet regeneration.
+//
+// Replaces the reference's per-cycle generate + integrate launches
+// (modules/particle/evolve/generate_par.h:51-62 -> ker_gen, then
+// evolve/integrator.h:47-63 -> ker_itg running photon::cart_t::proc) by one
+// persistent launch: every thread walks one packet at a time, segment by
+// segment, and when its packet ends (escape, absorption) it takes the next
+// packet index from a global counter.  Lanes that need new packets in the
+// same iteration take them with one warp-aggregated atomic (the warp's
+// coalesced group ballots, its leader adds the group size), so the warp
+// stays full while packet lifetimes differ by orders of magnitude.
+#include "kp_transport.cuh"
+
+namespace kp
+{
+namespace
+{
+namespace cg = cooperative_groups;
+
+template< int TALLY >
+__global__ void __launch_bounds__( 256 )
+k_forward( const __grid_constant__ fwd_params_t P )
+{
+    local_counts_t cnt;
+    packet_t p;
+    bool alive = false;
+    for( ;; )
+    {
+        if( ! alive )
+        {
+            unsigned long long idx;
+            {
+                cg::coalesced_group g = cg::coalesced_threads(  );
+                unsigned long long base = 0;
+                if( g.thread_rank(  ) == 0 )
+                    base = atomicAdd( P.work, ( unsigned long long ) g.size(  ) );
+                base = g.shfl( base, 0 );
+                idx  = base + g.thread_rank(  );
+            }
+            if( idx >= ( unsigned long long ) P.n_packets )
+                break;
+            if( ! emit_packet( P, P.pid0 + ( long long ) idx, p ) )
+            {
+                atomicOr( P.m.status, ST_BAD_SOURCE );
+                continue;
+            }
+            ++ cnt.emit;
+            const src_dev_t & s = P.src[ p.pid % P.n_src ];
+            if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
+            {   // direct light of an isotropic, unpolarized point source
+                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel );
+                if( tau <= P.tau_cut )
+                {
+                    const float I = __fmul_rn( 0x1.45f306p-4f,   // 1 / (4 pi)
+                                               ( float ) phys::kp_exp_neg( -( double ) tau ) );
+                    deposit_image< TALLY >( P, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
+                }
+            }
+            p.tau = sample_tau( p.rng );
+            alive = true;
+            continue;
+        }
+
+        // One segment: to the exit face of the current cell or to the
+        // interaction point inside it.
+        const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
+        const float ext = __fadd_rn( sg.x, sg.y );
+        int ax;
+        const double t = exit_dist( P.m, p.b, p.c, p.x, p.d, p.inv, ax );
+        const float dtau = __fmul_rn( ext, ( float ) t );
+        ++ cnt.steps;
+        ++ p.n_steps;
+        int end = 0;
+        if( dtau >= p.tau )
+        {
+            double ti = ( double ) __fdiv_rn( p.tau, ext );
+            ti = ti > t ? t : ti;
+            p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
+            p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
+            p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
+            // interaction: survival weighting by the albedo
+            ++ p.n_scat;
+            ++ cnt.scat;
+            p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, ext ) );
+            if( P.img_n > 0 )
+            {
+                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel );
+                if( tau <= P.tau_cut )
+                {
+                    float Q, U, V;
+                    const float I = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh,
+                                                       Q, U, V );
+                    const float att = __fmul_rn( p.w, ( float ) phys::kp_exp_neg( -( double ) tau ) );
+                    deposit_image< TALLY >( P, p.x, p.pid, __fmul_rn( att, I ),
+                                            __fmul_rn( att, Q ), __fmul_rn( att, U ),
+                                            __fmul_rn( att, V ) );
+                }
+            }
+            if( p.n_scat >= P.max_scatter )
+                end = PK_SCATTER_CAP;
+            else if( p.w < P.w_min )
+            {   // Russian roulette
+                const phys::u4 r = p.rng.next(  );
+                if( phys::u01( r.x ) < P.rr_survive )
+                    p.w = __fdiv_rn( p.w, P.rr_survive );
+                else
+                    end = PK_ABSORBED;
+            }
+            if( ! end )
+            {
+                phys::scatter( P.ph, p.rng, p.d, p.e1, p.S );
+                set_inv( p );
+                p.tau = sample_tau( p.rng );
+            }
+        }
+        else
+        {
+            p.tau = __fsub_rn( p.tau, dtau );
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a )
+                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
+            bool lost;
+            if( ! cross_face( P.m, p.b, p.c, p.x, ax, comp( p.d, ax ) > 0.0f, lost ) )
+            {
+                if( lost )
+                    end = PK_LOST;
+                else
+                {
+                    end = PK_ESCAPED;
+                    tally_escape< TALLY >( P, p );
+                }
+            }
+        }
+        if( ! end && p.n_steps >= P.max_steps )
+            end = PK_STEP_CAP;
+        if( end )
+        {
+            write_record( P, p, end );
+            cnt.esc  += end == PK_ESCAPED;
+            cnt.absb += end == PK_ABSORBED;
+            cnt.cap  += end == PK_SCATTER_CAP || end == PK_STEP_CAP;
+            cnt.lost += end == PK_LOST;
+            alive = false;
+        }
+    }
+    if( P.counters )
+    {
+        atomicAdd( P.counters + KP_CNT_STEPS,      cnt.steps );
+        atomicAdd( P.counters + KP_CNT_PEEL_STEPS, cnt.peel );
+        atomicAdd( P.counters + KP_CNT_SCATTER,    cnt.scat );
+        atomicAdd( P.counters + KP_CNT_ESCAPED,    cnt.esc );
+        atomicAdd( P.counters + KP_CNT_ABSORBED,   cnt.absb );
+        atomicAdd( P.counters + KP_CNT_CAPPED,     cnt.cap );
+        atomicAdd( P.counters + KP_CNT_LOST,       cnt.lost );
+        atomicAdd( P.counters + KP_CNT_EMITTED,    cnt.emit );
+    }
+}
+
+}   // namespace
+
+////////////////////////////////////////////////////////////
+// Host side
+
+// Fills the launch parameters from the C configuration (host work only).
+void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
+                      const kp_tallies_t & t, fwd_params_t & P )
+{
+    require( c.n_packets >= 0 && c.packet_offset >= 0, "negative packet count" );
+    require( c.n_sources >= 1 && c.n_sources <= MAX_SOURCES && c.sources,
+             "need 1..KP_MAX_SOURCES sources", KP_ERR_CAPACITY );
+    require( c.phase == KP_PHASE_RAYLEIGH || c.phase == KP_PHASE_HG_POL, "unknown phase" );
+    require( c.tally_mode == KP_TALLY_FIXED || c.tally_mode == KP_TALLY_FLOAT, "unknown tally mode" );
+    require( c.fx_shift >= 0 && c.fx_shift <= 48, "fx_shift out of range" );
+    require( c.n_batches >= 1 && c.n_batches <= KP_MAX_BATCHES, "n_batches out of range",
+             KP_ERR_CAPACITY );
+    require( c.n_mu_bins >= 0 && ( c.n_mu_bins == 0 || ( t.mu && c.mu_hi > c.mu_lo ) ),
+             "bad mu tally" );
+    require( c.image_n >= 0 && ( c.image_n == 0 || ( t.image && t.image_batch &&
+                                                     c.image_half_width > 0 ) ),
+             "bad image" );
+    require( c.n_record >= 0 && ( c.n_record == 0 || t.records ), "bad records" );
+    require( c.max_scatter >= 1 && c.max_steps >= 1, "caps must be positive" );
+    const auto & tab = mesh->tree->tables(  );
+    std::memset( & P, 0, sizeof( P ) );
+    P.m = mesh->view(  );
+    P.n_packets = c.n_packets;
+    P.pid0 = c.packet_offset;
+    P.seed = c.seed;
+    P.stream = c.stream_id;
+    P.ph = phys::phase_t { c.phase, c.hg_g, c.pol_max };
+    P.n_src = c.n_sources;
+    for( int k = 0; k < c.n_sources; ++ k )
+    {
+        const auto & s = c.sources[ k ];
+        require( s.kind == KP_SOURCE_POINT || s.kind == KP_SOURCE_PLANE_BASE, "unknown source" );
+        require( s.emit == KP_EMIT_ISOTROPIC || s.emit == KP_EMIT_UP_UNIFORM, "unknown emission" );
+        auto & d = P.src[ k ];
+        d.kind = s.kind;
+        d.emit = s.emit;
+        for( int a = 0; a < 3; ++ a ) d.pos[ a ] = s.pos[ a ];
+        d.ib = 0;
+        d.cell[ 0 ] = d.cell[ 1 ] = d.cell[ 2 ] = 0;
+        if( s.kind == KP_SOURCE_POINT )
+            require( mesh->tree->locate( s.pos, d.ib, d.cell ), "source outside the mesh",
+                     KP_ERR_CONFIG );
+    }
+    P.n_mu = c.n_mu_bins;
+    P.mu_lo = c.mu_lo;
+    P.mu_inv_w = c.n_mu_bins > 0 ? ( float ) ( c.n_mu_bins / ( ( double ) c.mu_hi - c.mu_lo ) ) : 0.f;
+    P.img_n = c.image_n;
+    // Observer at inclination i from +z and azimuth az about +z; image
+    // vertical ev is the projection of +z, horizontal eh = ev x o.
+    const double inc = c.inclination_deg * M_PI / 180.0, az = c.azimuth_deg * M_PI / 180.0;
+    const float o[ 3 ]  = { ( float ) ( std::sin( inc ) * std::cos( az ) ),
+                            ( float ) ( std::sin( inc ) * std::sin( az ) ),
+                            ( float ) std::cos( inc ) };
+    const float ev[ 3 ] = { ( float ) ( -std::cos( inc ) * std::cos( az ) ),
+                            ( float ) ( -std::cos( inc ) * std::sin( az ) ),
+                            ( float ) std::sin( inc ) };
+    const float eh[ 3 ] = { ev[ 1 ] * o[ 2 ] - ev[ 2 ] * o[ 1 ],
+                            ev[ 2 ] * o[ 0 ] - ev[ 0 ] * o[ 2 ],
+                            ev[ 0 ] * o[ 1 ] - ev[ 1 ] * o[ 0 ] };
+    P.o  = phys::v3 { o[ 0 ], o[ 1 ], o[ 2 ] };
+    P.ev = phys::v3 { ev[ 0 ], ev[ 1 ], ev[ 2 ] };
+    P.eh = phys::v3 { eh[ 0 ], eh[ 1 ], eh[ 2 ] };
+    for( int a = 0; a < 3; ++ a )
+    {
+        P.o_d[ a ]  = o[ a ];
+        P.ev_d[ a ] = ev[ a ];
+        P.eh_d[ a ] = eh[ a ];
+        P.inv_o[ a ] = o[ a ] != 0.0f ? 1.0 / ( double ) o[ a ] : 0.0;
+        P.img_c[ a ] = c.image_center[ a ];
+        P.lk_inv[ a ] = tab.lookup_n[ a ] / tab.l_box_d[ a ];
+    }
+    P.img_inv_pix = c.image_n > 0 ? c.image_n / ( 2.0 * c.image_half_width ) : 0.0;
+    P.tau_cut = c.tau_peel_max > 0 ? c.tau_peel_max : 40.0f;
+    P.fx_scale = std::ldexp( 1.0, c.fx_shift );
+    P.n_batch = c.n_batches;
+    P.w_min = c.w_min;
+    P.rr_survive = c.rr_survive > 0 ? c.rr_survive : 0.1f;
+    P.max_scatter = c.max_scatter;
+    P.max_steps = c.max_steps;
+    P.mu_tally = t.mu;
+    P.image = t.image;
+    P.img_batch = t.image_batch;
+    P.counters = t.counters;
+    P.records = t.records;
+    P.n_record = c.n_record;
+}
+
+int persistent_grid( const void * kernel, int threads )
+{
+    int dev = 0, n_sm = 0, per_sm = 0;
+    KP_CUDA( cudaGetDevice( & dev ) );
+    KP_CUDA( cudaDeviceGetAttribute( & n_sm, cudaDevAttrMultiProcessorCount, dev ) );
+    KP_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( & per_sm, kernel, threads, 0 ) );
+    return n_sm * std::max( per_sm, 1 );
+}
+
+void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s )
+{
+    if( P.n_packets == 0 ) return;
+    const int threads = 256;
+    const void * k = tally_mode == KP_TALLY_FIXED ? ( const void * ) k_forward< KP_TALLY_FIXED >
+                                                  : ( const void * ) k_forward< KP_TALLY_FLOAT >;
+    long long grid = persistent_grid( k, threads );
+    grid = std::min< long long >( grid, ( P.n_packets + threads - 1 ) / threads );
+    KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
+    if( tally_mode == KP_TALLY_FIXED )
+        k_forward< KP_TALLY_FIXED ><<< ( unsigned ) grid, threads, 0, s >>>( P );
+    else
+        k_forward< KP_TALLY_FLOAT ><<< ( unsigned ) grid, threads, 0, s >>>( P );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+
+}   // namespace kp
+
+extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                     const kp_tallies_t * tallies, void * stream )
+{
+    return kp::guarded( "kp_transport_forward", [ & ]
+    {
+        kp::require( mesh && cfg && tallies, "null argument" );
+        mesh->upload(  );
+        static thread_local kp::fwd_params_t P;
+        kp::make_fwd_params( mesh, * cfg, * tallies, P );
+        P.work = mesh->workspace(  );
+        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream );
+    } );
+}

@@ -1,0 +1,379 @@
+// Device building blocks of the polarized transport kernels: packet state,
+// emission, the FP64 cell walk with AMR hand-off, peel-off and tallies.
+//
+// The walk keeps the reference's cell-by-cell structure (one segment per
+// loop iteration, modules/particle/radiation/photon.h:104-125) and its
+// face-neighbour hand-off (types/proxy.h:64-121: sub-face chosen by the
+// transverse half when the neighbour is finer), with these differences of
+// design: positions are FP64 with precomputed inverse directions, the
+// crossing coordinate is snapped to the new block's face (this also performs
+// the periodic wrap of par_base_t::regulate, particle_base.h:37-56), and the
+// transverse cell indices are recomputed from the position after a block
+// change.
+#pragma once
+
+#include "kp_common.cuh"
+#include "kp_physics.cuh"
+
+#include <cooperative_groups.h>
+
+namespace kp
+{
+
+constexpr int MAX_SOURCES = KP_MAX_SOURCES;
+
+struct src_dev_t
+{
+    double pos[ 3 ];
+    int    ib;
+    int    cell[ 3 ];
+    int    kind;
+    int    emit;
+};
+
+// Everything a transport launch reads, passed by value.
+struct fwd_params_t
+{
+    mesh_view_t m;
+    long long   n_packets;         // packets of this launch
+    long long   pid0;              // global id of the first packet
+    uint32_t    seed, stream;
+    phys::phase_t ph;
+    int         n_src;
+    int         n_mu;
+    float       mu_lo, mu_inv_w;
+    int         img_n;
+    phys::v3    o, ev, eh;         // observer direction, image frame
+    double      inv_o[ 3 ];
+    double      o_d[ 3 ], ev_d[ 3 ], eh_d[ 3 ], img_c[ 3 ];
+    double      img_inv_pix;
+    float       tau_cut;
+    double      fx_scale;
+    int         n_batch;
+    float       w_min, rr_survive;
+    int         max_scatter;
+    long long   max_steps;
+    double      lk_inv[ 3 ];       // lookup cells per unit length
+    void      * mu_tally;
+    void      * image;
+    void      * img_batch;
+    unsigned long long * counters;
+    kp_packet_record_t * records;
+    long long   n_record;
+    unsigned long long * work;     // scratch: next packet index
+    src_dev_t   src[ MAX_SOURCES ];
+};
+
+enum pk_status { PK_ESCAPED = 1, PK_ABSORBED = 2, PK_SCATTER_CAP = 3, PK_STEP_CAP = 4,
+                 PK_LOST = 5 };
+
+struct packet_t
+{
+    double        x[ 3 ];
+    double        inv[ 3 ];
+    phys::v3      d, e1;
+    phys::stokes_t S;
+    float         w, tau;
+    int           b;
+    int           c[ 3 ];
+    int           n_scat;
+    long long     n_steps;
+    long long     pid;
+    phys::rng_t   rng;
+};
+
+struct local_counts_t
+{
+    unsigned long long steps = 0, peel = 0, scat = 0, esc = 0, absb = 0, cap = 0,
+                       lost = 0, emit = 0;
+};
+
+__device__ __forceinline__ float comp( const phys::v3 & v, int a )
+{
+    return a == 0 ? v.x : ( a == 1 ? v.y : v.z );
+}
+
+__device__ __forceinline__ void set_inv( packet_t & p )
+{
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        const float da = comp( p.d, a );
+        p.inv[ a ] = da != 0.0f ? __ddiv_rn( 1.0, ( double ) da ) : 0.0;
+    }
+}
+
+__device__ __forceinline__ size_t cell_index( const mesh_view_t & m, int b, const int c[ 3 ] )
+{
+    return ( size_t ) b * m.cpb + c[ 0 ] + m.nc[ 0 ] * ( c[ 1 ] + m.nc[ 1 ] * c[ 2 ] );
+}
+
+// Distance along d to the exit face of cell c of block b (first axis wins
+// ties; axes with d == 0 never exit).
+__device__ __forceinline__ double exit_dist( const mesh_view_t & m, int b, const int c[ 3 ],
+                                             const double x[ 3 ], const phys::v3 & d,
+                                             const double inv[ 3 ], int & ax )
+{
+    const double * g = m.geo_d + 16 * ( size_t ) b;
+    double t = 1e300;
+    ax = 0;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        const float da = comp( d, a );
+        if( da == 0.0f ) continue;
+        const double face = __fma_rn( ( double ) ( c[ a ] + ( da > 0.0f ? 1 : 0 ) ),
+                                      g[ 3 + a ], g[ a ] );
+        double ta = __dmul_rn( __dsub_rn( face, x[ a ] ), inv[ a ] );
+        ta = ta < 0.0 ? 0.0 : ta;
+        if( ta < t ) { t = ta; ax = a; }
+    }
+    return t;
+}
+
+// Steps into the neighbouring cell across face `ax` (x already advanced on
+// the other axes).  Returns false when the packet leaves the domain
+// (physical boundary) or finds no neighbour (lost = true).
+__device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int c[ 3 ],
+                                            double x[ 3 ], int ax, bool pos, bool & lost )
+{
+    lost = false;
+    int cn = c[ ax ] + ( pos ? 1 : -1 );
+    const double * g = m.geo_d + 16 * ( size_t ) b;
+    if( cn >= 0 && cn < m.nc[ ax ] )
+    {
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+            if( a == ax )
+            {
+                c[ a ] = cn;
+                x[ a ] = __fma_rn( ( double ) ( pos ? cn : cn + 1 ), g[ 3 + a ], g[ a ] );
+            }
+        return true;
+    }
+    const blk_meta_t md = m.meta[ b ];
+    const int side = pos ? 1 : 0;
+    if( ( md.phybnd >> ( 2 * ax + side ) ) & 1 )
+        return false;
+    const int a1 = ax == 2 ? 0 : ax + 1;
+    const int a2 = ax == 0 ? 2 : ax - 1;
+    int ca1 = 0, ca2 = 0;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { if( a == a1 ) ca1 = c[ a ]; if( a == a2 ) ca2 = c[ a ]; }
+    int j0 = 0, j1 = 0;
+    if( md.d_lvl[ 2 * ax + side ] > 0 )
+    {
+        j0 = ca1 >= m.nc[ a1 ] / 2;
+        j1 = ca2 >= m.nc[ a2 ] / 2;
+    }
+    const int nid = m.nb[ 24 * ( size_t ) b + ( ( ax * 2 + side ) * 2 + j0 ) * 2 + j1 ];
+    if( nid < 0 || nid >= m.n_blocks )
+    {
+        lost = true;
+        return false;
+    }
+    b = nid;
+    const double * h = m.geo_d + 16 * ( size_t ) nid;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        if( a == ax )
+        {
+            c[ a ] = pos ? 0 : m.nc[ a ] - 1;
+            x[ a ] = pos ? h[ a ] : __fma_rn( ( double ) m.nc[ a ], h[ 3 + a ], h[ a ] );
+        }
+        else
+        {
+            const double f = floor( __dmul_rn( __dsub_rn( x[ a ], h[ a ] ), h[ 8 + a ] ) );
+            int ci = f < 0.0 ? 0 : ( f > ( double ) ( m.nc[ a ] - 1 ) ? m.nc[ a ] - 1 : ( int ) f );
+            c[ a ] = ci;
+        }
+    }
+    return true;
+}
+
+// Optical depth from x to the domain boundary along the observer direction;
+// stops early (returns > tau_cut) once tau_cut is exceeded.
+__device__ __forceinline__ float peel_tau( const fwd_params_t & P, int b, const int c0[ 3 ],
+                                           const double x0[ 3 ], unsigned long long & steps )
+{
+    int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
+    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
+    float tau = 0.0f;
+    for( int k = 0; k < ( 1 << 20 ); ++ k )
+    {
+        const float2 sg = P.m.sigma[ cell_index( P.m, b, c ) ];
+        const float ext = __fadd_rn( sg.x, sg.y );
+        int ax;
+        const double t = exit_dist( P.m, b, c, x, P.o, P.inv_o, ax );
+        tau = __fadd_rn( tau, __fmul_rn( ext, ( float ) t ) );
+        ++ steps;
+        if( tau > P.tau_cut )
+            return tau;
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+            if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
+        bool lost;
+        if( ! cross_face( P.m, b, c, x, ax, comp( P.o, ax ) > 0.0f, lost ) )
+            return tau;
+    }
+    return tau;
+}
+
+template< int TALLY >
+__device__ __forceinline__ void add_tally( void * base, size_t i, float v, double sc )
+{
+    if( TALLY == KP_TALLY_FIXED )
+        atomicAdd( ( unsigned long long * ) base + i,
+                   ( unsigned long long ) __double2ll_rn( __dmul_rn( ( double ) v, sc ) ) );
+    else
+        atomicAdd( ( float * ) base + i, v );
+}
+
+// Adds a peel-off contribution (intensity per steradian I and image-frame
+// Q, U, V, already weighted) to the pixel under x.
+template< int TALLY >
+__device__ __forceinline__ void deposit_image( const fwd_params_t & P, const double x[ 3 ],
+                                               long long pid, float I, float Q, float U, float V )
+{
+    double r[ 3 ];
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) r[ a ] = __dsub_rn( x[ a ], P.img_c[ a ] );
+    const double hp = __dadd_rn( __dadd_rn( __dmul_rn( r[ 0 ], P.eh_d[ 0 ] ),
+                                            __dmul_rn( r[ 1 ], P.eh_d[ 1 ] ) ),
+                                 __dmul_rn( r[ 2 ], P.eh_d[ 2 ] ) );
+    const double vp = __dadd_rn( __dadd_rn( __dmul_rn( r[ 0 ], P.ev_d[ 0 ] ),
+                                            __dmul_rn( r[ 1 ], P.ev_d[ 1 ] ) ),
+                                 __dmul_rn( r[ 2 ], P.ev_d[ 2 ] ) );
+    const double half = 0.5 * P.img_n;
+    const double fx = floor( __fma_rn( hp, P.img_inv_pix, half ) );
+    const double fy = floor( __fma_rn( vp, P.img_inv_pix, half ) );
+    const int batch = ( int ) ( pid % P.n_batch );
+    add_tally< TALLY >( P.img_batch, 4 * batch + 0, I, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, 4 * batch + 1, Q, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, 4 * batch + 2, U, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, 4 * batch + 3, V, P.fx_scale );
+    if( fx < 0.0 || fy < 0.0 || fx >= P.img_n || fy >= P.img_n )
+        return;
+    const size_t pix = ( ( size_t ) fy * P.img_n + ( size_t ) fx ) * 4;
+    add_tally< TALLY >( P.image, pix + 0, I, P.fx_scale );
+    add_tally< TALLY >( P.image, pix + 1, Q, P.fx_scale );
+    add_tally< TALLY >( P.image, pix + 2, U, P.fx_scale );
+    add_tally< TALLY >( P.image, pix + 3, V, P.fx_scale );
+}
+
+// Escape tally: mu = d.z bins, Stokes in the meridian frame (Q > 0 in the
+// plane of d and +z).
+template< int TALLY >
+__device__ __forceinline__ void tally_escape( const fwd_params_t & P, const packet_t & p )
+{
+    if( P.n_mu <= 0 ) return;
+    const float fb = floorf( __fmul_rn( __fsub_rn( p.d.z, P.mu_lo ), P.mu_inv_w ) );
+    if( !( fb >= 0.0f && fb < ( float ) P.n_mu ) ) return;
+    const int bin = ( int ) fb;
+    const phys::v3 e2 = phys::cross( p.d, p.e1 );
+    float c2, s2;
+    phys::double_angle( p.e1.z, e2.z, c2, s2 );
+    float q = p.S.q, u = p.S.u;
+    phys::rotate( q, u, c2, s2 );
+    const int batch = ( int ) ( p.pid % P.n_batch );
+    const size_t i = ( ( size_t ) batch * P.n_mu + bin ) * 4;
+    add_tally< TALLY >( P.mu_tally, i + 0, p.w, P.fx_scale );
+    add_tally< TALLY >( P.mu_tally, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
+    add_tally< TALLY >( P.mu_tally, i + 2, __fmul_rn( p.w, u ), P.fx_scale );
+    add_tally< TALLY >( P.mu_tally, i + 3, __fmul_rn( p.w, p.S.v ), P.fx_scale );
+}
+
+__device__ __forceinline__ float sample_tau( phys::rng_t & rng )
+{
+    const phys::u4 r = rng.next(  );
+    return ( float ) ( -phys::kp_log( ( double ) phys::u01( r.x ) ) );
+}
+
+// Direction uniform on the sphere (emit 0) or with mu uniform in (0,1)
+// about +z (emit 1); (cos phi, sin phi) from a point in the unit disk.
+__device__ __forceinline__ phys::v3 sample_emission_dir( phys::rng_t & rng, int emit )
+{
+    float mu = 0.0f, a = 1.0f, b = 0.0f, r2 = 1.0f;
+    for( int trial = 0; trial < 64; ++ trial )
+    {
+        const phys::u4 r = rng.next(  );
+        mu = emit == KP_EMIT_UP_UNIFORM ? phys::u01( r.x ) : phys::usym( r.x );
+        a  = phys::usym( r.y );
+        b  = phys::usym( r.z );
+        r2 = __fadd_rn( __fmul_rn( a, a ), __fmul_rn( b, b ) );
+        if( r2 <= 1.0f && r2 > 0.0f ) break;
+        a = 1.0f; b = 0.0f; r2 = 1.0f;
+    }
+    const float rr = __fsqrt_rn( r2 );
+    return phys::dir_from( mu, __fdiv_rn( a, rr ), __fdiv_rn( b, rr ) );
+}
+
+// Creates packet `pid` (global id) at its source.  Returns false if the
+// source position lies outside the mesh.
+__device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long pid, packet_t & p )
+{
+    p.pid = pid;
+    p.rng = phys::rng_t { P.seed, P.stream, ( uint32_t ) pid, ( uint32_t ) ( pid >> 32 ), 0u };
+    const src_dev_t & s = P.src[ pid % P.n_src ];
+    if( s.kind == KP_SOURCE_POINT )
+    {
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a ) { p.x[ a ] = s.pos[ a ]; p.c[ a ] = s.cell[ a ]; }
+        p.b = s.ib;
+    }
+    else
+    {   // uniform over the domain's lower z face
+        const phys::u4 r = p.rng.next(  );
+        p.x[ 0 ] = __fma_rn( ( double ) phys::u01( r.x ), P.m.lbox_d[ 0 ], P.m.xlim_d[ 0 ][ 0 ] );
+        p.x[ 1 ] = __fma_rn( ( double ) phys::u01( r.y ), P.m.lbox_d[ 1 ], P.m.xlim_d[ 0 ][ 1 ] );
+        p.x[ 2 ] = P.m.xlim_d[ 0 ][ 2 ];
+        int li[ 3 ];
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+        {
+            const double f = floor( __dmul_rn( __dsub_rn( p.x[ a ], P.m.xlim_d[ 0 ][ a ] ),
+                                               P.lk_inv[ a ] ) );
+            li[ a ] = f < 0.0 ? 0 : ( f >= P.m.lookup_n[ a ] ? P.m.lookup_n[ a ] - 1 : ( int ) f );
+        }
+        p.b = P.m.lookup[ ( ( size_t ) li[ 2 ] * P.m.lookup_n[ 1 ] + li[ 1 ] )
+                          * P.m.lookup_n[ 0 ] + li[ 0 ] ];
+        if( p.b < 0 || p.b >= P.m.n_blocks ) return false;
+        const double * h = P.m.geo_d + 16 * ( size_t ) p.b;
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+        {
+            const double f = floor( __dmul_rn( __dsub_rn( p.x[ a ], h[ a ] ), h[ 8 + a ] ) );
+            p.c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( P.m.nc[ a ] - 1 ) ? P.m.nc[ a ] - 1 : ( int ) f );
+        }
+    }
+    if( p.b < 0 || p.b >= P.m.n_blocks ) return false;
+    p.d  = sample_emission_dir( p.rng, s.emit );
+    p.e1 = phys::frame_for( p.d );
+    p.S  = phys::stokes_t { 0.0f, 0.0f, 0.0f };
+    p.w  = 1.0f;
+    p.n_scat  = 0;
+    p.n_steps = 0;
+    set_inv( p );
+    return true;
+}
+
+__device__ __forceinline__ void write_record( const fwd_params_t & P, const packet_t & p, int status )
+{
+    const long long k = p.pid - P.pid0;
+    if( P.records == nullptr || k < 0 || k >= P.n_record ) return;
+    kp_packet_record_t r;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { r.x[ a ] = p.x[ a ]; r.cell[ a ] = p.c[ a ]; }
+    r.d[ 0 ] = p.d.x; r.d[ 1 ] = p.d.y; r.d[ 2 ] = p.d.z;
+    r.stokes[ 0 ] = p.S.q; r.stokes[ 1 ] = p.S.u; r.stokes[ 2 ] = p.S.v;
+    r.w = p.w;
+    r.ib = p.b;
+    r.n_scatter = p.n_scat;
+    r.status = status;
+    r.rng_draws = p.rng.draw;
+    r.n_steps = p.n_steps;
+    P.records[ k ] = r;
+}
+
+}   // namespace kp

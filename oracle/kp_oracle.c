@@ -5,6 +5,7 @@
 
 #include <float.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 enum { TO_KEEP = -2, TO_RM = -3 };   /* particle::todo_t, particle_base.h:12 */
@@ -166,4 +167,453 @@ int kpo_trace( const kpo_mesh_t * m, int precision, long n, double * x,
                       step + p, todo + p, scale, flux_f, flux_fx );
     }
     return 0;
+}
+
+/* ====================================================================== */
+/* Polarized transport restatement                                         */
+
+#include "oracle_math.h"
+
+enum { ST_ESCAPED = 1, ST_ABSORBED = 2, ST_SCATTER_CAP = 3, ST_STEP_CAP = 4, ST_LOST = 5 };
+
+typedef struct
+{
+    const kpo_mesh_t * m;
+    const float      * sig;
+    const int        * lookup;
+    int                lk_n[ 3 ];
+    double             lk_inv[ 3 ];
+    double           * inv_dx;         /* [nb][3] */
+    int                cpb;
+    om_phase           ph;
+    int                n_mu;
+    float              mu_lo, mu_inv_w;
+    int                img_n;
+    om_v3              o, ev, eh;
+    double             inv_o[ 3 ], o_d[ 3 ], ev_d[ 3 ], eh_d[ 3 ], img_c[ 3 ];
+    double             img_inv_pix;
+    float              tau_cut;
+    double             fx_scale;
+    int                n_batch;
+    float              w_min, rr_survive;
+    int                max_scatter;
+    long long          max_steps;
+    long long         *mu, *image, *img_batch;
+} tctx;
+
+typedef struct
+{
+    double    x[ 3 ], inv[ 3 ];
+    om_v3     d, e1;
+    om_stokes S;
+    float     w, tau;
+    int       b, c[ 3 ], n_scat;
+    long long n_steps, pid;
+    om_rng    rng;
+} tpk;
+
+static long tcell( const tctx * t, int b, const int * c )
+{
+    return ( long ) b * t->cpb + c[ 0 ] + t->m->nc[ 0 ] * ( c[ 1 ] + t->m->nc[ 1 ] * c[ 2 ] );
+}
+
+static void tset_inv( tpk * p )
+{
+    for( int a = 0; a < 3; ++ a )
+    {
+        const float da = om_comp( p->d, a );
+        p->inv[ a ] = da != 0.0f ? 1.0 / ( double ) da : 0.0;
+    }
+}
+
+static double texit( const tctx * t, int b, const int * c, const double * x, om_v3 d,
+                     const double * inv, int * ax )
+{
+    double tm = 1e300;
+    * ax = 0;
+    for( int a = 0; a < 3; ++ a )
+    {
+        const float da = om_comp( d, a );
+        if( da == 0.0f ) continue;
+        const double face = fma( ( double ) ( c[ a ] + ( da > 0.0f ? 1 : 0 ) ),
+                                 t->m->dx0[ 3 * b + a ], t->m->xf0[ 3 * b + a ] );
+        double ta = ( face - x[ a ] ) * inv[ a ];
+        ta = ta < 0.0 ? 0.0 : ta;
+        if( ta < tm ) { tm = ta; * ax = a; }
+    }
+    return tm;
+}
+
+/* returns 1 if still inside, 0 if it left the domain (lost set if no
+ * neighbour) */
+static int tcross( const tctx * t, int * b, int * c, double * x, int ax, int pos, int * lost )
+{
+    const kpo_mesh_t * m = t->m;
+    * lost = 0;
+    const int cn = c[ ax ] + ( pos ? 1 : -1 );
+    if( cn >= 0 && cn < m->nc[ ax ] )
+    {
+        c[ ax ] = cn;
+        x[ ax ] = fma( ( double ) ( pos ? cn : cn + 1 ), m->dx0[ 3 * * b + ax ], m->xf0[ 3 * * b + ax ] );
+        return 1;
+    }
+    const int side = pos ? 1 : 0;
+    if( m->phybnd[ 6 * * b + 2 * ax + side ] ) return 0;
+    const int a1 = ( ax + 1 ) % 3, a2 = ( ax + 2 ) % 3;
+    int j0 = 0, j1 = 0;
+    if( m->d_lvl[ 6 * * b + 2 * ax + side ] > 0 )
+    {
+        j0 = c[ a1 ] >= m->nc[ a1 ] / 2;
+        j1 = c[ a2 ] >= m->nc[ a2 ] / 2;
+    }
+    const int nid = m->nb_id[ 24 * * b + ( ( ax * 2 + side ) * 2 + j0 ) * 2 + j1 ];
+    if( nid < 0 || nid >= m->n_blocks ) { * lost = 1; return 0; }
+    * b = nid;
+    for( int a = 0; a < 3; ++ a )
+    {
+        if( a == ax )
+        {
+            c[ a ] = pos ? 0 : m->nc[ a ] - 1;
+            x[ a ] = pos ? m->xf0[ 3 * nid + a ]
+                         : fma( ( double ) m->nc[ a ], m->dx0[ 3 * nid + a ], m->xf0[ 3 * nid + a ] );
+        }
+        else
+        {
+            const double f = floor( ( x[ a ] - m->xf0[ 3 * nid + a ] ) * t->inv_dx[ 3 * nid + a ] );
+            c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( m->nc[ a ] - 1 ) ? m->nc[ a ] - 1 : ( int ) f );
+        }
+    }
+    return 1;
+}
+
+static float tpeel_tau( const tctx * t, int b, const int * c0, const double * x0,
+                        unsigned long long * steps )
+{
+    int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
+    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
+    float tau = 0.0f;
+    for( int k = 0; k < ( 1 << 20 ); ++ k )
+    {
+        const long ci = tcell( t, b, c );
+        const float ext = t->sig[ 2 * ci ] + t->sig[ 2 * ci + 1 ];
+        int ax;
+        const double tt = texit( t, b, c, x, t->o, t->inv_o, & ax );
+        tau = tau + ext * ( float ) tt;
+        ++ * steps;
+        if( tau > t->tau_cut ) return tau;
+        for( int a = 0; a < 3; ++ a )
+            if( a != ax ) x[ a ] = fma( tt, t->o_d[ a ], x[ a ] );
+        int lost;
+        if( ! tcross( t, & b, c, x, ax, om_comp( t->o, ax ) > 0.0f, & lost ) ) return tau;
+    }
+    return tau;
+}
+
+static void tadd( long long * base, long i, float v, double sc )
+{
+    base[ i ] += llrint( ( double ) v * sc );
+}
+
+static void tdeposit_image( const tctx * t, const double * x, long long pid,
+                            float I, float Q, float U, float V )
+{
+    double r[ 3 ];
+    for( int a = 0; a < 3; ++ a ) r[ a ] = x[ a ] - t->img_c[ a ];
+    const double hp = ( r[ 0 ] * t->eh_d[ 0 ] + r[ 1 ] * t->eh_d[ 1 ] ) + r[ 2 ] * t->eh_d[ 2 ];
+    const double vp = ( r[ 0 ] * t->ev_d[ 0 ] + r[ 1 ] * t->ev_d[ 1 ] ) + r[ 2 ] * t->ev_d[ 2 ];
+    const double half = 0.5 * t->img_n;
+    const double fx = floor( fma( hp, t->img_inv_pix, half ) );
+    const double fy = floor( fma( vp, t->img_inv_pix, half ) );
+    const int batch = ( int ) ( pid % t->n_batch );
+    tadd( t->img_batch, 4 * batch + 0, I, t->fx_scale );
+    tadd( t->img_batch, 4 * batch + 1, Q, t->fx_scale );
+    tadd( t->img_batch, 4 * batch + 2, U, t->fx_scale );
+    tadd( t->img_batch, 4 * batch + 3, V, t->fx_scale );
+    if( fx < 0.0 || fy < 0.0 || fx >= t->img_n || fy >= t->img_n ) return;
+    const long pix = ( ( long ) fy * t->img_n + ( long ) fx ) * 4;
+    tadd( t->image, pix + 0, I, t->fx_scale );
+    tadd( t->image, pix + 1, Q, t->fx_scale );
+    tadd( t->image, pix + 2, U, t->fx_scale );
+    tadd( t->image, pix + 3, V, t->fx_scale );
+}
+
+static void ttally_escape( const tctx * t, const tpk * p )
+{
+    if( t->n_mu <= 0 ) return;
+    const float fb = floorf( ( p->d.z - t->mu_lo ) * t->mu_inv_w );
+    if( !( fb >= 0.0f && fb < ( float ) t->n_mu ) ) return;
+    const int bin = ( int ) fb;
+    const om_v3 e2 = om_cross( p->d, p->e1 );
+    float c2, s2;
+    om_double_angle( p->e1.z, e2.z, & c2, & s2 );
+    float q = p->S.q, u = p->S.u;
+    om_rotate( & q, & u, c2, s2 );
+    const int batch = ( int ) ( p->pid % t->n_batch );
+    const long i = ( ( long ) batch * t->n_mu + bin ) * 4;
+    tadd( t->mu, i + 0, p->w, t->fx_scale );
+    tadd( t->mu, i + 1, p->w * q, t->fx_scale );
+    tadd( t->mu, i + 2, p->w * u, t->fx_scale );
+    tadd( t->mu, i + 3, p->w * p->S.v, t->fx_scale );
+}
+
+static float tsample_tau( om_rng * g )
+{
+    const om_u4 r = om_next( g );
+    return ( float ) ( -om_log( ( double ) om_u01( r.x ) ) );
+}
+
+static om_v3 temit_dir( om_rng * g, int emit )
+{
+    float mu = 0.0f, a = 1.0f, b = 0.0f, r2 = 1.0f;
+    for( int trial = 0; trial < 64; ++ trial )
+    {
+        const om_u4 r = om_next( g );
+        mu = emit == 1 ? om_u01( r.x ) : om_usym( r.x );
+        a = om_usym( r.y );
+        b = om_usym( r.z );
+        r2 = a * a + b * b;
+        if( r2 <= 1.0f && r2 > 0.0f ) break;
+        a = 1.0f; b = 0.0f; r2 = 1.0f;
+    }
+    const float rr = sqrtf( r2 );
+    return om_dir_from( mu, a / rr, b / rr );
+}
+
+static int temit( const tctx * t, const kpo_cfg_t * c, long long pid, tpk * p )
+{
+    const kpo_mesh_t * m = t->m;
+    p->pid = pid;
+    p->rng.k0 = c->seed; p->rng.k1 = c->stream_id;
+    p->rng.pid_lo = ( uint32_t ) pid; p->rng.pid_hi = ( uint32_t ) ( pid >> 32 );
+    p->rng.draw = 0;
+    const kpo_source_t * s = c->sources + pid % c->n_sources;
+    if( s->kind == 0 )
+    {
+        for( int a = 0; a < 3; ++ a ) { p->x[ a ] = s->pos[ a ]; p->c[ a ] = s->cell[ a ]; }
+        p->b = s->ib;
+    }
+    else
+    {
+        const om_u4 r = om_next( & p->rng );
+        p->x[ 0 ] = fma( ( double ) om_u01( r.x ), m->lbox[ 0 ], m->xlim[ 0 ][ 0 ] );
+        p->x[ 1 ] = fma( ( double ) om_u01( r.y ), m->lbox[ 1 ], m->xlim[ 0 ][ 1 ] );
+        p->x[ 2 ] = m->xlim[ 0 ][ 2 ];
+        int li[ 3 ];
+        for( int a = 0; a < 3; ++ a )
+        {
+            const double f = floor( ( p->x[ a ] - m->xlim[ 0 ][ a ] ) * t->lk_inv[ a ] );
+            li[ a ] = f < 0.0 ? 0 : ( f >= t->lk_n[ a ] ? t->lk_n[ a ] - 1 : ( int ) f );
+        }
+        p->b = t->lookup[ ( ( long ) li[ 2 ] * t->lk_n[ 1 ] + li[ 1 ] ) * t->lk_n[ 0 ] + li[ 0 ] ];
+        if( p->b < 0 || p->b >= m->n_blocks ) return 0;
+        for( int a = 0; a < 3; ++ a )
+        {
+            const double f = floor( ( p->x[ a ] - m->xf0[ 3 * p->b + a ] ) * t->inv_dx[ 3 * p->b + a ] );
+            p->c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( m->nc[ a ] - 1 ) ? m->nc[ a ] - 1 : ( int ) f );
+        }
+    }
+    if( p->b < 0 || p->b >= m->n_blocks ) return 0;
+    p->d = temit_dir( & p->rng, s->emit );
+    p->e1 = om_frame_for( p->d );
+    p->S.q = p->S.u = p->S.v = 0.0f;
+    p->w = 1.0f;
+    p->n_scat = 0;
+    p->n_steps = 0;
+    tset_inv( p );
+    return 1;
+}
+
+static void trecord( const kpo_cfg_t * c, kpo_record_t * rec, const tpk * p, int status )
+{
+    const long long k = p->pid - c->packet_offset;
+    if( ! rec || k < 0 || k >= c->n_record ) return;
+    kpo_record_t * r = rec + k;
+    for( int a = 0; a < 3; ++ a ) { r->x[ a ] = p->x[ a ]; r->cell[ a ] = p->c[ a ]; }
+    r->d[ 0 ] = p->d.x; r->d[ 1 ] = p->d.y; r->d[ 2 ] = p->d.z;
+    r->stokes[ 0 ] = p->S.q; r->stokes[ 1 ] = p->S.u; r->stokes[ 2 ] = p->S.v;
+    r->w = p->w; r->ib = p->b; r->n_scatter = p->n_scat; r->status = status;
+    r->rng_draws = p->rng.draw; r->n_steps = p->n_steps;
+}
+
+int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
+                   const int * lookup_n, const kpo_cfg_t * c, long long * mu,
+                   long long * image, long long * img_batch,
+                   unsigned long long * counters, kpo_record_t * rec )
+{
+    tctx t;
+    memset( & t, 0, sizeof( t ) );
+    t.m = m; t.sig = sigma2; t.lookup = lookup;
+    t.cpb = m->nc[ 0 ] * m->nc[ 1 ] * m->nc[ 2 ];
+    t.inv_dx = ( double * ) malloc( sizeof( double ) * 3 * ( size_t ) m->n_blocks );
+    if( ! t.inv_dx ) return -2;
+    for( int b = 0; b < m->n_blocks; ++ b )
+        for( int a = 0; a < 3; ++ a )
+            t.inv_dx[ 3 * b + a ] = 1.0 / m->dx0[ 3 * b + a ];
+    for( int a = 0; a < 3; ++ a )
+    {
+        t.lk_n[ a ] = lookup_n[ a ];
+        t.lk_inv[ a ] = lookup_n[ a ] / m->lbox[ a ];
+    }
+    t.ph.kind = c->phase; t.ph.g = c->hg_g; t.ph.pmax = c->pol_max;
+    t.n_mu = c->n_mu_bins;
+    t.mu_lo = c->mu_lo;
+    t.mu_inv_w = c->n_mu_bins > 0 ? ( float ) ( c->n_mu_bins / ( ( double ) c->mu_hi - c->mu_lo ) ) : 0.f;
+    t.img_n = c->image_n;
+    const double inc = c->inclination_deg * M_PI / 180.0, az = c->azimuth_deg * M_PI / 180.0;
+    const float o[ 3 ]  = { ( float ) ( sin( inc ) * cos( az ) ), ( float ) ( sin( inc ) * sin( az ) ),
+                            ( float ) cos( inc ) };
+    const float ev[ 3 ] = { ( float ) ( -cos( inc ) * cos( az ) ), ( float ) ( -cos( inc ) * sin( az ) ),
+                            ( float ) sin( inc ) };
+    const float eh[ 3 ] = { ev[ 1 ] * o[ 2 ] - ev[ 2 ] * o[ 1 ], ev[ 2 ] * o[ 0 ] - ev[ 0 ] * o[ 2 ],
+                            ev[ 0 ] * o[ 1 ] - ev[ 1 ] * o[ 0 ] };
+    t.o.x = o[ 0 ]; t.o.y = o[ 1 ]; t.o.z = o[ 2 ];
+    t.ev.x = ev[ 0 ]; t.ev.y = ev[ 1 ]; t.ev.z = ev[ 2 ];
+    t.eh.x = eh[ 0 ]; t.eh.y = eh[ 1 ]; t.eh.z = eh[ 2 ];
+    for( int a = 0; a < 3; ++ a )
+    {
+        t.o_d[ a ] = o[ a ]; t.ev_d[ a ] = ev[ a ]; t.eh_d[ a ] = eh[ a ];
+        t.inv_o[ a ] = o[ a ] != 0.0f ? 1.0 / ( double ) o[ a ] : 0.0;
+        t.img_c[ a ] = c->image_center[ a ];
+    }
+    t.img_inv_pix = c->image_n > 0 ? c->image_n / ( 2.0 * c->image_half_width ) : 0.0;
+    t.tau_cut = c->tau_peel_max > 0 ? c->tau_peel_max : 40.0f;
+    t.fx_scale = ldexp( 1.0, c->fx_shift );
+    t.n_batch = c->n_batches;
+    t.w_min = c->w_min;
+    t.rr_survive = c->rr_survive > 0 ? c->rr_survive : 0.1f;
+    t.max_scatter = c->max_scatter;
+    t.max_steps = c->max_steps;
+    t.mu = mu; t.image = image; t.img_batch = img_batch;
+
+    unsigned long long cnt[ 8 ] = { 0, 0, 0, 0, 0, 0, 0, 0 };
+    for( long long k = 0; k < c->n_packets; ++ k )
+    {
+        tpk p;
+        if( ! temit( & t, c, c->packet_offset + k, & p ) ) { free( t.inv_dx ); return -1; }
+        ++ cnt[ 7 ];
+        const kpo_source_t * s = c->sources + p.pid % c->n_sources;
+        if( t.img_n > 0 && s->kind == 0 && s->emit == 0 )
+        {
+            const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ] );
+            if( tau <= t.tau_cut )
+            {
+                const float I = 0x1.45f306p-4f * ( float ) om_exp_neg( -( double ) tau );
+                tdeposit_image( & t, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
+            }
+        }
+        p.tau = tsample_tau( & p.rng );
+        for( ;; )
+        {
+            const long ci = tcell( & t, p.b, p.c );
+            const float ss = sigma2[ 2 * ci ], sa = sigma2[ 2 * ci + 1 ];
+            const float ext = ss + sa;
+            int ax;
+            const double tt = texit( & t, p.b, p.c, p.x, p.d, p.inv, & ax );
+            const float dtau = ext * ( float ) tt;
+            ++ cnt[ 0 ];
+            ++ p.n_steps;
+            int end = 0;
+            if( dtau >= p.tau )
+            {
+                double ti = ( double ) ( p.tau / ext );
+                ti = ti > tt ? tt : ti;
+                p.x[ 0 ] = fma( ti, ( double ) p.d.x, p.x[ 0 ] );
+                p.x[ 1 ] = fma( ti, ( double ) p.d.y, p.x[ 1 ] );
+                p.x[ 2 ] = fma( ti, ( double ) p.d.z, p.x[ 2 ] );
+                ++ p.n_scat;
+                ++ cnt[ 2 ];
+                p.w = p.w * ( ss / ext );
+                if( t.img_n > 0 )
+                {
+                    const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ] );
+                    if( tau <= t.tau_cut )
+                    {
+                        float Q, U, V;
+                        const float I = om_peel_stokes( t.ph, p.d, p.e1, p.S, t.o, t.ev, t.eh,
+                                                        & Q, & U, & V );
+                        const float att = p.w * ( float ) om_exp_neg( -( double ) tau );
+                        tdeposit_image( & t, p.x, p.pid, att * I, att * Q, att * U, att * V );
+                    }
+                }
+                if( p.n_scat >= t.max_scatter )
+                    end = ST_SCATTER_CAP;
+                else if( p.w < t.w_min )
+                {
+                    const om_u4 r = om_next( & p.rng );
+                    if( om_u01( r.x ) < t.rr_survive ) p.w = p.w / t.rr_survive;
+                    else end = ST_ABSORBED;
+                }
+                if( ! end )
+                {
+                    om_scatter( t.ph, & p.rng, & p.d, & p.e1, & p.S );
+                    tset_inv( & p );
+                    p.tau = tsample_tau( & p.rng );
+                }
+            }
+            else
+            {
+                p.tau = p.tau - dtau;
+                for( int a = 0; a < 3; ++ a )
+                    if( a != ax ) p.x[ a ] = fma( tt, ( double ) om_comp( p.d, a ), p.x[ a ] );
+                int lost;
+                if( ! tcross( & t, & p.b, p.c, p.x, ax, om_comp( p.d, ax ) > 0.0f, & lost ) )
+                {
+                    if( lost ) end = ST_LOST;
+                    else { end = ST_ESCAPED; ttally_escape( & t, & p ); }
+                }
+            }
+            if( ! end && p.n_steps >= t.max_steps ) end = ST_STEP_CAP;
+            if( end )
+            {
+                trecord( c, rec, & p, end );
+                cnt[ 3 ] += end == ST_ESCAPED;
+                cnt[ 4 ] += end == ST_ABSORBED;
+                cnt[ 5 ] += end == ST_SCATTER_CAP || end == ST_STEP_CAP;
+                cnt[ 6 ] += end == ST_LOST;
+                break;
+            }
+        }
+    }
+    if( counters )
+        for( int k = 0; k < 8; ++ k ) counters[ k ] += cnt[ k ];
+    free( t.inv_dx );
+    return 0;
+}
+
+/* ====================================================================== */
+/* Unit-test exports of the physics primitives                             */
+
+void kpo_philox( const uint32_t * ctr, const uint32_t * key, uint32_t * out )
+{
+    om_u4 c = { ctr[ 0 ], ctr[ 1 ], ctr[ 2 ], ctr[ 3 ] };
+    const om_u4 r = om_philox( c, key[ 0 ], key[ 1 ] );
+    out[ 0 ] = r.x; out[ 1 ] = r.y; out[ 2 ] = r.z; out[ 3 ] = r.w;
+}
+
+void kpo_log_exp( long n, const double * x, double * ln_x, double * exp_negx )
+{
+    for( long i = 0; i < n; ++ i )
+    {
+        ln_x[ i ] = om_log( x[ i ] );
+        exp_negx[ i ] = om_exp_neg( -x[ i ] );
+    }
+}
+
+/* Scatters n packets travelling along +z (frame e1 = +x) with Stokes
+ * (q, u, v); writes per packet the new direction, frame and Stokes. */
+void kpo_scatter_sample( long n, uint32_t seed, int kind, float g, float pmax,
+                         float q, float u, float v, float * out /* n*9 */ )
+{
+    om_phase ph = { kind, g, pmax };
+    for( long i = 0; i < n; ++ i )
+    {
+        om_rng r = { seed, 7u, ( uint32_t ) i, 0u, 0u };
+        om_v3 d = { 0.0f, 0.0f, 1.0f }, e1 = { 1.0f, 0.0f, 0.0f };
+        om_stokes S = { q, u, v };
+        om_scatter( ph, & r, & d, & e1, & S );
+        float * o = out + 9 * i;
+        o[ 0 ] = d.x; o[ 1 ] = d.y; o[ 2 ] = d.z;
+        o[ 3 ] = e1.x; o[ 4 ] = e1.y; o[ 5 ] = e1.z;
+        o[ 6 ] = S.q; o[ 7 ] = S.u; o[ 8 ] = S.v;
+    }
 }

@@ -51,3 +51,69 @@ int kpo_trace( const kpo_mesh_t * m, int precision, long n, double * x,
 #endif
 
 #endif
+
+/* ---------------------------------------------------------------------- */
+/* Polarized transport restatement (same algorithm and operation order as  */
+/* the device kernels; sequential packets; int64 fixed-point tallies).    */
+#ifndef KPO_TRANSPORT_DECLS
+#define KPO_TRANSPORT_DECLS
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct kpo_source
+{
+    int    kind, emit;      /* 0 point / 1 plane at the lower z face; 0 iso / 1 up */
+    double pos[ 3 ];
+    int    ib;              /* block and cell of a point source              */
+    int    cell[ 3 ];
+} kpo_source_t;
+
+typedef struct kpo_cfg
+{
+    long long n_packets, packet_offset;
+    uint32_t  seed, stream_id;
+    int       phase;
+    float     hg_g, pol_max;
+    int       n_sources;
+    const kpo_source_t * sources;
+    int       n_mu_bins;
+    float     mu_lo, mu_hi;
+    int       image_n;
+    double    inclination_deg, azimuth_deg;
+    double    image_center[ 3 ];
+    double    image_half_width;
+    float     tau_peel_max;
+    int       fx_shift;
+    int       n_batches;
+    float     w_min, rr_survive;
+    int       max_scatter;
+    long long max_steps;
+    long long n_record;
+} kpo_cfg_t;
+
+typedef struct kpo_record
+{
+    double    x[ 3 ];
+    float     d[ 3 ];
+    float     stokes[ 3 ];
+    float     w;
+    int       ib;
+    int       cell[ 3 ];
+    int       n_scatter;
+    int       status;
+    uint32_t  rng_draws;
+    long long n_steps;
+} kpo_record_t;
+
+/* sigma2: [n_cells][2] (sca, abs); lookup: finest-level leaf ids.
+ * Outputs are accumulated into (int64 fixed point). */
+int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
+                   const int * lookup_n, const kpo_cfg_t * c, long long * mu,
+                   long long * image, long long * img_batch,
+                   unsigned long long * counters, kpo_record_t * rec );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -108,3 +108,84 @@ def trace(tab: Tables, precision: int, x, dir, cell, ib, proper, steps, fx_shift
     if st != 0:
         raise RuntimeError("kpo_trace: bad block id")
     return dict(x=x, cell=cell, ib=ib, step=steps, todo=todo, flux=flux_f, flux_fx=flux_fx)
+
+
+# ---------------------------------------------------------------------------
+# Polarized transport restatement (kpo_transport)
+
+class _Source(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("emit", ctypes.c_int), ("pos", ctypes.c_double * 3),
+                ("ib", ctypes.c_int), ("cell", ctypes.c_int * 3)]
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [("n_packets", ctypes.c_longlong), ("packet_offset", ctypes.c_longlong),
+                ("seed", ctypes.c_uint32), ("stream_id", ctypes.c_uint32), ("phase", ctypes.c_int),
+                ("hg_g", ctypes.c_float), ("pol_max", ctypes.c_float), ("n_sources", ctypes.c_int),
+                ("sources", ctypes.POINTER(_Source)), ("n_mu_bins", ctypes.c_int),
+                ("mu_lo", ctypes.c_float), ("mu_hi", ctypes.c_float), ("image_n", ctypes.c_int),
+                ("inclination_deg", ctypes.c_double), ("azimuth_deg", ctypes.c_double),
+                ("image_center", ctypes.c_double * 3), ("image_half_width", ctypes.c_double),
+                ("tau_peel_max", ctypes.c_float), ("fx_shift", ctypes.c_int),
+                ("n_batches", ctypes.c_int), ("w_min", ctypes.c_float), ("rr_survive", ctypes.c_float),
+                ("max_scatter", ctypes.c_int), ("max_steps", ctypes.c_longlong),
+                ("n_record", ctypes.c_longlong)]
+
+
+def lookup_grid(levels, regs, nc_root_blocks):
+    """Finest-level leaf lookup built from the blocks' region keys."""
+    L = int(levels.max())
+    n = [int(v) << L for v in nc_root_blocks]
+    g = np.full((n[2], n[1], n[0]), -1, np.int32)
+    for b, (lev, r) in enumerate(zip(levels, regs)):
+        f = 1 << (L - int(lev))
+        g[r[2] * f:(r[2] + 1) * f, r[1] * f:(r[1] + 1) * f, r[0] * f:(r[0] + 1) * f] = b
+    return g, n
+
+
+def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
+    """Runs the restated transport for a TransportConfig-like ``cfg``.
+
+    ``source_cells``: (ib, cell[3]) per source (point sources), located by
+    the caller.  Returns dict of int64 tallies, counters and records.
+    """
+    src = (_Source * max(1, len(cfg.sources)))()
+    for k, s in enumerate(cfg.sources):
+        src[k].kind, src[k].emit = int(s.kind), int(s.emit)
+        for a in range(3):
+            src[k].pos[a] = float(s.pos[a])
+        ib, cell = source_cells[k]
+        src[k].ib = int(ib)
+        for a in range(3):
+            src[k].cell[a] = int(cell[a])
+    c = _Cfg()
+    for name, _ in _Cfg._fields_:
+        if name in ("sources", "n_sources", "image_center"):
+            continue
+        setattr(c, name, getattr(cfg, name))
+    c.n_sources = len(cfg.sources)
+    c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
+    for a in range(3):
+        c.image_center[a] = float(cfg.image_center[a])
+    nm = max(cfg.n_mu_bins, 1)
+    ni = max(cfg.image_n, 1)
+    out = dict(mu=np.zeros((cfg.n_batches, nm, 4), np.int64),
+               image=np.zeros((ni, ni, 4), np.int64),
+               image_batch=np.zeros((cfg.n_batches, 4), np.int64),
+               counters=np.zeros(8, np.uint64))
+    from kratos_polrad_b200.transport import RECORD_DTYPE
+    rec = np.zeros(max(cfg.n_record, 1), RECORD_DTYPE)
+    sigma2 = np.ascontiguousarray(sigma2, np.float32)
+    lookup = np.ascontiguousarray(lookup, np.int32)
+    lk_n = np.ascontiguousarray(lookup_n, np.int32)
+    s = tab._struct()
+    L = lib()
+    L.kpo_transport.argtypes = [ctypes.c_void_p] * 10
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)
+    st = L.kpo_transport(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
+                         p(out["mu"]), p(out["image"]), p(out["image_batch"]), p(out["counters"]),
+                         p(rec))
+    if st != 0:
+        raise RuntimeError(f"kpo_transport failed ({st})")
+    out["records"] = rec[:cfg.n_record]
+    return out

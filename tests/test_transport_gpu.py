@@ -1,0 +1,66 @@
+"""Polarized transport on the GPU vs the C restatement, bit for bit.
+
+Per-packet final states (position, direction, Stokes, weight, cell, block,
+interaction and step counts, RNG draws), int64 escape tallies, peel-off
+images, batch sums and counters must be identical.
+"""
+import numpy as np
+import pytest
+import torch
+
+from kratos_polrad_b200.transport import TALLY_FLOAT, Tallies, forward
+from oracle import port
+from transport_cases import case, run_oracle
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not port.available(), reason="oracle not built")]
+
+
+@pytest.mark.parametrize("name", ["slab", "amr_point", "hg_multi"])
+def test_transport_bit_exact(name):
+    mesh, sig, t = case(name)
+    mesh.set_sigma(sig)
+    tal = forward(mesh, t)
+    torch.cuda.synchronize()
+    assert mesh.status() == 0
+    ref = run_oracle(mesh, sig, t)
+    rec, rref = tal.record_array(), ref["records"]
+    for f in rec.dtype.names:
+        np.testing.assert_array_equal(rec[f], rref[f], err_msg=f)
+    np.testing.assert_array_equal(tal.counters.cpu().numpy(), ref["counters"].astype(np.int64))
+    if t.n_mu_bins:
+        np.testing.assert_array_equal(tal.mu.cpu().numpy(), ref["mu"])
+    if t.image_n:
+        np.testing.assert_array_equal(tal.image.cpu().numpy(), ref["image"])
+        np.testing.assert_array_equal(tal.image_batch.cpu().numpy(), ref["image_batch"])
+
+
+def test_transport_repeatable_and_split():
+    """Same packets in two launches (offsets) give the same int64 tallies."""
+    mesh, sig, t = case("amr_point")
+    mesh.set_sigma(sig)
+    a = forward(mesh, t)
+    t1 = case("amr_point")[2]
+    t1.n_packets, t1.n_record = 1200, 0
+    b = forward(mesh, t1)
+    t1.packet_offset, t1.n_packets = 1200, 800
+    forward(mesh, t1, b)
+    torch.cuda.synchronize()
+    assert torch.equal(a.image, b.image)
+    assert torch.equal(a.mu, b.mu)
+    assert torch.equal(a.counters, b.counters)
+
+
+def test_float_tally_mode_close_to_fixed():
+    mesh, sig, t = case("amr_point")
+    mesh.set_sigma(sig)
+    fx = forward(mesh, t)
+    t.tally_mode = TALLY_FLOAT
+    t.n_record = 0
+    fl = forward(mesh, t)
+    torch.cuda.synchronize()
+    img_fx = fx.image.cpu().numpy() * fx.scale()
+    img_fl = fl.image.cpu().numpy().astype(np.float64)
+    # float atomics: reordering error <= n_terms * eps * sum|terms| per pixel;
+    # with int64 rounding 2^-32 per term the two agree to 1e-5 of the peak.
+    np.testing.assert_allclose(img_fl, img_fx, rtol=0, atol=1e-5 * np.abs(img_fx).max())
+    np.testing.assert_allclose(img_fl[..., 0].sum(), img_fx[..., 0].sum(), rtol=1e-6)
