@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the polarized photon-packet transport (packet-steps/s).
+
+Workload: the static 2-level AMR clump scene (root 128^3 in 16^3 blocks,
+refined x2 where the density exceeds 3x its mean; Gaussian clump peak 100,
+FWHM 0.1 box; centre-to-edge extinction depth 5; albedo log-uniform in
+[0.5, 0.99], seed 2; 1e7 packets from a central isotropic point source;
+128x128 peel-off I/Q/U/V image; int64 fixed-point tallies).  A step is one
+forward solve of all packets.  Packet-steps are walk segments plus peel-off
+segments (reported separately).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank solves its own 1e7 packets (its own packet-id
+range: weak scaling) and the int64 tallies are summed with one NCCL
+all-reduce per step.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import dataclasses
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "packet-steps/s (walk + peel-off segments), 2-level AMR clump, 1e7 packets"
+UNIT = "packet-steps/s"
+L2_FLUSH_BYTES = 512 << 20      # > 126 MB L2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--packets", type=float, default=1e7)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(cfg, n_packets):
+    return {"workload": "clump_amr_2level", "root_cells": "128^3", "block_cells": "16^3",
+            "levels": 2, "tau_edge": 5.0, "albedo": "log-uniform [0.5,0.99] seed 2",
+            "packets_per_gpu": int(n_packets), "source": "central isotropic point",
+            "image": f"{cfg.image_n}x{cfg.image_n} IQUV peel-off, inclination "
+                     f"{cfg.inclination_deg:g} deg", "tallies": "int64 fixed point",
+            "l2": "flushed between timed steps (512 MiB write)"}
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_packet():
+    """DRAM bytes per packet of the transport kernel from the committed ncu
+    summary (profiles/k_forward_clump_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "k_forward_clump_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["dram_bytes"]) / float(d["packets"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def algorithmic_bytes(c):
+    """Bytes the solve must move: 8 B of (sigma_sca, sigma_abs) per walk or
+    peel-off segment, 8 B per block hand-off, 32 B (int64 IQUV) per tally
+    deposit, and a 64-byte packet state written at emission and read at the
+    end (2 x 64 B per packet)."""
+    return (8 * (c["steps"] + c["peel_steps"]) + 8 * c["hops"] + 32 * c["deposits"]
+            + 128 * c["emitted"])
+
+
+def cpu_baseline(mesh, sigma2, cfg, budget_s=20.0, threads=None):
+    """Times the oracle's C restatement on the host cores over a bounded
+    sample of the same workload (packets 0..n of the same scene)."""
+    from oracle import port
+    threads = threads or os.cpu_count() or 1
+    tab = port.Tables.from_mesh(mesh, 8)
+    lev, reg = mesh.blocks()
+    roots = [int(round((mesh.x_max[a] - mesh.x_min[a]) / (tab.dx0[0, a] * mesh.nc[a] * 2 ** lev[0])))
+             for a in range(3)]
+    grid, gn = port.lookup_grid(lev, reg, roots)
+    cells = []
+    for s in cfg.sources:
+        ib, cell = mesh.locate([s.pos])
+        cells.append((ib[0], cell[0]))
+    # calibrate on a small sample, then size the timed sample to the budget
+    probe = dataclasses.replace(cfg, n_packets=2000, n_record=0)
+    t0 = time.perf_counter()
+    r = port.transport(tab, sigma2, grid, gn, probe, cells)
+    per_pkt = (time.perf_counter() - t0) / 2000
+    chunk = max(50, int(budget_s / per_pkt / threads / 4))
+    n_chunks = threads * 4
+
+    def work(k):
+        c = dataclasses.replace(cfg, n_packets=chunk, packet_offset=k * chunk, n_record=0)
+        return port.transport(tab, sigma2, grid, gn, c, cells)["counters"]
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        outs = list(ex.map(work, range(n_chunks)))
+    dt = time.perf_counter() - t0
+    tot = sum(o.astype(float) for o in outs)
+    steps = float(tot[0] + tot[1])
+    return {"value": steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{chunk * n_chunks} packets (ids 0..{chunk * n_chunks - 1}) of the same scene, "
+                      f"{steps:.3g} packet-steps in {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU implementation of this path on the host cores.
+
+    The reference has no scattering physics for this workload, so the timed
+    CPU implementation is the oracle's restatement (kind "port")."""
+    if rank != 0:
+        return
+    from kratos_polrad_b200 import scenes
+    mesh, sigma2, cfg = scenes.clump_amr(n_packets=int(args.packets))
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(mesh, sigma2, cfg, budget_s=8.0)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 positions / f32 Stokes",
+            "data": "synthetic", "config": workload_config(cfg, args.packets),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    from kratos_polrad_b200 import scenes
+    from kratos_polrad_b200._lib import call, ptr
+    from kratos_polrad_b200.transport import Tallies, forward
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n_pk = int(args.packets)
+    mesh, sigma2, cfg = scenes.clump_amr(n_packets=n_pk)
+    cfg = dataclasses.replace(cfg, packet_offset=rank * n_pk)
+    mesh.set_sigma(sigma2)
+    tal = Tallies(cfg)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def allreduce():
+        if world > 1:
+            for t in (tal.image, tal.mu, tal.image_batch, tal.counters):
+                dist.all_reduce(t)
+
+    for _ in range(args.warmup):
+        tal.zero_()
+        forward(mesh, cfg, tal)
+        allreduce()
+    torch.cuda.synchronize()
+    assert mesh.status() == 0
+
+    # ---- device-timed region: K solves, L2 flushed before each ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    counts = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            tal.zero_()
+            flush.fill_(float(k))
+            ev[k][0].record()
+            kev[k][0].record()
+            forward(mesh, cfg, tal)
+            kev[k][1].record()
+            allreduce()
+            ev[k][1].record()
+            counts.append(tal.counters.clone())
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    kern_ms = [a.elapsed_time(b) for a, b in kev]
+    t_local = sum(step_ms) / 1e3
+    t = torch.tensor([t_local], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_max = float(t.item())
+    c = {k: int(v) for k, v in zip(tal.counts().keys(), counts[-1].cpu().numpy())}
+    if world > 1:   # counters were all-reduced: whole-job totals already
+        job_steps = (c["steps"] + c["peel_steps"]) * args.steps
+    else:
+        job_steps = sum(int(x[0]) + int(x[1]) for x in (cc.cpu().numpy() for cc in counts))
+    value = job_steps / t_max
+
+    # quality: batch-means relative std-error of the tangential polarization
+    scale = 2.0 ** -cfg.fx_shift
+    p_tan, rel_err = scenes.batch_rel_error(tal.image_batch.cpu().numpy() * scale)
+
+    # roofline of the transport kernel (per launch, this rank)
+    c_rank = {k: int(v) for k, v in zip(tal.counts().keys(), counts[-1].cpu().numpy())}
+    if world > 1:
+        c_rank = {k: v // world for k, v in c_rank.items()}
+    kern_s = statistics.mean(kern_ms) / 1e3
+    peak, peak_kind = measured_peak()
+    ach = algorithmic_bytes(c_rank) / kern_s / 1e9
+    tpp = ncu_traffic_per_packet()
+    roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_source": peak_kind, "kernel": "k_forward",
+                "traffic": (tpp * n_pk) if tpp else None,
+                "algorithmic_bytes": algorithmic_bytes(c_rank),
+                "kernel_ms": statistics.mean(kern_ms)}
+
+    # ---- end to end through the C ABI with host buffers ----
+    import ctypes
+    n_cells = mesh.n_cells
+    h_sigma = torch.from_numpy(sigma2.reshape(-1)).pin_memory()
+    h_img = torch.empty_like(tal.image, device="cpu").pin_memory()
+    h_mu = torch.empty_like(tal.mu, device="cpu").pin_memory()
+    h_cnt = torch.empty_like(tal.counters, device="cpu").pin_memory()
+    d_sig = ctypes.c_void_p()
+    call("kp_mesh_sigma_ptr", mesh.handle, ctypes.byref(d_sig))
+    s = torch.cuda.current_stream().cuda_stream
+    e2e_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    h2d = h_sigma.numel() * 4
+    d2h = (h_img.numel() + h_mu.numel() + h_cnt.numel()) * 8
+    e2e_steps = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    for k in range(args.steps):
+        tal.zero_()
+        flush.fill_(float(k))
+        e2e_ev[0].record()
+        call("kp_memcpy_async", d_sig.value, ptr(h_sigma), h2d, s)
+        forward(mesh, cfg, tal)
+        allreduce()
+        call("kp_memcpy_async", ptr(h_img), ptr(tal.image), h_img.numel() * 8, s)
+        call("kp_memcpy_async", ptr(h_mu), ptr(tal.mu), h_mu.numel() * 8, s)
+        call("kp_memcpy_async", ptr(h_cnt), ptr(tal.counters), h_cnt.numel() * 8, s)
+        e2e_ev[1].record()
+        torch.cuda.synchronize()
+        e2e_ms += e2e_ev[0].elapsed_time(e2e_ev[1])
+        e2e_steps += int(h_cnt[0]) + int(h_cnt[1])
+    t2 = torch.tensor([e2e_ms / 1e3], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = (e2e_steps if world > 1 else e2e_steps) / float(t2.item())
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(mesh, sigma2, cfg)
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64 positions / f32 Stokes",
+               "data": "synthetic", "config": workload_config(cfg, n_pk),
+               "walk_steps_per_solve": c_rank["steps"], "peel_steps_per_solve": c_rank["peel_steps"],
+               "pol_tangential": p_tan, "pol_rel_std_err": rel_err,
+               "roofline": roofline, "cpu_baseline": cpu,
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h},
+               "gpu_launches": args.steps, "clocks": clk.summary()}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -198,6 +198,8 @@ enum kp_counter
     KP_CNT_CAPPED,          /* ended by max_scatter or max_steps          */
     KP_CNT_LOST,            /* no neighbour across an inner face          */
     KP_CNT_EMITTED,
+    KP_CNT_HOPS,            /* block-to-block hand-offs (walk and peel-off) */
+    KP_CNT_DEPOSITS,        /* tally deposits (escape bins, image pixels)  */
     KP_NCOUNTERS
 };
 
@@ -232,6 +234,7 @@ typedef struct kp_transport_cfg
     int       tally_mode;      /* enum kp_tally_mode                           */
     int       fx_shift;        /* fixed point: round(value * 2^fx_shift)       */
     int       n_batches;       /* batch-means tallies: packet p -> p % n       */
+    int       image_batch_n;   /* side of the per-batch coarse image (>=1)     */
     float     w_min;           /* Russian roulette below this weight (0: off)  */
     float     rr_survive;      /* roulette survival probability (<=0: 0.1)     */
     int       max_scatter;     /* interactions per packet before it is ended   */
@@ -257,7 +260,8 @@ typedef struct kp_packet_record
  * first call.  Element type int64 (KP_TALLY_FIXED) or float (KP_TALLY_FLOAT).
  *   mu          [n_batches][n_mu_bins][4]  escaping I,Q,U,V (meridian frame)
  *   image       [image_n][image_n][4]      peel-off I,Q,U,V (Q>0 vertical)
- *   image_batch [n_batches][4]             image sums per batch
+ *   image_batch [n_batches][image_batch_n][image_batch_n][4]  coarse image
+ *                                          per batch (pixel i -> i*bn/n)
  *   counters    [KP_NCOUNTERS] uint64 (optional)
  *   records     [n_record] (optional) */
 typedef struct kp_tallies

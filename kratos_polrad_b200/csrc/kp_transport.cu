@@ -48,12 +48,12 @@ k_forward( const __grid_constant__ fwd_params_t P )
             const src_dev_t & s = P.src[ p.pid % P.n_src ];
             if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
             {   // direct light of an isotropic, unpolarized point source
-                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel );
+                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel, cnt.hops );
                 if( tau <= P.tau_cut )
                 {
                     const float I = __fmul_rn( 0x1.45f306p-4f,   // 1 / (4 pi)
                                                ( float ) phys::kp_exp_neg( -( double ) tau ) );
-                    deposit_image< TALLY >( P, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
+                    cnt.dep += deposit_image< TALLY >( P, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
                 }
             }
             p.tau = sample_tau( p.rng );
@@ -84,14 +84,14 @@ k_forward( const __grid_constant__ fwd_params_t P )
             p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, ext ) );
             if( P.img_n > 0 )
             {
-                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel );
+                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel, cnt.hops );
                 if( tau <= P.tau_cut )
                 {
                     float Q, U, V;
                     const float I = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh,
                                                        Q, U, V );
                     const float att = __fmul_rn( p.w, ( float ) phys::kp_exp_neg( -( double ) tau ) );
-                    deposit_image< TALLY >( P, p.x, p.pid, __fmul_rn( att, I ),
+                    cnt.dep += deposit_image< TALLY >( P, p.x, p.pid, __fmul_rn( att, I ),
                                             __fmul_rn( att, Q ), __fmul_rn( att, U ),
                                             __fmul_rn( att, V ) );
                 }
@@ -120,6 +120,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             for( int a = 0; a < 3; ++ a )
                 if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
             bool lost;
+            const int b_old = p.b;
             if( ! cross_face( P.m, p.b, p.c, p.x, ax, comp( p.d, ax ) > 0.0f, lost ) )
             {
                 if( lost )
@@ -127,9 +128,11 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 else
                 {
                     end = PK_ESCAPED;
-                    tally_escape< TALLY >( P, p );
+                    cnt.dep += tally_escape< TALLY >( P, p );
                 }
             }
+            else
+                cnt.hops += p.b != b_old;
         }
         if( ! end && p.n_steps >= P.max_steps )
             end = PK_STEP_CAP;
@@ -153,6 +156,8 @@ k_forward( const __grid_constant__ fwd_params_t P )
         atomicAdd( P.counters + KP_CNT_CAPPED,     cnt.cap );
         atomicAdd( P.counters + KP_CNT_LOST,       cnt.lost );
         atomicAdd( P.counters + KP_CNT_EMITTED,    cnt.emit );
+        atomicAdd( P.counters + KP_CNT_HOPS,       cnt.hops );
+        atomicAdd( P.counters + KP_CNT_DEPOSITS,   cnt.dep );
     }
 }
 
@@ -236,6 +241,9 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
     P.tau_cut = c.tau_peel_max > 0 ? c.tau_peel_max : 40.0f;
     P.fx_scale = std::ldexp( 1.0, c.fx_shift );
     P.n_batch = c.n_batches;
+    require( c.image_n == 0 || ( c.image_batch_n >= 1 && c.image_batch_n <= c.image_n ),
+             "image_batch_n must be in 1..image_n" );
+    P.img_bn = c.image_batch_n >= 1 ? c.image_batch_n : 1;
     P.w_min = c.w_min;
     P.rr_survive = c.rr_survive > 0 ? c.rr_survive : 0.1f;
     P.max_scatter = c.max_scatter;

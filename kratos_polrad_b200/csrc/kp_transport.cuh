@@ -50,6 +50,7 @@ struct fwd_params_t
     float       tau_cut;
     double      fx_scale;
     int         n_batch;
+    int         img_bn;            // coarse per-batch image side
     float       w_min, rr_survive;
     int         max_scatter;
     long long   max_steps;
@@ -85,7 +86,7 @@ struct packet_t
 struct local_counts_t
 {
     unsigned long long steps = 0, peel = 0, scat = 0, esc = 0, absb = 0, cap = 0,
-                       lost = 0, emit = 0;
+                       lost = 0, emit = 0, hops = 0, dep = 0;
 };
 
 __device__ __forceinline__ float comp( const phys::v3 & v, int a )
@@ -195,7 +196,8 @@ __device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int 
 // Optical depth from x to the domain boundary along the observer direction;
 // stops early (returns > tau_cut) once tau_cut is exceeded.
 __device__ __forceinline__ float peel_tau( const fwd_params_t & P, int b, const int c0[ 3 ],
-                                           const double x0[ 3 ], unsigned long long & steps )
+                                           const double x0[ 3 ], unsigned long long & steps,
+                                           unsigned long long & hops )
 {
     int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
     double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
@@ -214,8 +216,10 @@ __device__ __forceinline__ float peel_tau( const fwd_params_t & P, int b, const 
         for( int a = 0; a < 3; ++ a )
             if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
         bool lost;
+        const int b_old = b;
         if( ! cross_face( P.m, b, c, x, ax, comp( P.o, ax ) > 0.0f, lost ) )
             return tau;
+        hops += b != b_old;
     }
     return tau;
 }
@@ -233,7 +237,7 @@ __device__ __forceinline__ void add_tally( void * base, size_t i, float v, doubl
 // Adds a peel-off contribution (intensity per steradian I and image-frame
 // Q, U, V, already weighted) to the pixel under x.
 template< int TALLY >
-__device__ __forceinline__ void deposit_image( const fwd_params_t & P, const double x[ 3 ],
+__device__ __forceinline__ bool deposit_image( const fwd_params_t & P, const double x[ 3 ],
                                                long long pid, float I, float Q, float U, float V )
 {
     double r[ 3 ];
@@ -248,28 +252,32 @@ __device__ __forceinline__ void deposit_image( const fwd_params_t & P, const dou
     const double half = 0.5 * P.img_n;
     const double fx = floor( __fma_rn( hp, P.img_inv_pix, half ) );
     const double fy = floor( __fma_rn( vp, P.img_inv_pix, half ) );
-    const int batch = ( int ) ( pid % P.n_batch );
-    add_tally< TALLY >( P.img_batch, 4 * batch + 0, I, P.fx_scale );
-    add_tally< TALLY >( P.img_batch, 4 * batch + 1, Q, P.fx_scale );
-    add_tally< TALLY >( P.img_batch, 4 * batch + 2, U, P.fx_scale );
-    add_tally< TALLY >( P.img_batch, 4 * batch + 3, V, P.fx_scale );
     if( fx < 0.0 || fy < 0.0 || fx >= P.img_n || fy >= P.img_n )
-        return;
-    const size_t pix = ( ( size_t ) fy * P.img_n + ( size_t ) fx ) * 4;
+        return false;
+    const int ix = ( int ) fx, iy = ( int ) fy;
+    const size_t pix = ( ( size_t ) iy * P.img_n + ix ) * 4;
     add_tally< TALLY >( P.image, pix + 0, I, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 1, Q, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 2, U, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 3, V, P.fx_scale );
+    const int batch = ( int ) ( pid % P.n_batch );
+    const size_t bp = ( ( ( size_t ) batch * P.img_bn + iy * P.img_bn / P.img_n ) * P.img_bn
+                        + ix * P.img_bn / P.img_n ) * 4;
+    add_tally< TALLY >( P.img_batch, bp + 0, I, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, bp + 1, Q, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, bp + 2, U, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, bp + 3, V, P.fx_scale );
+    return true;
 }
 
 // Escape tally: mu = d.z bins, Stokes in the meridian frame (Q > 0 in the
 // plane of d and +z).
 template< int TALLY >
-__device__ __forceinline__ void tally_escape( const fwd_params_t & P, const packet_t & p )
+__device__ __forceinline__ bool tally_escape( const fwd_params_t & P, const packet_t & p )
 {
-    if( P.n_mu <= 0 ) return;
+    if( P.n_mu <= 0 ) return false;
     const float fb = floorf( __fmul_rn( __fsub_rn( p.d.z, P.mu_lo ), P.mu_inv_w ) );
-    if( !( fb >= 0.0f && fb < ( float ) P.n_mu ) ) return;
+    if( !( fb >= 0.0f && fb < ( float ) P.n_mu ) ) return false;
     const int bin = ( int ) fb;
     const phys::v3 e2 = phys::cross( p.d, p.e1 );
     float c2, s2;
@@ -282,6 +290,7 @@ __device__ __forceinline__ void tally_escape( const fwd_params_t & P, const pack
     add_tally< TALLY >( P.mu_tally, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
     add_tally< TALLY >( P.mu_tally, i + 2, __fmul_rn( p.w, u ), P.fx_scale );
     add_tally< TALLY >( P.mu_tally, i + 3, __fmul_rn( p.w, p.S.v ), P.fx_scale );
+    return true;
 }
 
 __device__ __forceinline__ float sample_tau( phys::rng_t & rng )

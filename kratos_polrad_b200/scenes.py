@@ -1,0 +1,116 @@
+"""Synthetic problem set-ups (the counterpart of the reference's user problem
+generator, src/user/probgen.cpp:8-22, whose default ``prob::run`` is empty).
+
+Each builder returns ``(mesh, sigma2, TransportConfig)`` where ``sigma2`` is
+the per-cell (sigma_sca, sigma_abs) array in block-id, x-fastest order.
+All inputs are seeded synthetic fields; no external dataset is involved.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .mesh import Mesh, MeshConfig, RefineRegion
+from .transport import (EMIT_ISOTROPIC, EMIT_UP_UNIFORM, PHASE_HG_POL, PHASE_RAYLEIGH,
+                        SOURCE_PLANE_BASE, SOURCE_POINT, Source, TransportConfig)
+
+
+def cell_centers(mesh: Mesh) -> np.ndarray:
+    """Cell-centre coordinates [n_cells, 3] in the mesh's cell order."""
+    xf0, dx0, _, _ = mesh.geometry(8)
+    nc = mesh.nc
+    k, j, i = np.meshgrid(np.arange(nc[2]), np.arange(nc[1]), np.arange(nc[0]), indexing="ij")
+    idx = np.stack([i.ravel(), j.ravel(), k.ravel()], 1) + 0.5
+    return (xf0[:, None, :] + idx[None] * dx0[:, None, :]).reshape(-1, 3)
+
+
+def root_refine_boxes(field_fn, n_root, block, box_lo, box_hi, threshold, level=1):
+    """One refine region per root block whose field exceeds ``threshold`` at
+    any root-cell centre (static, data-driven refinement expressed as the
+    reference's [refine_region*] boxes)."""
+    nb = [n_root[a] // block[a] for a in range(3)]
+    h = [(box_hi[a] - box_lo[a]) / n_root[a] for a in range(3)]
+    axes = [box_lo[a] + (np.arange(n_root[a]) + 0.5) * h[a] for a in range(3)]
+    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    f = field_fn(np.stack([X, Y, Z], -1)).reshape(nb[2], block[2], nb[1], block[1], nb[0], block[0])
+    fmax = f.max(axis=(1, 3, 5))
+    boxes = []
+    for kz, ky, kx in zip(*np.nonzero(fmax > threshold)):
+        lo = [box_lo[a] + (k + 0.25) * block[a] * h[a] for a, k in enumerate((kx, ky, kz))]
+        hi = [box_lo[a] + (k + 0.75) * block[a] * h[a] for a, k in enumerate((kx, ky, kz))]
+        boxes.append(RefineRegion(level, tuple(lo), tuple(hi)))
+    return boxes
+
+
+def clump_amr(n_packets=10_000_000, n_root=128, block=16, peak=100.0, fwhm=0.1, tau_edge=5.0,
+              albedo=(0.5, 0.99), seed=2, image_n=128, inclination=90.0):
+    """Static 2-level AMR clump: root n_root^3 in block^3, refined x2 where the
+    density exceeds 3x its mean; Gaussian clump (peak, FWHM in box units) on a
+    unit background with centre-to-edge extinction depth tau_edge; per-cell
+    albedo log-uniform in [albedo]; isotropic point source at the centre;
+    peel-off image and int64 tallies."""
+    s = fwhm / (2.0 * math.sqrt(2.0 * math.log(2.0)))
+
+    def rho(x):
+        r2 = ((np.asarray(x) - 0.5) ** 2).sum(-1)
+        return 1.0 + (peak - 1.0) * np.exp(-r2 / (2 * s * s))
+
+    n3 = (n_root,) * 3
+    g = (np.arange(n_root) + 0.5) / n_root
+    mean = (1.0 + (peak - 1.0) * np.exp(-((g - 0.5) ** 2) / (2 * s * s)).mean() ** 3)
+    boxes = root_refine_boxes(rho, n3, (block,) * 3, (0, 0, 0), (1, 1, 1), 3.0 * mean)
+    mesh = Mesh(MeshConfig((0, 0, 0), (1, 1, 1), n3, (block,) * 3, (False,) * 3, boxes))
+    c = cell_centers(mesh)
+    # extinction coefficient: integral of kappa*rho from the centre to a face = tau_edge
+    col = 0.5 + (peak - 1.0) * s * math.sqrt(math.pi / 2) * math.erf(0.5 / (s * math.sqrt(2)))
+    ext = (tau_edge / col) * rho(c)
+    rng = np.random.default_rng(seed)
+    alb = np.exp(rng.uniform(math.log(albedo[0]), math.log(albedo[1]), mesh.n_cells))
+    sigma2 = np.stack([ext * alb, ext * (1.0 - alb)], 1).astype(np.float32)
+    cfg = TransportConfig(n_packets=n_packets, seed=seed,
+                          sources=[Source(SOURCE_POINT, EMIT_ISOTROPIC, (0.5, 0.5, 0.5))],
+                          phase=PHASE_RAYLEIGH, n_mu_bins=20, mu_lo=-1.0, mu_hi=1.0,
+                          image_n=image_n, inclination_deg=inclination,
+                          image_center=(0.5, 0.5, 0.5), image_half_width=0.5,
+                          image_batch_n=8, n_batches=32, w_min=0.01, fx_shift=32)
+    return mesh, sigma2, cfg
+
+
+def slab(n_packets=1_000_000, nx=128, ny=128, nz=64, block=16, tau=10.0, seed=1, n_mu=20):
+    """Plane-parallel electron-scattering slab: periodic in x, y; albedo 1;
+    Thomson (Rayleigh) phase matrix; vertical optical depth tau; unpolarized
+    packets from the base with mu uniform in (0, 1]; escaping I,Q,U,V in
+    n_mu bins of mu in [0, 1]."""
+    mesh = Mesh(MeshConfig((0, 0, 0), (nx, ny, nz), (nx, ny, nz), (block,) * 3,
+                           (True, True, False)))
+    sigma2 = np.zeros((mesh.n_cells, 2), np.float32)
+    sigma2[:, 0] = tau / nz
+    cfg = TransportConfig(n_packets=n_packets, seed=seed,
+                          sources=[Source(SOURCE_PLANE_BASE, EMIT_UP_UNIFORM)],
+                          phase=PHASE_RAYLEIGH, n_mu_bins=n_mu, mu_lo=0.0, mu_hi=1.0,
+                          n_batches=32, fx_shift=24)
+    return mesh, sigma2, cfg
+
+
+def tangential_polarization(img_iquv: np.ndarray) -> float:
+    """Intensity-weighted tangential polarization of an image about its centre:
+    sum(-Q cos 2phi + U sin 2phi) / sum(I), phi the pixel's position angle
+    from the vertical toward the horizontal image axis (positive for the
+    centrosymmetric pattern of scattered light).  The image's Stokes frame is
+    e1 = vertical, e2 = -horizontal, hence the sign of the U term."""
+    n = img_iquv.shape[0]
+    c = (np.arange(n) + 0.5) - n / 2
+    Y, X = np.meshgrid(c, c, indexing="ij")
+    phi = np.arctan2(X, Y)
+    I, Q, U = (img_iquv[..., k].astype(np.float64) for k in range(3))
+    return float((-Q * np.cos(2 * phi) + U * np.sin(2 * phi)).sum() / max(I.sum(), 1e-300))
+
+
+def batch_rel_error(batch_images: np.ndarray) -> tuple[float, float]:
+    """Tangential polarization and its batch-means relative std-error from
+    per-batch coarse images [n_batches, bn, bn, 4]."""
+    p = np.array([tangential_polarization(b) for b in batch_images])
+    tot = tangential_polarization(batch_images.sum(0))
+    err = p.std(ddof=1) / math.sqrt(len(p))
+    return tot, (err / abs(tot) if tot != 0 else float("inf"))

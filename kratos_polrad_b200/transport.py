@@ -28,7 +28,7 @@ EMIT_ISOTROPIC, EMIT_UP_UNIFORM = 0, 1
 TALLY_FIXED, TALLY_FLOAT = 0, 1
 MAX_SOURCES, MAX_BATCHES = 64, 64
 COUNTERS = ("steps", "peel_steps", "scatter", "escaped", "absorbed", "capped", "lost",
-            "emitted")
+            "emitted", "hops", "deposits")
 
 
 class CSource(ctypes.Structure):
@@ -43,7 +43,8 @@ class CTransportCfg(ctypes.Structure):
                 ("image_n", c_int), ("inclination_deg", c_double), ("azimuth_deg", c_double),
                 ("image_center", c_double * 3), ("image_half_width", c_double),
                 ("tau_peel_max", c_float), ("tally_mode", c_int), ("fx_shift", c_int),
-                ("n_batches", c_int), ("w_min", c_float), ("rr_survive", c_float),
+                ("n_batches", c_int), ("image_batch_n", c_int), ("w_min", c_float),
+                ("rr_survive", c_float),
                 ("max_scatter", c_int), ("max_steps", c_ll), ("n_record", c_ll)]
 
 
@@ -92,10 +93,11 @@ class TransportConfig:
     tally_mode: int = TALLY_FIXED
     fx_shift: int = 32
     n_batches: int = 32
+    image_batch_n: int = 1
     w_min: float = 0.0
     rr_survive: float = 0.1
     max_scatter: int = 100000
-    max_steps: int = 1 << 40
+    max_steps: int = 1 << 24
     n_record: int = 0
 
     def to_c(self):
@@ -126,7 +128,8 @@ class Tallies:
         self.mu = torch.zeros((cfg.n_batches, max(cfg.n_mu_bins, 1), 4), dtype=dt, device=device)
         n = max(cfg.image_n, 1)
         self.image = torch.zeros((n, n, 4), dtype=dt, device=device)
-        self.image_batch = torch.zeros((cfg.n_batches, 4), dtype=dt, device=device)
+        bn = max(cfg.image_batch_n, 1)
+        self.image_batch = torch.zeros((cfg.n_batches, bn, bn, 4), dtype=dt, device=device)
         self.counters = torch.zeros(len(COUNTERS), dtype=torch.int64, device=device)
         self.records = (torch.zeros((max(cfg.n_record, 1), 88), dtype=torch.uint8, device=device)
                         if cfg.n_record else None)

@@ -194,7 +194,7 @@ typedef struct
     double             img_inv_pix;
     float              tau_cut;
     double             fx_scale;
-    int                n_batch;
+    int                n_batch, img_bn;
     float              w_min, rr_survive;
     int                max_scatter;
     long long          max_steps;
@@ -287,7 +287,7 @@ static int tcross( const tctx * t, int * b, int * c, double * x, int ax, int pos
 }
 
 static float tpeel_tau( const tctx * t, int b, const int * c0, const double * x0,
-                        unsigned long long * steps )
+                        unsigned long long * steps, unsigned long long * hops )
 {
     int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
     double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
@@ -304,7 +304,9 @@ static float tpeel_tau( const tctx * t, int b, const int * c0, const double * x0
         for( int a = 0; a < 3; ++ a )
             if( a != ax ) x[ a ] = fma( tt, t->o_d[ a ], x[ a ] );
         int lost;
+        const int b_old = b;
         if( ! tcross( t, & b, c, x, ax, om_comp( t->o, ax ) > 0.0f, & lost ) ) return tau;
+        * hops += b != b_old;
     }
     return tau;
 }
@@ -314,8 +316,8 @@ static void tadd( long long * base, long i, float v, double sc )
     base[ i ] += llrint( ( double ) v * sc );
 }
 
-static void tdeposit_image( const tctx * t, const double * x, long long pid,
-                            float I, float Q, float U, float V )
+static int tdeposit_image( const tctx * t, const double * x, long long pid,
+                           float I, float Q, float U, float V )
 {
     double r[ 3 ];
     for( int a = 0; a < 3; ++ a ) r[ a ] = x[ a ] - t->img_c[ a ];
@@ -324,24 +326,28 @@ static void tdeposit_image( const tctx * t, const double * x, long long pid,
     const double half = 0.5 * t->img_n;
     const double fx = floor( fma( hp, t->img_inv_pix, half ) );
     const double fy = floor( fma( vp, t->img_inv_pix, half ) );
-    const int batch = ( int ) ( pid % t->n_batch );
-    tadd( t->img_batch, 4 * batch + 0, I, t->fx_scale );
-    tadd( t->img_batch, 4 * batch + 1, Q, t->fx_scale );
-    tadd( t->img_batch, 4 * batch + 2, U, t->fx_scale );
-    tadd( t->img_batch, 4 * batch + 3, V, t->fx_scale );
-    if( fx < 0.0 || fy < 0.0 || fx >= t->img_n || fy >= t->img_n ) return;
-    const long pix = ( ( long ) fy * t->img_n + ( long ) fx ) * 4;
+    if( fx < 0.0 || fy < 0.0 || fx >= t->img_n || fy >= t->img_n ) return 0;
+    const int ix = ( int ) fx, iy = ( int ) fy;
+    const long pix = ( ( long ) iy * t->img_n + ix ) * 4;
     tadd( t->image, pix + 0, I, t->fx_scale );
     tadd( t->image, pix + 1, Q, t->fx_scale );
     tadd( t->image, pix + 2, U, t->fx_scale );
     tadd( t->image, pix + 3, V, t->fx_scale );
+    const int batch = ( int ) ( pid % t->n_batch );
+    const long bp = ( ( ( long ) batch * t->img_bn + iy * t->img_bn / t->img_n ) * t->img_bn
+                      + ix * t->img_bn / t->img_n ) * 4;
+    tadd( t->img_batch, bp + 0, I, t->fx_scale );
+    tadd( t->img_batch, bp + 1, Q, t->fx_scale );
+    tadd( t->img_batch, bp + 2, U, t->fx_scale );
+    tadd( t->img_batch, bp + 3, V, t->fx_scale );
+    return 1;
 }
 
-static void ttally_escape( const tctx * t, const tpk * p )
+static int ttally_escape( const tctx * t, const tpk * p )
 {
-    if( t->n_mu <= 0 ) return;
+    if( t->n_mu <= 0 ) return 0;
     const float fb = floorf( ( p->d.z - t->mu_lo ) * t->mu_inv_w );
-    if( !( fb >= 0.0f && fb < ( float ) t->n_mu ) ) return;
+    if( !( fb >= 0.0f && fb < ( float ) t->n_mu ) ) return 0;
     const int bin = ( int ) fb;
     const om_v3 e2 = om_cross( p->d, p->e1 );
     float c2, s2;
@@ -354,6 +360,7 @@ static void ttally_escape( const tctx * t, const tpk * p )
     tadd( t->mu, i + 1, p->w * q, t->fx_scale );
     tadd( t->mu, i + 2, p->w * u, t->fx_scale );
     tadd( t->mu, i + 3, p->w * p->S.v, t->fx_scale );
+    return 1;
 }
 
 static float tsample_tau( om_rng * g )
@@ -479,13 +486,14 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
     t.tau_cut = c->tau_peel_max > 0 ? c->tau_peel_max : 40.0f;
     t.fx_scale = ldexp( 1.0, c->fx_shift );
     t.n_batch = c->n_batches;
+    t.img_bn = c->image_batch_n >= 1 ? c->image_batch_n : 1;
     t.w_min = c->w_min;
     t.rr_survive = c->rr_survive > 0 ? c->rr_survive : 0.1f;
     t.max_scatter = c->max_scatter;
     t.max_steps = c->max_steps;
     t.mu = mu; t.image = image; t.img_batch = img_batch;
 
-    unsigned long long cnt[ 8 ] = { 0, 0, 0, 0, 0, 0, 0, 0 };
+    unsigned long long cnt[ 10 ] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
     for( long long k = 0; k < c->n_packets; ++ k )
     {
         tpk p;
@@ -494,11 +502,11 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
         const kpo_source_t * s = c->sources + p.pid % c->n_sources;
         if( t.img_n > 0 && s->kind == 0 && s->emit == 0 )
         {
-            const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ] );
+            const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
             if( tau <= t.tau_cut )
             {
                 const float I = 0x1.45f306p-4f * ( float ) om_exp_neg( -( double ) tau );
-                tdeposit_image( & t, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
+                cnt[ 9 ] += tdeposit_image( & t, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
             }
         }
         p.tau = tsample_tau( & p.rng );
@@ -525,14 +533,14 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
                 p.w = p.w * ( ss / ext );
                 if( t.img_n > 0 )
                 {
-                    const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ] );
+                    const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
                     if( tau <= t.tau_cut )
                     {
                         float Q, U, V;
                         const float I = om_peel_stokes( t.ph, p.d, p.e1, p.S, t.o, t.ev, t.eh,
                                                         & Q, & U, & V );
                         const float att = p.w * ( float ) om_exp_neg( -( double ) tau );
-                        tdeposit_image( & t, p.x, p.pid, att * I, att * Q, att * U, att * V );
+                        cnt[ 9 ] += tdeposit_image( & t, p.x, p.pid, att * I, att * Q, att * U, att * V );
                     }
                 }
                 if( p.n_scat >= t.max_scatter )
@@ -556,11 +564,14 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
                 for( int a = 0; a < 3; ++ a )
                     if( a != ax ) p.x[ a ] = fma( tt, ( double ) om_comp( p.d, a ), p.x[ a ] );
                 int lost;
+                const int b_old = p.b;
                 if( ! tcross( & t, & p.b, p.c, p.x, ax, om_comp( p.d, ax ) > 0.0f, & lost ) )
                 {
                     if( lost ) end = ST_LOST;
-                    else { end = ST_ESCAPED; ttally_escape( & t, & p ); }
+                    else { end = ST_ESCAPED; cnt[ 9 ] += ttally_escape( & t, & p ); }
                 }
+                else
+                    cnt[ 8 ] += p.b != b_old;
             }
             if( ! end && p.n_steps >= t.max_steps ) end = ST_STEP_CAP;
             if( end )
@@ -575,7 +586,7 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
         }
     }
     if( counters )
-        for( int k = 0; k < 8; ++ k ) counters[ k ] += cnt[ k ];
+        for( int k = 0; k < 10; ++ k ) counters[ k ] += cnt[ k ];
     free( t.inv_dx );
     return 0;
 }

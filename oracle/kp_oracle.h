@@ -86,6 +86,7 @@ typedef struct kpo_cfg
     float     tau_peel_max;
     int       fx_shift;
     int       n_batches;
+    int       image_batch_n;
     float     w_min, rr_survive;
     int       max_scatter;
     long long max_steps;

@@ -127,7 +127,8 @@ class _Cfg(ctypes.Structure):
                 ("inclination_deg", ctypes.c_double), ("azimuth_deg", ctypes.c_double),
                 ("image_center", ctypes.c_double * 3), ("image_half_width", ctypes.c_double),
                 ("tau_peel_max", ctypes.c_float), ("fx_shift", ctypes.c_int),
-                ("n_batches", ctypes.c_int), ("w_min", ctypes.c_float), ("rr_survive", ctypes.c_float),
+                ("n_batches", ctypes.c_int), ("image_batch_n", ctypes.c_int),
+                ("w_min", ctypes.c_float), ("rr_survive", ctypes.c_float),
                 ("max_scatter", ctypes.c_int), ("max_steps", ctypes.c_longlong),
                 ("n_record", ctypes.c_longlong)]
 
@@ -171,8 +172,9 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
     ni = max(cfg.image_n, 1)
     out = dict(mu=np.zeros((cfg.n_batches, nm, 4), np.int64),
                image=np.zeros((ni, ni, 4), np.int64),
-               image_batch=np.zeros((cfg.n_batches, 4), np.int64),
-               counters=np.zeros(8, np.uint64))
+               image_batch=np.zeros((cfg.n_batches, max(cfg.image_batch_n, 1),
+                                     max(cfg.image_batch_n, 1), 4), np.int64),
+               counters=np.zeros(10, np.uint64))
     from kratos_polrad_b200.transport import RECORD_DTYPE
     rec = np.zeros(max(cfg.n_record, 1), RECORD_DTYPE)
     sigma2 = np.ascontiguousarray(sigma2, np.float32)

@@ -4,6 +4,8 @@ Per-packet final states (position, direction, Stokes, weight, cell, block,
 interaction and step counts, RNG draws), int64 escape tallies, peel-off
 images, batch sums and counters must be identical.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -54,11 +56,10 @@ def test_float_tally_mode_close_to_fixed():
     mesh, sig, t = case("amr_point")
     mesh.set_sigma(sig)
     fx = forward(mesh, t)
-    t.tally_mode = TALLY_FLOAT
-    t.n_record = 0
-    fl = forward(mesh, t)
+    tf = dataclasses.replace(t, tally_mode=TALLY_FLOAT, n_record=0)
+    fl = forward(mesh, tf)
     torch.cuda.synchronize()
-    img_fx = fx.image.cpu().numpy() * fx.scale()
+    img_fx = fx.image.cpu().numpy() * 2.0 ** -t.fx_shift
     img_fl = fl.image.cpu().numpy().astype(np.float64)
     # float atomics: reordering error <= n_terms * eps * sum|terms| per pixel;
     # with int64 rounding 2^-32 per term the two agree to 1e-5 of the peak.

@@ -38,7 +38,7 @@ def case(name):
         sig = np.stack([ext * alb, ext * (1 - alb)], 1).astype(np.float32)
         t = TransportConfig(n_packets=2000, sources=[Source(SOURCE_POINT, EMIT_ISOTROPIC, (0.5, 0.5, 0.5))],
                             seed=2, image_n=32, inclination_deg=60.0, image_center=(0.5, 0.5, 0.5),
-                            image_half_width=0.87, w_min=0.05, n_mu_bins=8, mu_lo=-1, mu_hi=1,
+                            image_half_width=0.87, w_min=0.05, image_batch_n=4, n_mu_bins=8, mu_lo=-1, mu_hi=1,
                             n_record=2000)
     elif name == "hg_multi":
         mesh = Mesh(AMR_PERIODIC)
