@@ -17,13 +17,35 @@ namespace
 {
 namespace cg = cooperative_groups;
 
+// Per-thread event counts (32-bit: a thread walks far fewer than 2^32
+// segments in one launch), flushed once at exit.
+struct counts32_t
+{
+    unsigned steps = 0, peel = 0, scat = 0, esc = 0, absb = 0, cap = 0, lost = 0,
+             emit = 0, hops = 0, dep = 0;
+};
+
+// Each thread runs a small state machine.  Every loop iteration advances the
+// thread's active ray by exactly one cell segment, whether that ray is the
+// packet's own walk or a peel-off ray toward the observer, so that the lanes
+// of a warp execute the same segment code together.  A peel-off ray starts
+// at an emission or interaction point: the walk position is parked, the ray
+// marches to the boundary (or beyond tau_cut), its contribution is
+// deposited, and the walk resumes.  Peel-off rays draw no random numbers, so
+// each packet's history equals a sequential walk that marches every peel-off
+// ray at the moment of its interaction.
 template< int TALLY >
-__global__ void __launch_bounds__( 256 )
+__global__ void __launch_bounds__( 256, 2 )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
-    local_counts_t cnt;
+    counts32_t cnt;
     packet_t p;
-    bool alive = false;
+    bool alive = false, peel = false;
+    double wx0 = 0, wx1 = 0, wx2 = 0;            // parked walk position
+    int wc0 = 0, wc1 = 0, wc2 = 0, wb = 0;
+    float pw = 0, pI = 0, pQ = 0, pU = 0, pV = 0, ptau = 0;   // pending peel-off
+    int ppix = 0, pk = 0, pend = 0;
+
     for( ;; )
     {
         if( ! alive )
@@ -45,55 +67,103 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             ++ cnt.emit;
+            p.tau = sample_tau( p.rng );
+            alive = true;
             const src_dev_t & s = P.src[ p.pid % P.n_src ];
             if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
             {   // direct light of an isotropic, unpolarized point source
-                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel, cnt.hops );
-                if( tau <= P.tau_cut )
+                const int pix = image_pixel( P, p.x );
+                if( pix >= 0 )
                 {
-                    const float I = __fmul_rn( 0x1.45f306p-4f,   // 1 / (4 pi)
-                                               ( float ) phys::kp_exp_neg( -( double ) tau ) );
-                    cnt.dep += deposit_image< TALLY >( P, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
+                    pw = 1.0f; pI = 0x1.45f306p-4f;             // 1 / (4 pi)
+                    pQ = pU = pV = 0.0f;
+                    ppix = pix; pend = 0; ptau = 0.0f; pk = 0;
+                    wx0 = p.x[ 0 ]; wx1 = p.x[ 1 ]; wx2 = p.x[ 2 ];
+                    wc0 = p.c[ 0 ]; wc1 = p.c[ 1 ]; wc2 = p.c[ 2 ]; wb = p.b;
+                    peel = true;
                 }
             }
-            p.tau = sample_tau( p.rng );
-            alive = true;
             continue;
         }
 
-        // One segment: to the exit face of the current cell or to the
-        // interaction point inside it.
+        // ---- one segment of the active ray ----
         const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
         const float ext = __fadd_rn( sg.x, sg.y );
+        const phys::v3 dd = peel ? P.o : p.d;
+        const double inv[ 3 ] = { peel ? P.inv_o[ 0 ] : p.inv[ 0 ],
+                                  peel ? P.inv_o[ 1 ] : p.inv[ 1 ],
+                                  peel ? P.inv_o[ 2 ] : p.inv[ 2 ] };
         int ax;
-        const double t = exit_dist( P.m, p.b, p.c, p.x, p.d, p.inv, ax );
-        const float dtau = __fmul_rn( ext, ( float ) t );
+        const double t = exit_dist( P.m, p.b, p.c, p.x, dd, inv, ax );
+        const float et = __fmul_rn( ext, ( float ) t );
+
+        if( peel )
+        {
+            ++ cnt.peel;
+            ++ pk;
+            ptau = __fadd_rn( ptau, et );
+            bool done = ptau > P.tau_cut;
+            if( ! done )
+            {
+                #pragma unroll
+                for( int a = 0; a < 3; ++ a )
+                    if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
+                bool lost;
+                const int b_old = p.b;
+                if( ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost ) )
+                    done = true;
+                else
+                    cnt.hops += p.b != b_old;
+                done = done || pk >= ( 1 << 20 );
+            }
+            if( done )
+            {
+                if( ptau <= P.tau_cut )
+                {
+                    const float att = __fmul_rn( pw, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    deposit_pixel< TALLY >( P, ppix, p.pid, __fmul_rn( att, pI ),
+                                            __fmul_rn( att, pQ ), __fmul_rn( att, pU ),
+                                            __fmul_rn( att, pV ) );
+                    ++ cnt.dep;
+                }
+                p.x[ 0 ] = wx0; p.x[ 1 ] = wx1; p.x[ 2 ] = wx2;
+                p.c[ 0 ] = wc0; p.c[ 1 ] = wc1; p.c[ 2 ] = wc2; p.b = wb;
+                peel = false;
+                if( pend )
+                {
+                    write_record( P, p, pend );
+                    cnt.absb += pend == PK_ABSORBED;
+                    cnt.cap  += pend == PK_SCATTER_CAP || pend == PK_STEP_CAP;
+                    alive = false;
+                }
+            }
+            continue;
+        }
+
+        // walk segment: to the exit face or to the interaction point
         ++ cnt.steps;
         ++ p.n_steps;
         int end = 0;
-        if( dtau >= p.tau )
+        if( et >= p.tau )
         {
             double ti = ( double ) __fdiv_rn( p.tau, ext );
             ti = ti > t ? t : ti;
             p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
             p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
             p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
-            // interaction: survival weighting by the albedo
             ++ p.n_scat;
             ++ cnt.scat;
-            p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, ext ) );
+            p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, ext ) );   // survival weighting
+            bool do_peel = false;
             if( P.img_n > 0 )
             {
-                const float tau = peel_tau( P, p.b, p.c, p.x, cnt.peel, cnt.hops );
-                if( tau <= P.tau_cut )
+                const int pix = image_pixel( P, p.x );
+                if( pix >= 0 )
                 {
-                    float Q, U, V;
-                    const float I = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh,
-                                                       Q, U, V );
-                    const float att = __fmul_rn( p.w, ( float ) phys::kp_exp_neg( -( double ) tau ) );
-                    cnt.dep += deposit_image< TALLY >( P, p.x, p.pid, __fmul_rn( att, I ),
-                                            __fmul_rn( att, Q ), __fmul_rn( att, U ),
-                                            __fmul_rn( att, V ) );
+                    pI = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh, pQ, pU, pV );
+                    pw = p.w;
+                    ppix = pix;
+                    do_peel = true;
                 }
             }
             if( p.n_scat >= P.max_scatter )
@@ -112,10 +182,20 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 set_inv( p );
                 p.tau = sample_tau( p.rng );
             }
+            if( ! end && p.n_steps >= P.max_steps )
+                end = PK_STEP_CAP;
+            if( do_peel )
+            {
+                wx0 = p.x[ 0 ]; wx1 = p.x[ 1 ]; wx2 = p.x[ 2 ];
+                wc0 = p.c[ 0 ]; wc1 = p.c[ 1 ]; wc2 = p.c[ 2 ]; wb = p.b;
+                ptau = 0.0f; pk = 0; pend = end;
+                peel = true;
+                continue;
+            }
         }
         else
         {
-            p.tau = __fsub_rn( p.tau, dtau );
+            p.tau = __fsub_rn( p.tau, et );
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
                 if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
@@ -133,9 +213,9 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             else
                 cnt.hops += p.b != b_old;
+            if( ! end && p.n_steps >= P.max_steps )
+                end = PK_STEP_CAP;
         }
-        if( ! end && p.n_steps >= P.max_steps )
-            end = PK_STEP_CAP;
         if( end )
         {
             write_record( P, p, end );
@@ -148,16 +228,16 @@ k_forward( const __grid_constant__ fwd_params_t P )
     }
     if( P.counters )
     {
-        atomicAdd( P.counters + KP_CNT_STEPS,      cnt.steps );
-        atomicAdd( P.counters + KP_CNT_PEEL_STEPS, cnt.peel );
-        atomicAdd( P.counters + KP_CNT_SCATTER,    cnt.scat );
-        atomicAdd( P.counters + KP_CNT_ESCAPED,    cnt.esc );
-        atomicAdd( P.counters + KP_CNT_ABSORBED,   cnt.absb );
-        atomicAdd( P.counters + KP_CNT_CAPPED,     cnt.cap );
-        atomicAdd( P.counters + KP_CNT_LOST,       cnt.lost );
-        atomicAdd( P.counters + KP_CNT_EMITTED,    cnt.emit );
-        atomicAdd( P.counters + KP_CNT_HOPS,       cnt.hops );
-        atomicAdd( P.counters + KP_CNT_DEPOSITS,   cnt.dep );
+        atomicAdd( P.counters + KP_CNT_STEPS,      ( unsigned long long ) cnt.steps );
+        atomicAdd( P.counters + KP_CNT_PEEL_STEPS, ( unsigned long long ) cnt.peel );
+        atomicAdd( P.counters + KP_CNT_SCATTER,    ( unsigned long long ) cnt.scat );
+        atomicAdd( P.counters + KP_CNT_ESCAPED,    ( unsigned long long ) cnt.esc );
+        atomicAdd( P.counters + KP_CNT_ABSORBED,   ( unsigned long long ) cnt.absb );
+        atomicAdd( P.counters + KP_CNT_CAPPED,     ( unsigned long long ) cnt.cap );
+        atomicAdd( P.counters + KP_CNT_LOST,       ( unsigned long long ) cnt.lost );
+        atomicAdd( P.counters + KP_CNT_EMITTED,    ( unsigned long long ) cnt.emit );
+        atomicAdd( P.counters + KP_CNT_HOPS,       ( unsigned long long ) cnt.hops );
+        atomicAdd( P.counters + KP_CNT_DEPOSITS,   ( unsigned long long ) cnt.dep );
     }
 }
 

@@ -234,11 +234,8 @@ __device__ __forceinline__ void add_tally( void * base, size_t i, float v, doubl
         atomicAdd( ( float * ) base + i, v );
 }
 
-// Adds a peel-off contribution (intensity per steradian I and image-frame
-// Q, U, V, already weighted) to the pixel under x.
-template< int TALLY >
-__device__ __forceinline__ bool deposit_image( const fwd_params_t & P, const double x[ 3 ],
-                                               long long pid, float I, float Q, float U, float V )
+// Image pixel (iy * n + ix) under position x, or -1 outside the image.
+__device__ __forceinline__ int image_pixel( const fwd_params_t & P, const double x[ 3 ] )
 {
     double r[ 3 ];
     #pragma unroll
@@ -253,9 +250,19 @@ __device__ __forceinline__ bool deposit_image( const fwd_params_t & P, const dou
     const double fx = floor( __fma_rn( hp, P.img_inv_pix, half ) );
     const double fy = floor( __fma_rn( vp, P.img_inv_pix, half ) );
     if( fx < 0.0 || fy < 0.0 || fx >= P.img_n || fy >= P.img_n )
-        return false;
-    const int ix = ( int ) fx, iy = ( int ) fy;
-    const size_t pix = ( ( size_t ) iy * P.img_n + ix ) * 4;
+        return -1;
+    return ( int ) fy * P.img_n + ( int ) fx;
+}
+
+// Adds a peel-off contribution (intensity per steradian I and image-frame
+// Q, U, V, already weighted) to image pixel `pix` (>= 0) and to the packet's
+// batch image.
+template< int TALLY >
+__device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel,
+                                               long long pid, float I, float Q, float U, float V )
+{
+    const int ix = pixel % P.img_n, iy = pixel / P.img_n;
+    const size_t pix = ( size_t ) pixel * 4;
     add_tally< TALLY >( P.image, pix + 0, I, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 1, Q, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 2, U, P.fx_scale );
@@ -267,7 +274,6 @@ __device__ __forceinline__ bool deposit_image( const fwd_params_t & P, const dou
     add_tally< TALLY >( P.img_batch, bp + 1, Q, P.fx_scale );
     add_tally< TALLY >( P.img_batch, bp + 2, U, P.fx_scale );
     add_tally< TALLY >( P.img_batch, bp + 3, V, P.fx_scale );
-    return true;
 }
 
 // Escape tally: mu = d.z bins, Stokes in the meridian frame (Q > 0 in the

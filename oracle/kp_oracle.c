@@ -316,8 +316,8 @@ static void tadd( long long * base, long i, float v, double sc )
     base[ i ] += llrint( ( double ) v * sc );
 }
 
-static int tdeposit_image( const tctx * t, const double * x, long long pid,
-                           float I, float Q, float U, float V )
+/* Image pixel (iy * n + ix) under x, or -1 outside the image. */
+static int timage_pixel( const tctx * t, const double * x )
 {
     double r[ 3 ];
     for( int a = 0; a < 3; ++ a ) r[ a ] = x[ a ] - t->img_c[ a ];
@@ -326,9 +326,15 @@ static int tdeposit_image( const tctx * t, const double * x, long long pid,
     const double half = 0.5 * t->img_n;
     const double fx = floor( fma( hp, t->img_inv_pix, half ) );
     const double fy = floor( fma( vp, t->img_inv_pix, half ) );
-    if( fx < 0.0 || fy < 0.0 || fx >= t->img_n || fy >= t->img_n ) return 0;
-    const int ix = ( int ) fx, iy = ( int ) fy;
-    const long pix = ( ( long ) iy * t->img_n + ix ) * 4;
+    if( fx < 0.0 || fy < 0.0 || fx >= t->img_n || fy >= t->img_n ) return -1;
+    return ( int ) fy * t->img_n + ( int ) fx;
+}
+
+static void tdeposit_pixel( const tctx * t, int pixel, long long pid,
+                            float I, float Q, float U, float V )
+{
+    const int ix = pixel % t->img_n, iy = pixel / t->img_n;
+    const long pix = ( long ) pixel * 4;
     tadd( t->image, pix + 0, I, t->fx_scale );
     tadd( t->image, pix + 1, Q, t->fx_scale );
     tadd( t->image, pix + 2, U, t->fx_scale );
@@ -340,7 +346,6 @@ static int tdeposit_image( const tctx * t, const double * x, long long pid,
     tadd( t->img_batch, bp + 1, Q, t->fx_scale );
     tadd( t->img_batch, bp + 2, U, t->fx_scale );
     tadd( t->img_batch, bp + 3, V, t->fx_scale );
-    return 1;
 }
 
 static int ttally_escape( const tctx * t, const tpk * p )
@@ -501,12 +506,18 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
         ++ cnt[ 7 ];
         const kpo_source_t * s = c->sources + p.pid % c->n_sources;
         if( t.img_n > 0 && s->kind == 0 && s->emit == 0 )
-        {
-            const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
-            if( tau <= t.tau_cut )
+        {   /* direct light: peel-off rays start only inside the image */
+            const int pix = timage_pixel( & t, p.x );
+            if( pix >= 0 )
             {
-                const float I = 0x1.45f306p-4f * ( float ) om_exp_neg( -( double ) tau );
-                cnt[ 9 ] += tdeposit_image( & t, p.x, p.pid, I, 0.0f, 0.0f, 0.0f );
+                const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
+                if( tau <= t.tau_cut )
+                {
+                    const float att = 1.0f * ( float ) om_exp_neg( -( double ) tau );
+                    tdeposit_pixel( & t, pix, p.pid, att * 0x1.45f306p-4f, att * 0.0f,
+                                    att * 0.0f, att * 0.0f );
+                    ++ cnt[ 9 ];
+                }
             }
         }
         p.tau = tsample_tau( & p.rng );
@@ -531,7 +542,8 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
                 ++ p.n_scat;
                 ++ cnt[ 2 ];
                 p.w = p.w * ( ss / ext );
-                if( t.img_n > 0 )
+                const int pix = t.img_n > 0 ? timage_pixel( & t, p.x ) : -1;
+                if( pix >= 0 )
                 {
                     const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
                     if( tau <= t.tau_cut )
@@ -540,7 +552,8 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
                         const float I = om_peel_stokes( t.ph, p.d, p.e1, p.S, t.o, t.ev, t.eh,
                                                         & Q, & U, & V );
                         const float att = p.w * ( float ) om_exp_neg( -( double ) tau );
-                        cnt[ 9 ] += tdeposit_image( & t, p.x, p.pid, att * I, att * Q, att * U, att * V );
+                        tdeposit_pixel( & t, pix, p.pid, att * I, att * Q, att * U, att * V );
+                        ++ cnt[ 9 ];
                     }
                 }
                 if( p.n_scat >= t.max_scatter )
