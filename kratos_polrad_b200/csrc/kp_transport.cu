@@ -25,42 +25,69 @@ struct counts32_t
              emit = 0, hops = 0, dep = 0;
 };
 
-// Each thread runs a small state machine.  Every loop iteration advances the
-// thread's active ray by exactly one cell segment, whether that ray is the
-// packet's own walk or a peel-off ray toward the observer, so that the lanes
-// of a warp execute the same segment code together.  A peel-off ray starts
-// at an emission or interaction point: the walk position is parked, the ray
-// marches to the boundary (or beyond tau_cut), its contribution is
-// deposited, and the walk resumes.  Peel-off rays draw no random numbers, so
-// each packet's history equals a sequential walk that marches every peel-off
-// ray at the moment of its interaction.
+// Lane phases of the forward kernel.
+enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3 };
+
+// Warp-synchronous scheduler.  Each lane carries one packet through a small
+// state machine: EMIT (needs a packet), SEGMENT (advance its active ray by
+// one cell segment: the packet's own walk, or a peel-off ray toward the
+// observer), EVENT (an interaction to process).  Every iteration the warp
+// ballots the lane phases and runs ONE phase for all lanes in it: events and
+// emissions, which are long and rare, wait until at least `ev_batch` lanes
+// need them (or no lane can step), so their code runs with many lanes
+// active; segments, which are short and frequent, run otherwise.  A peel-off
+// ray starts at an emission or interaction point: the walk position is
+// parked, the ray marches to the boundary (or beyond tau_cut), its
+// contribution is deposited and the walk resumes.  Peel-off rays draw no
+// random numbers, so each packet's history equals a sequential walk that
+// marches every peel-off ray at the moment of its interaction.
 template< int TALLY >
 __global__ void __launch_bounds__( 256, 2 )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
     counts32_t cnt;
     packet_t p;
-    bool alive = false, peel = false;
+    int  phase = PH_EMIT;
+    bool peel = false;
     double wx0 = 0, wx1 = 0, wx2 = 0;            // parked walk position
     int wc0 = 0, wc1 = 0, wc2 = 0, wb = 0;
     float pw = 0, pI = 0, pQ = 0, pU = 0, pV = 0, ptau = 0;   // pending peel-off
     int ppix = 0, pk = 0, pend = 0;
+    float ev_ext = 0.f, ev_sca = 0.f;             // coefficients at the interaction
 
     for( ;; )
     {
-        if( ! alive )
+        const unsigned m_emit = __ballot_sync( FULL, phase == PH_EMIT );
+        const unsigned m_seg  = __ballot_sync( FULL, phase == PH_SEGMENT );
+        const unsigned m_ev   = __ballot_sync( FULL, phase == PH_EVENT );
+        if( ( m_emit | m_seg | m_ev ) == 0u )
+            break;
+        const int n_seg = __popc( m_seg ), n_ev = __popc( m_ev ), n_emit = __popc( m_emit );
+        int run;
+        if( n_ev > 0 && ( n_ev >= P.ev_batch || n_seg == 0 ) )
+            run = PH_EVENT;
+        else if( n_emit > 0 && ( n_emit >= P.ev_batch || n_seg == 0 ) )
+            run = PH_EMIT;
+        else
+            run = PH_SEGMENT;
+
+        if( run == PH_EMIT )
         {
-            unsigned long long idx;
-            {
-                cg::coalesced_group g = cg::coalesced_threads(  );
-                unsigned long long base = 0;
-                if( g.thread_rank(  ) == 0 )
-                    base = atomicAdd( P.work, ( unsigned long long ) g.size(  ) );
-                base = g.shfl( base, 0 );
-                idx  = base + g.thread_rank(  );
-            }
+            if( phase != PH_EMIT ) continue;
+            const int leader = __ffs( m_emit ) - 1;
+            const unsigned rank = __popc( m_emit & ( ( 1u << lane ) - 1u ) );
+            unsigned long long base = 0;
+            if( ( int ) lane == leader )
+                base = atomicAdd( P.work, ( unsigned long long ) n_emit );
+            base = __shfl_sync( m_emit, base, leader );
+            const unsigned long long idx = base + rank;
             if( idx >= ( unsigned long long ) P.n_packets )
-                break;
+            {
+                phase = PH_DONE;
+                continue;
+            }
             if( ! emit_packet( P, P.pid0 + ( long long ) idx, p ) )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
@@ -68,7 +95,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             ++ cnt.emit;
             p.tau = sample_tau( p.rng );
-            alive = true;
+            phase = PH_SEGMENT;
             const src_dev_t & s = P.src[ p.pid % P.n_src ];
             if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
             {   // direct light of an isotropic, unpolarized point source
@@ -86,74 +113,13 @@ k_forward( const __grid_constant__ fwd_params_t P )
             continue;
         }
 
-        // ---- one segment of the active ray ----
-        const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
-        const float ext = __fadd_rn( sg.x, sg.y );
-        const phys::v3 dd = peel ? P.o : p.d;
-        const double inv[ 3 ] = { peel ? P.inv_o[ 0 ] : p.inv[ 0 ],
-                                  peel ? P.inv_o[ 1 ] : p.inv[ 1 ],
-                                  peel ? P.inv_o[ 2 ] : p.inv[ 2 ] };
-        int ax;
-        const double t = exit_dist( P.m, p.b, p.c, p.x, dd, inv, ax );
-        const float et = __fmul_rn( ext, ( float ) t );
-
-        if( peel )
+        if( run == PH_EVENT )
         {
-            ++ cnt.peel;
-            ++ pk;
-            ptau = __fadd_rn( ptau, et );
-            bool done = ptau > P.tau_cut;
-            if( ! done )
-            {
-                #pragma unroll
-                for( int a = 0; a < 3; ++ a )
-                    if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
-                bool lost;
-                const int b_old = p.b;
-                if( ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost ) )
-                    done = true;
-                else
-                    cnt.hops += p.b != b_old;
-                done = done || pk >= ( 1 << 20 );
-            }
-            if( done )
-            {
-                if( ptau <= P.tau_cut )
-                {
-                    const float att = __fmul_rn( pw, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                    deposit_pixel< TALLY >( P, ppix, p.pid, __fmul_rn( att, pI ),
-                                            __fmul_rn( att, pQ ), __fmul_rn( att, pU ),
-                                            __fmul_rn( att, pV ) );
-                    ++ cnt.dep;
-                }
-                p.x[ 0 ] = wx0; p.x[ 1 ] = wx1; p.x[ 2 ] = wx2;
-                p.c[ 0 ] = wc0; p.c[ 1 ] = wc1; p.c[ 2 ] = wc2; p.b = wb;
-                peel = false;
-                if( pend )
-                {
-                    write_record( P, p, pend );
-                    cnt.absb += pend == PK_ABSORBED;
-                    cnt.cap  += pend == PK_SCATTER_CAP || pend == PK_STEP_CAP;
-                    alive = false;
-                }
-            }
-            continue;
-        }
-
-        // walk segment: to the exit face or to the interaction point
-        ++ cnt.steps;
-        ++ p.n_steps;
-        int end = 0;
-        if( et >= p.tau )
-        {
-            double ti = ( double ) __fdiv_rn( p.tau, ext );
-            ti = ti > t ? t : ti;
-            p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
-            p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
-            p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
+            if( phase != PH_EVENT ) continue;
+            // interaction at p.x (already moved there by its segment)
             ++ p.n_scat;
             ++ cnt.scat;
-            p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, ext ) );   // survival weighting
+            p.w = __fmul_rn( p.w, __fdiv_rn( ev_sca, ev_ext ) );   // survival weighting
             bool do_peel = false;
             if( P.img_n > 0 )
             {
@@ -166,6 +132,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     do_peel = true;
                 }
             }
+            int end = 0;
             if( p.n_scat >= P.max_scatter )
                 end = PK_SCATTER_CAP;
             else if( p.w < P.w_min )
@@ -190,40 +157,113 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 wc0 = p.c[ 0 ]; wc1 = p.c[ 1 ]; wc2 = p.c[ 2 ]; wb = p.b;
                 ptau = 0.0f; pk = 0; pend = end;
                 peel = true;
-                continue;
+                phase = PH_SEGMENT;
             }
+            else if( end )
+            {
+                write_record( P, p, end );
+                cnt.absb += end == PK_ABSORBED;
+                cnt.cap  += end == PK_SCATTER_CAP || end == PK_STEP_CAP;
+                phase = PH_EMIT;
+            }
+            else
+                phase = PH_SEGMENT;
+            continue;
+        }
+
+        // ---- PH_SEGMENT: one segment of the active ray ----
+        if( phase != PH_SEGMENT ) continue;
+        const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
+        const float ext = __fadd_rn( sg.x, sg.y );
+        const phys::v3 dd = peel ? P.o : p.d;
+        const double inv[ 3 ] = { peel ? P.inv_o[ 0 ] : p.inv[ 0 ],
+                                  peel ? P.inv_o[ 1 ] : p.inv[ 1 ],
+                                  peel ? P.inv_o[ 2 ] : p.inv[ 2 ] };
+        int ax;
+        const double t = exit_dist( P.m, p.b, p.c, p.x, dd, inv, ax );
+        const float et = __fmul_rn( ext, ( float ) t );
+        bool interact = false, peel_cut = false;
+        if( peel )
+        {
+            ++ cnt.peel;
+            ++ pk;
+            ptau = __fadd_rn( ptau, et );
+            peel_cut = ptau > P.tau_cut;
         }
         else
         {
-            p.tau = __fsub_rn( p.tau, et );
+            ++ cnt.steps;
+            ++ p.n_steps;
+            interact = et >= p.tau;
+        }
+        bool left = false, lost = false;
+        if( interact )
+        {
+            double ti = ( double ) __fdiv_rn( p.tau, ext );
+            ti = ti > t ? t : ti;
+            p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
+            p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
+            p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
+            ev_ext = ext;
+            ev_sca = sg.x;
+            phase = PH_EVENT;
+            continue;
+        }
+        if( ! peel_cut )
+        {   // advance to the exit face and into the next cell (shared code)
+            if( ! peel ) p.tau = __fsub_rn( p.tau, et );
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
-                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
-            bool lost;
+                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
             const int b_old = p.b;
-            if( ! cross_face( P.m, p.b, p.c, p.x, ax, comp( p.d, ax ) > 0.0f, lost ) )
+            left = ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost );
+            if( ! left ) cnt.hops += p.b != b_old;
+        }
+        if( peel )
+        {
+            if( peel_cut || left || pk >= ( 1 << 20 ) )
             {
-                if( lost )
-                    end = PK_LOST;
-                else
+                if( ptau <= P.tau_cut )
                 {
-                    end = PK_ESCAPED;
-                    cnt.dep += tally_escape< TALLY >( P, p );
+                    const float att = __fmul_rn( pw, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    deposit_pixel< TALLY >( P, ppix, p.pid, __fmul_rn( att, pI ),
+                                            __fmul_rn( att, pQ ), __fmul_rn( att, pU ),
+                                            __fmul_rn( att, pV ) );
+                    ++ cnt.dep;
+                }
+                p.x[ 0 ] = wx0; p.x[ 1 ] = wx1; p.x[ 2 ] = wx2;
+                p.c[ 0 ] = wc0; p.c[ 1 ] = wc1; p.c[ 2 ] = wc2; p.b = wb;
+                peel = false;
+                if( pend )
+                {
+                    write_record( P, p, pend );
+                    cnt.absb += pend == PK_ABSORBED;
+                    cnt.cap  += pend == PK_SCATTER_CAP || pend == PK_STEP_CAP;
+                    phase = PH_EMIT;
                 }
             }
-            else
-                cnt.hops += p.b != b_old;
-            if( ! end && p.n_steps >= P.max_steps )
-                end = PK_STEP_CAP;
+            continue;
         }
+        int end = 0;
+        if( left )
+        {
+            if( lost )
+                end = PK_LOST;
+            else
+            {
+                end = PK_ESCAPED;
+                cnt.dep += tally_escape< TALLY >( P, p );
+            }
+        }
+        else if( p.n_steps >= P.max_steps )
+            end = PK_STEP_CAP;
         if( end )
         {
             write_record( P, p, end );
             cnt.esc  += end == PK_ESCAPED;
-            cnt.absb += end == PK_ABSORBED;
-            cnt.cap  += end == PK_SCATTER_CAP || end == PK_STEP_CAP;
+            cnt.cap  += end == PK_STEP_CAP;
             cnt.lost += end == PK_LOST;
-            alive = false;
+            phase = PH_EMIT;
         }
     }
     if( P.counters )
@@ -328,6 +368,8 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
     P.rr_survive = c.rr_survive > 0 ? c.rr_survive : 0.1f;
     P.max_scatter = c.max_scatter;
     P.max_steps = c.max_steps;
+    require( c.lane_batch >= 0 && c.lane_batch <= 32, "lane_batch must be in 0..32" );
+    P.ev_batch = c.lane_batch > 0 ? c.lane_batch : 12;
     P.mu_tally = t.mu;
     P.image = t.image;
     P.img_batch = t.image_batch;
@@ -354,6 +396,7 @@ void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s )
     long long grid = persistent_grid( k, threads );
     grid = std::min< long long >( grid, ( P.n_packets + threads - 1 ) / threads );
     KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
+    // whole warps only: the scheduler ballots over full warps
     if( tally_mode == KP_TALLY_FIXED )
         k_forward< KP_TALLY_FIXED ><<< ( unsigned ) grid, threads, 0, s >>>( P );
     else

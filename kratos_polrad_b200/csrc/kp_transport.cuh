@@ -54,6 +54,7 @@ struct fwd_params_t
     float       w_min, rr_survive;
     int         max_scatter;
     long long   max_steps;
+    int         ev_batch;          // lanes that must wait for an event batch
     double      lk_inv[ 3 ];       // lookup cells per unit length
     void      * mu_tally;
     void      * image;

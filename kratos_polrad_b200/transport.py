@@ -45,7 +45,8 @@ class CTransportCfg(ctypes.Structure):
                 ("tau_peel_max", c_float), ("tally_mode", c_int), ("fx_shift", c_int),
                 ("n_batches", c_int), ("image_batch_n", c_int), ("w_min", c_float),
                 ("rr_survive", c_float),
-                ("max_scatter", c_int), ("max_steps", c_ll), ("n_record", c_ll)]
+                ("max_scatter", c_int), ("max_steps", c_ll), ("n_record", c_ll),
+                ("lane_batch", c_int)]
 
 
 class CTallies(ctypes.Structure):
@@ -99,6 +100,7 @@ class TransportConfig:
     max_scatter: int = 100000
     max_steps: int = 1 << 24
     n_record: int = 0
+    lane_batch: int = 0
 
     def to_c(self):
         src = (CSource * max(1, len(self.sources)))()
