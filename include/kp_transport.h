@@ -241,7 +241,7 @@ typedef struct kp_transport_cfg
     long long max_steps;       /* segments per packet before it is ended       */
     long long n_record;        /* final-state records for the first n packets  */
     int       lane_batch;      /* scheduling: lanes of a warp that wait for an
-                                  interaction or emission batch (0: default 12) */
+                                  interaction or emission batch (0: default 6)  */
 } kp_transport_cfg_t;
 
 typedef struct kp_packet_record

@@ -17,13 +17,47 @@ namespace
 {
 namespace cg = cooperative_groups;
 
-// Per-thread event counts (32-bit: a thread walks far fewer than 2^32
-// segments in one launch), flushed once at exit.
+// Segment counts stay in registers (32-bit: a thread walks far fewer than
+// 2^32 segments in one launch); rare events are counted in shared memory.
 struct counts32_t
 {
-    unsigned steps = 0, peel = 0, scat = 0, esc = 0, absb = 0, cap = 0, lost = 0,
-             emit = 0, hops = 0, dep = 0;
+    unsigned steps = 0, peel = 0;
 };
+
+constexpr int FWD_THREADS = 256;
+
+// Rarely touched per-lane state kept in shared memory (structure of arrays):
+// the parked walk position while a peel-off ray runs, and the pending
+// peel-off contribution.
+struct park_t
+{
+    double x[ 3 ][ FWD_THREADS ];
+    int    c[ 3 ][ FWD_THREADS ];
+    int    b[ FWD_THREADS ];
+    float  w[ FWD_THREADS ], I[ FWD_THREADS ], Q[ FWD_THREADS ], U[ FWD_THREADS ],
+           V[ FWD_THREADS ];
+    int    pix[ FWD_THREADS ];
+    unsigned long long cnt[ KP_NCOUNTERS ];
+};
+
+__device__ __forceinline__ void park_walk( park_t & sp, const packet_t & p )
+{
+    const int t = threadIdx.x;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { sp.x[ a ][ t ] = p.x[ a ]; sp.c[ a ][ t ] = p.c[ a ]; }
+    sp.b[ t ] = p.b;
+}
+__device__ __forceinline__ void unpark_walk( const park_t & sp, packet_t & p )
+{
+    const int t = threadIdx.x;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { p.x[ a ] = sp.x[ a ][ t ]; p.c[ a ] = sp.c[ a ][ t ]; }
+    p.b = sp.b[ t ];
+}
+__device__ __forceinline__ void count( park_t & sp, int k, unsigned v = 1u )
+{
+    atomicAdd( sp.cnt + k, ( unsigned long long ) v );
+}
 
 // Lane phases of the forward kernel.
 enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3 };
@@ -42,20 +76,20 @@ enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3 };
 // random numbers, so each packet's history equals a sequential walk that
 // marches every peel-off ray at the moment of its interaction.
 template< int TALLY >
-__global__ void __launch_bounds__( 256, 2 )
+__global__ void __launch_bounds__( FWD_THREADS, 3 )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
+    __shared__ park_t sp;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
+    if( threadIdx.x < KP_NCOUNTERS ) sp.cnt[ threadIdx.x ] = 0;
+    __syncthreads(  );
     counts32_t cnt;
     packet_t p;
     int  phase = PH_EMIT;
     bool peel = false;
-    double wx0 = 0, wx1 = 0, wx2 = 0;            // parked walk position
-    int wc0 = 0, wc1 = 0, wc2 = 0, wb = 0;
-    float pw = 0, pI = 0, pQ = 0, pU = 0, pV = 0, ptau = 0;   // pending peel-off
-    int ppix = 0, pk = 0, pend = 0;
-    float ev_ext = 0.f, ev_sca = 0.f;             // coefficients at the interaction
+    float ptau = 0;
+    int pk = 0, pend = 0;
 
     for( ;; )
     {
@@ -93,20 +127,21 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 atomicOr( P.m.status, ST_BAD_SOURCE );
                 continue;
             }
-            ++ cnt.emit;
+            count( sp, KP_CNT_EMITTED );
             p.tau = sample_tau( p.rng );
             phase = PH_SEGMENT;
-            const src_dev_t & s = P.src[ p.pid % P.n_src ];
+            const src_dev_t & s = P.src[ p.pid(  ) % P.n_src ];
             if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
             {   // direct light of an isotropic, unpolarized point source
                 const int pix = image_pixel( P, p.x );
                 if( pix >= 0 )
                 {
-                    pw = 1.0f; pI = 0x1.45f306p-4f;             // 1 / (4 pi)
-                    pQ = pU = pV = 0.0f;
-                    ppix = pix; pend = 0; ptau = 0.0f; pk = 0;
-                    wx0 = p.x[ 0 ]; wx1 = p.x[ 1 ]; wx2 = p.x[ 2 ];
-                    wc0 = p.c[ 0 ]; wc1 = p.c[ 1 ]; wc2 = p.c[ 2 ]; wb = p.b;
+                    const int t = threadIdx.x;
+                    sp.w[ t ] = 1.0f; sp.I[ t ] = 0x1.45f306p-4f;     // 1 / (4 pi)
+                    sp.Q[ t ] = sp.U[ t ] = sp.V[ t ] = 0.0f;
+                    sp.pix[ t ] = pix;
+                    pend = 0; ptau = 0.0f; pk = 0;
+                    park_walk( sp, p );
                     peel = true;
                 }
             }
@@ -118,17 +153,23 @@ k_forward( const __grid_constant__ fwd_params_t P )
             if( phase != PH_EVENT ) continue;
             // interaction at p.x (already moved there by its segment)
             ++ p.n_scat;
-            ++ cnt.scat;
-            p.w = __fmul_rn( p.w, __fdiv_rn( ev_sca, ev_ext ) );   // survival weighting
+            count( sp, KP_CNT_SCATTER );
+            {
+                const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
+                p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, __fadd_rn( sg.x, sg.y ) ) );
+            }   // survival weighting by the albedo
             bool do_peel = false;
             if( P.img_n > 0 )
             {
                 const int pix = image_pixel( P, p.x );
                 if( pix >= 0 )
                 {
-                    pI = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh, pQ, pU, pV );
-                    pw = p.w;
-                    ppix = pix;
+                    const int t = threadIdx.x;
+                    float Q, U, V;
+                    sp.I[ t ] = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh, Q, U, V );
+                    sp.Q[ t ] = Q; sp.U[ t ] = U; sp.V[ t ] = V;
+                    sp.w[ t ] = p.w;
+                    sp.pix[ t ] = pix;
                     do_peel = true;
                 }
             }
@@ -153,8 +194,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 end = PK_STEP_CAP;
             if( do_peel )
             {
-                wx0 = p.x[ 0 ]; wx1 = p.x[ 1 ]; wx2 = p.x[ 2 ];
-                wc0 = p.c[ 0 ]; wc1 = p.c[ 1 ]; wc2 = p.c[ 2 ]; wb = p.b;
+                park_walk( sp, p );
                 ptau = 0.0f; pk = 0; pend = end;
                 peel = true;
                 phase = PH_SEGMENT;
@@ -162,8 +202,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             else if( end )
             {
                 write_record( P, p, end );
-                cnt.absb += end == PK_ABSORBED;
-                cnt.cap  += end == PK_SCATTER_CAP || end == PK_STEP_CAP;
+                count( sp, end == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
                 phase = PH_EMIT;
             }
             else
@@ -204,8 +243,6 @@ k_forward( const __grid_constant__ fwd_params_t P )
             p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
             p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
             p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
-            ev_ext = ext;
-            ev_sca = sg.x;
             phase = PH_EVENT;
             continue;
         }
@@ -217,7 +254,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
             const int b_old = p.b;
             left = ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost );
-            if( ! left ) cnt.hops += p.b != b_old;
+            if( ! left && p.b != b_old ) count( sp, KP_CNT_HOPS );
         }
         if( peel )
         {
@@ -225,20 +262,20 @@ k_forward( const __grid_constant__ fwd_params_t P )
             {
                 if( ptau <= P.tau_cut )
                 {
-                    const float att = __fmul_rn( pw, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                    deposit_pixel< TALLY >( P, ppix, p.pid, __fmul_rn( att, pI ),
-                                            __fmul_rn( att, pQ ), __fmul_rn( att, pU ),
-                                            __fmul_rn( att, pV ) );
-                    ++ cnt.dep;
+                    const int th = threadIdx.x;
+                    const float att = __fmul_rn( sp.w[ th ],
+                                                 ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    deposit_pixel< TALLY >( P, sp.pix[ th ], p.pid(  ), __fmul_rn( att, sp.I[ th ] ),
+                                            __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
+                                            __fmul_rn( att, sp.V[ th ] ) );
+                    count( sp, KP_CNT_DEPOSITS );
                 }
-                p.x[ 0 ] = wx0; p.x[ 1 ] = wx1; p.x[ 2 ] = wx2;
-                p.c[ 0 ] = wc0; p.c[ 1 ] = wc1; p.c[ 2 ] = wc2; p.b = wb;
+                unpark_walk( sp, p );
                 peel = false;
                 if( pend )
                 {
                     write_record( P, p, pend );
-                    cnt.absb += pend == PK_ABSORBED;
-                    cnt.cap  += pend == PK_SCATTER_CAP || pend == PK_STEP_CAP;
+                    count( sp, pend == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
                     phase = PH_EMIT;
                 }
             }
@@ -252,7 +289,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             else
             {
                 end = PK_ESCAPED;
-                cnt.dep += tally_escape< TALLY >( P, p );
+                if( tally_escape< TALLY >( P, p ) ) count( sp, KP_CNT_DEPOSITS );
             }
         }
         else if( p.n_steps >= P.max_steps )
@@ -260,25 +297,16 @@ k_forward( const __grid_constant__ fwd_params_t P )
         if( end )
         {
             write_record( P, p, end );
-            cnt.esc  += end == PK_ESCAPED;
-            cnt.cap  += end == PK_STEP_CAP;
-            cnt.lost += end == PK_LOST;
+            count( sp, end == PK_ESCAPED ? KP_CNT_ESCAPED
+                     : ( end == PK_LOST ? KP_CNT_LOST : KP_CNT_CAPPED ) );
             phase = PH_EMIT;
         }
     }
-    if( P.counters )
-    {
-        atomicAdd( P.counters + KP_CNT_STEPS,      ( unsigned long long ) cnt.steps );
-        atomicAdd( P.counters + KP_CNT_PEEL_STEPS, ( unsigned long long ) cnt.peel );
-        atomicAdd( P.counters + KP_CNT_SCATTER,    ( unsigned long long ) cnt.scat );
-        atomicAdd( P.counters + KP_CNT_ESCAPED,    ( unsigned long long ) cnt.esc );
-        atomicAdd( P.counters + KP_CNT_ABSORBED,   ( unsigned long long ) cnt.absb );
-        atomicAdd( P.counters + KP_CNT_CAPPED,     ( unsigned long long ) cnt.cap );
-        atomicAdd( P.counters + KP_CNT_LOST,       ( unsigned long long ) cnt.lost );
-        atomicAdd( P.counters + KP_CNT_EMITTED,    ( unsigned long long ) cnt.emit );
-        atomicAdd( P.counters + KP_CNT_HOPS,       ( unsigned long long ) cnt.hops );
-        atomicAdd( P.counters + KP_CNT_DEPOSITS,   ( unsigned long long ) cnt.dep );
-    }
+    count( sp, KP_CNT_STEPS, cnt.steps );
+    count( sp, KP_CNT_PEEL_STEPS, cnt.peel );
+    __syncthreads(  );
+    if( P.counters && threadIdx.x < KP_NCOUNTERS && sp.cnt[ threadIdx.x ] )
+        atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );
 }
 
 }   // namespace
@@ -367,9 +395,9 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
     P.w_min = c.w_min;
     P.rr_survive = c.rr_survive > 0 ? c.rr_survive : 0.1f;
     P.max_scatter = c.max_scatter;
-    P.max_steps = c.max_steps;
+    P.max_steps = std::min< long long >( c.max_steps, 0x7fffffff );
     require( c.lane_batch >= 0 && c.lane_batch <= 32, "lane_batch must be in 0..32" );
-    P.ev_batch = c.lane_batch > 0 ? c.lane_batch : 12;
+    P.ev_batch = c.lane_batch > 0 ? c.lane_batch : 6;
     P.mu_tally = t.mu;
     P.image = t.image;
     P.img_batch = t.image_batch;
@@ -390,7 +418,7 @@ int persistent_grid( const void * kernel, int threads )
 void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s )
 {
     if( P.n_packets == 0 ) return;
-    const int threads = 256;
+    const int threads = FWD_THREADS;
     const void * k = tally_mode == KP_TALLY_FIXED ? ( const void * ) k_forward< KP_TALLY_FIXED >
                                                   : ( const void * ) k_forward< KP_TALLY_FLOAT >;
     long long grid = persistent_grid( k, threads );

@@ -79,9 +79,12 @@ struct packet_t
     int           b;
     int           c[ 3 ];
     int           n_scat;
-    long long     n_steps;
-    long long     pid;
+    int           n_steps;
     phys::rng_t   rng;
+    __device__ __forceinline__ long long pid(  ) const
+    {
+        return ( long long ) ( ( ( unsigned long long ) rng.pid_hi << 32 ) | rng.pid_lo );
+    }
 };
 
 struct local_counts_t
@@ -291,7 +294,7 @@ __device__ __forceinline__ bool tally_escape( const fwd_params_t & P, const pack
     phys::double_angle( p.e1.z, e2.z, c2, s2 );
     float q = p.S.q, u = p.S.u;
     phys::rotate( q, u, c2, s2 );
-    const int batch = ( int ) ( p.pid % P.n_batch );
+    const int batch = ( int ) ( p.pid(  ) % P.n_batch );
     const size_t i = ( ( size_t ) batch * P.n_mu + bin ) * 4;
     add_tally< TALLY >( P.mu_tally, i + 0, p.w, P.fx_scale );
     add_tally< TALLY >( P.mu_tally, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
@@ -329,7 +332,6 @@ __device__ __forceinline__ phys::v3 sample_emission_dir( phys::rng_t & rng, int 
 // source position lies outside the mesh.
 __device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long pid, packet_t & p )
 {
-    p.pid = pid;
     p.rng = phys::rng_t { P.seed, P.stream, ( uint32_t ) pid, ( uint32_t ) ( pid >> 32 ), 0u };
     const src_dev_t & s = P.src[ pid % P.n_src ];
     if( s.kind == KP_SOURCE_POINT )
@@ -376,7 +378,7 @@ __device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long p
 
 __device__ __forceinline__ void write_record( const fwd_params_t & P, const packet_t & p, int status )
 {
-    const long long k = p.pid - P.pid0;
+    const long long k = p.pid(  ) - P.pid0;
     if( P.records == nullptr || k < 0 || k >= P.n_record ) return;
     kp_packet_record_t r;
     #pragma unroll
