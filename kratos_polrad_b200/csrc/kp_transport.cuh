@@ -143,7 +143,9 @@ __device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int 
                                             double x[ 3 ], int ax, bool pos, bool & lost )
 {
     lost = false;
-    int cn = c[ ax ] + ( pos ? 1 : -1 );
+    // select, not c[ ax ]: a runtime index would move c[] to local memory
+    const int cax = ax == 0 ? c[ 0 ] : ( ax == 1 ? c[ 1 ] : c[ 2 ] );
+    int cn = cax + ( pos ? 1 : -1 );
     const double * g = m.geo_d + 16 * ( size_t ) b;
     if( cn >= 0 && cn < m.nc[ ax ] )
     {
@@ -380,18 +382,17 @@ __device__ __forceinline__ void write_record( const fwd_params_t & P, const pack
 {
     const long long k = p.pid(  ) - P.pid0;
     if( P.records == nullptr || k < 0 || k >= P.n_record ) return;
-    kp_packet_record_t r;
+    kp_packet_record_t * r = P.records + k;       // field by field: no local copy
     #pragma unroll
-    for( int a = 0; a < 3; ++ a ) { r.x[ a ] = p.x[ a ]; r.cell[ a ] = p.c[ a ]; }
-    r.d[ 0 ] = p.d.x; r.d[ 1 ] = p.d.y; r.d[ 2 ] = p.d.z;
-    r.stokes[ 0 ] = p.S.q; r.stokes[ 1 ] = p.S.u; r.stokes[ 2 ] = p.S.v;
-    r.w = p.w;
-    r.ib = p.b;
-    r.n_scatter = p.n_scat;
-    r.status = status;
-    r.rng_draws = p.rng.draw;
-    r.n_steps = p.n_steps;
-    P.records[ k ] = r;
+    for( int a = 0; a < 3; ++ a ) { r->x[ a ] = p.x[ a ]; r->cell[ a ] = p.c[ a ]; }
+    r->d[ 0 ] = p.d.x; r->d[ 1 ] = p.d.y; r->d[ 2 ] = p.d.z;
+    r->stokes[ 0 ] = p.S.q; r->stokes[ 1 ] = p.S.u; r->stokes[ 2 ] = p.S.v;
+    r->w = p.w;
+    r->ib = p.b;
+    r->n_scatter = p.n_scat;
+    r->status = status;
+    r->rng_draws = p.rng.draw;
+    r->n_steps = p.n_steps;
 }
 
 }   // namespace kp

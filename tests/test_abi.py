@@ -1,0 +1,30 @@
+"""The C-ABI library loads without a GPU and exports every declared symbol."""
+import ctypes
+
+from kratos_polrad_b200 import _lib
+
+
+def test_every_header_symbol_is_exported():
+    names = _lib.header_symbols()
+    assert "kp_transport_forward" in names and "kp_trace" in names
+    missing = [n for n in names if not hasattr(_lib.lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version_and_error_channel():
+    assert _lib.lib.kp_abi_version() == 1
+    # a failing call reports a status and a message, without touching a GPU
+    st = _lib.lib.kp_mesh_create(None, None)
+    assert st == _lib.KP_ERR_ARG
+    assert b"null" in _lib.lib.kp_last_error()
+
+
+def test_bad_mesh_config_is_refused():
+    d = _lib.MeshDesc()
+    for a in range(3):
+        d.x_min[a], d.x_max[a] = 0.0, 1.0
+        d.n_cell_global[a], d.n_cell_block[a] = 30, 16       # not divisible
+    h = ctypes.c_void_p()
+    st = _lib.lib.kp_mesh_create(ctypes.byref(d), ctypes.byref(h))
+    assert st == _lib.KP_ERR_CONFIG
+    assert b"indivisible" in _lib.lib.kp_last_error()
