@@ -280,6 +280,26 @@ typedef struct kp_tallies
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
+/* Same solve as kp_transport_forward, for callers that must not allocate
+ * device memory during the call: code that owns every device byte itself
+ * (a fixed arena or pool it sized at start-up), or a step that has to run
+ * in a region where cudaMalloc is not allowed.  It calls no cudaMalloc,
+ * cudaFree or allocating library routine.  The kernel's only scratch, the
+ * 64-bit counter that hands out packet indices, lives in a static device
+ * array of KP_NOALLOC_SCRATCH_BYTES that the library holds on every GPU
+ * that loads it, until the process exits.  Inputs and outputs are the
+ * caller's: the mesh must already be on the current device (kp_mesh_upload,
+ * or an earlier kp_mesh_set_sigma, at set-up time), else KP_ERR_CONFIG; a
+ * solve whose scratch would not fit is rejected with KP_ERR_CAPACITY.  The
+ * first call on a device looks up the array's device address, so make that
+ * first call before any stream capture.  Every call uses the same array and
+ * zeroes the counter at its start, so calls that overlap on the GPU race:
+ * run them one after another.  This entry point has no counterpart in the
+ * reference. */
+#define KP_NOALLOC_SCRATCH_BYTES 256
+int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                  const kp_tallies_t * tallies, void * stream );
+
 #ifdef __cplusplus
 }
 #endif

@@ -447,3 +447,66 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream );
     } );
 }
+
+////////////////////////////////////////////////////////////
+// No-allocation entry point: the forward solve with its packet counter in a
+// static device array instead of the mesh's workspace.
+
+#include <mutex>
+
+namespace kp
+{
+namespace
+{
+
+// Scratch of kp_transport_forward_noalloc.  In host code this name is only a
+// stand-in for the symbol: kernels receive the device address looked up
+// below, never the name itself.
+static __device__ __align__( 256 ) unsigned char g_noalloc_scratch[ KP_NOALLOC_SCRATCH_BYTES ];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex    g_noalloc_mutex;
+void        * g_noalloc_addr[ NOALLOC_MAX_DEVICES ] = {  };
+
+// Device address of the scratch array on the current device, looked up once
+// per device (with that device current) and cached.
+void * noalloc_scratch(  )
+{
+    int dev = 0;
+    KP_CUDA( cudaGetDevice( & dev ) );
+    require( dev >= 0 && dev < NOALLOC_MAX_DEVICES, "device index too large for the scratch table",
+             KP_ERR_CAPACITY );
+    std::lock_guard< std::mutex > lock( g_noalloc_mutex );
+    if( g_noalloc_addr[ dev ] == nullptr )
+    {
+        void * p = nullptr;
+        KP_CUDA( cudaGetSymbolAddress( & p, g_noalloc_scratch ) );
+        g_noalloc_addr[ dev ] = p;
+    }
+    return g_noalloc_addr[ dev ];
+}
+
+}   // namespace
+}   // namespace kp
+
+extern "C" int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                             const kp_tallies_t * tallies, void * stream )
+{
+    return kp::guarded( "kp_transport_forward_noalloc", [ & ]
+    {
+        kp::require( mesh && cfg && tallies, "null argument" );
+        kp::require( mesh->uploaded, "mesh is not on the device: call kp_mesh_upload at set-up",
+                     KP_ERR_CONFIG );
+        int dev = 0;
+        KP_CUDA( cudaGetDevice( & dev ) );
+        kp::require( dev == mesh->device, "mesh was uploaded to another device", KP_ERR_CONFIG );
+        // Scratch needed by one forward launch: one 64-bit packet counter.
+        const size_t need = sizeof( unsigned long long );
+        kp::require( need <= KP_NOALLOC_SCRATCH_BYTES,
+                     "forward scratch exceeds KP_NOALLOC_SCRATCH_BYTES", KP_ERR_CAPACITY );
+        static thread_local kp::fwd_params_t P;
+        kp::make_fwd_params( mesh, * cfg, * tallies, P );
+        P.work = static_cast< unsigned long long * >( kp::noalloc_scratch(  ) );
+        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream );
+    } );
+}
