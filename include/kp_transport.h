@@ -280,6 +280,22 @@ typedef struct kp_tallies
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
+/* Path-replay adjoint of the peel-off image.  No reference counterpart (the
+ * reference's transport is not differentiable); it differentiates the
+ * solve of kp_transport_forward with the same cfg (same seed, packet ids
+ * and sources) with respect to the per-cell coefficients.  adj_image
+ * (device, float [image_n][image_n][4]) is dL/dimage in the units of the
+ * forward image tally.  Accumulates, as int64 round(v * 2^grad_fx_shift)
+ * (cfg->tally_mode KP_TALLY_FIXED) or float, per cell:
+ *     grad_len  the path-length term, grad_int  the interaction term, so
+ *     dL/dsigma_sca = grad_len + grad_int,  dL/dsigma_abs = grad_len.
+ * Each packet is replayed twice from its RNG counter; no path is stored.
+ * counters (optional) receives the KP_CNT_* counts of both replays. */
+int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                          const float * adj_image, int grad_fx_shift,
+                          void * grad_len, void * grad_int,
+                          unsigned long long * counters, void * stream );
+
 /* Same solve as kp_transport_forward, for callers that must not allocate
  * device memory during the call: code that owns every device byte itself
  * (a fixed arena or pool it sized at start-up), or a step that has to run

@@ -1,0 +1,391 @@
+// Path-replay adjoint of the peel-off image (gradient of an image loss with
+// respect to the per-cell scattering and absorption coefficients).
+//
+// The reference has no differentiable transport.  The estimator follows path
+// replay backpropagation (Vicini, Speierer & Jakob, SIGGRAPH 2021) for the
+// volumetric case with tau-threshold sampling: for a sampled path held fixed,
+// the peel-off contribution C_k of vertex k (k = 0 the emission, k >= 1 the
+// interactions) has
+//     d ln f_k / d sigma_sca(c) = n_k(c) / sigma_sca(c) - L_k(c) - L_obs,k(c)
+//     d ln f_k / d sigma_abs(c) =                      - L_k(c) - L_obs,k(c)
+// where n_k(c) counts interactions in cell c among vertices 1..k, L_k(c) is
+// the walk's path length in c up to vertex k and L_obs,k(c) the peel-off
+// ray's.  With G_k = <dL/dimage[pixel_k], C_k>, the gradient is
+// sum_k G_k d ln f_k.  Every packet is replayed twice from its RNG counter
+// (no path is stored): pass 0 computes each G_k (kept in a 32-entry per-lane
+// array; later vertices are re-measured in pass 1) and R = sum_{k>=1} G_k;
+// pass 1 deposits -R * length along walk segments (R the suffix sum of the
+// vertices still ahead), +R / sigma_sca at interactions, and -G_k * length
+// along each peel-off ray, subtracting G_k from R after vertex k.
+// Outputs: g_len (length term, shared by both coefficients) and g_int
+// (interaction term, scattering only):
+//     dL/dsigma_sca = g_len + g_int,  dL/dsigma_abs = g_len.
+#include "kp_transport.cuh"
+
+namespace kp
+{
+namespace
+{
+
+constexpr int ADJ_KMAX = 32;
+enum ray_kind { RAY_WALK = 0, RAY_MEASURE = 1, RAY_DEPOSIT = 2 };
+
+template< int TALLY >
+__device__ __forceinline__ void add_grad( void * base, size_t i, double v, double sc )
+{
+    if( TALLY == KP_TALLY_FIXED )
+        atomicAdd( ( unsigned long long * ) base + i,
+                   ( unsigned long long ) __double2ll_rn( __dmul_rn( v, sc ) ) );
+    else
+        atomicAdd( ( float * ) base + i, ( float ) v );
+}
+
+// <dL/dimage[pix], (I, Q, U, V)>
+__device__ __forceinline__ float score( const fwd_params_t & P, int pix, float I, float Q,
+                                        float U, float V )
+{
+    const float4 g = P.adj_img[ pix ];
+    return __fadd_rn( __fadd_rn( __fadd_rn( __fmul_rn( g.x, I ), __fmul_rn( g.y, Q ) ),
+                                 __fmul_rn( g.z, U ) ), __fmul_rn( g.w, V ) );
+}
+
+template< int TALLY >
+__global__ void __launch_bounds__( FWD_THREADS, 3 )
+k_adjoint( const __grid_constant__ fwd_params_t P )
+{
+    __shared__ park_t sp;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const int th = threadIdx.x;
+    if( threadIdx.x < KP_NCOUNTERS ) sp.cnt[ threadIdx.x ] = 0;
+    __syncthreads(  );
+    counts32_t cnt;
+    packet_t p;
+    int   phase = PH_EMIT, ray = RAY_WALK, pass = 0;
+    float ptau = 0.f, pG = 0.f, G0 = 0.f;
+    int   pk = 0, pend = 0, nv = 0;
+    bool  remeasure = false;
+    double R = 0.0;
+    float gk[ ADJ_KMAX ];
+
+    // Starts pass 1 of the lane's packet (same id, RNG from its start).
+    auto begin_pass1 = [ & ](  )
+    {
+        const long long pid = p.pid(  );
+        emit_packet( P, pid, p );
+        p.tau = sample_tau( p.rng );
+        pass = 1;
+        nv = 0;
+        phase = PH_SEGMENT;
+        ray = RAY_WALK;
+        const src_dev_t & s = P.src[ pid % P.n_src ];
+        if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC && G0 != 0.0f )
+        {
+            park_walk( sp, p );
+            pG = G0; ptau = 0.f; pk = 0; pend = 0;
+            ray = RAY_DEPOSIT;
+        }
+    };
+    // The lane's packet has ended (in the current pass).
+    auto end_packet = [ & ](  )
+    {
+        if( pass == 0 )
+            begin_pass1(  );
+        else
+        {
+            phase = PH_EMIT;
+            pass = 0;
+        }
+    };
+
+    for( ;; )
+    {
+        const unsigned m_emit = __ballot_sync( FULL, phase == PH_EMIT );
+        const unsigned m_seg  = __ballot_sync( FULL, phase == PH_SEGMENT );
+        const unsigned m_ev   = __ballot_sync( FULL, phase == PH_EVENT );
+        if( ( m_emit | m_seg | m_ev ) == 0u )
+            break;
+        const int n_seg = __popc( m_seg ), n_ev = __popc( m_ev ), n_emit = __popc( m_emit );
+        int run;
+        if( n_ev > 0 && ( n_ev >= P.ev_batch || n_seg == 0 ) )
+            run = PH_EVENT;
+        else if( n_emit > 0 && ( n_emit >= P.ev_batch || n_seg == 0 ) )
+            run = PH_EMIT;
+        else
+            run = PH_SEGMENT;
+
+        if( run == PH_EMIT )
+        {
+            if( phase != PH_EMIT ) continue;
+            const int leader = __ffs( m_emit ) - 1;
+            const unsigned rank = __popc( m_emit & ( ( 1u << lane ) - 1u ) );
+            unsigned long long base = 0;
+            if( ( int ) lane == leader )
+                base = atomicAdd( P.work, ( unsigned long long ) n_emit );
+            base = __shfl_sync( m_emit, base, leader );
+            const unsigned long long idx = base + rank;
+            if( idx >= ( unsigned long long ) P.n_packets )
+            {
+                phase = PH_DONE;
+                continue;
+            }
+            if( ! emit_packet( P, P.pid0 + ( long long ) idx, p ) )
+            {
+                atomicOr( P.m.status, ST_BAD_SOURCE );
+                continue;
+            }
+            count( sp, KP_CNT_EMITTED );
+            p.tau = sample_tau( p.rng );
+            pass = 0; nv = 0; R = 0.0; G0 = 0.f;
+            phase = PH_SEGMENT;
+            ray = RAY_WALK;
+            const src_dev_t & s = P.src[ p.pid(  ) % P.n_src ];
+            if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
+            {
+                const int pix = image_pixel( P, p.x );
+                if( pix >= 0 )
+                {
+                    sp.w[ th ] = 1.0f; sp.I[ th ] = 0x1.45f306p-4f;    // 1 / (4 pi)
+                    sp.Q[ th ] = sp.U[ th ] = sp.V[ th ] = 0.0f;
+                    sp.pix[ th ] = pix;
+                    pend = 0; ptau = 0.0f; pk = 0;
+                    park_walk( sp, p );
+                    ray = RAY_MEASURE;
+                }
+            }
+            continue;
+        }
+
+        if( run == PH_EVENT )
+        {
+            if( phase != PH_EVENT ) continue;
+            ++ p.n_scat;
+            count( sp, KP_CNT_SCATTER );
+            const size_t ci = cell_index( P.m, p.b, p.c );
+            {
+                const float2 sg = P.m.sigma[ ci ];
+                p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, __fadd_rn( sg.x, sg.y ) ) );
+                if( pass == 1 && R != 0.0 )
+                    add_grad< TALLY >( P.g_int, ci, __ddiv_rn( R, ( double ) sg.x ), P.g_scale );
+            }
+            ++ nv;
+            bool do_peel = false;
+            if( P.img_n > 0 )
+            {
+                const int pix = image_pixel( P, p.x );
+                if( pix >= 0 )
+                {
+                    float Q, U, V;
+                    sp.I[ th ] = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev, P.eh, Q, U, V );
+                    sp.Q[ th ] = Q; sp.U[ th ] = U; sp.V[ th ] = V;
+                    sp.w[ th ] = p.w;
+                    sp.pix[ th ] = pix;
+                    do_peel = true;
+                }
+            }
+            int end = 0;
+            if( p.n_scat >= P.max_scatter )
+                end = PK_SCATTER_CAP;
+            else if( p.w < P.w_min )
+            {
+                const phys::u4 r = p.rng.next(  );
+                if( phys::u01( r.x ) < P.rr_survive )
+                    p.w = __fdiv_rn( p.w, P.rr_survive );
+                else
+                    end = PK_ABSORBED;
+            }
+            if( ! end )
+            {
+                phys::scatter( P.ph, p.rng, p.d, p.e1, p.S );
+                set_inv( p );
+                p.tau = sample_tau( p.rng );
+            }
+            if( ! end && p.n_steps >= P.max_steps )
+                end = PK_STEP_CAP;
+            phase = PH_SEGMENT;
+            if( do_peel )
+            {
+                pend = end;
+                ptau = 0.f; pk = 0;
+                if( pass == 0 || nv > ADJ_KMAX )
+                {
+                    park_walk( sp, p );
+                    ray = RAY_MEASURE;
+                    remeasure = pass == 1;
+                    continue;
+                }
+                pG = gk[ nv - 1 ];
+                if( pG != 0.0f )
+                {
+                    park_walk( sp, p );
+                    ray = RAY_DEPOSIT;
+                    continue;
+                }
+            }
+            if( end )
+                end_packet(  );
+            continue;
+        }
+
+        // ---- PH_SEGMENT ----
+        if( phase != PH_SEGMENT ) continue;
+        const bool peel = ray != RAY_WALK;
+        const size_t ci = cell_index( P.m, p.b, p.c );
+        const float2 sg = P.m.sigma[ ci ];
+        const float ext = __fadd_rn( sg.x, sg.y );
+        const phys::v3 dd = peel ? P.o : p.d;
+        const double inv[ 3 ] = { peel ? P.inv_o[ 0 ] : p.inv[ 0 ],
+                                  peel ? P.inv_o[ 1 ] : p.inv[ 1 ],
+                                  peel ? P.inv_o[ 2 ] : p.inv[ 2 ] };
+        int ax;
+        const double t = exit_dist( P.m, p.b, p.c, p.x, dd, inv, ax );
+        const float et = __fmul_rn( ext, ( float ) t );
+        bool interact = false, peel_cut = false;
+        if( peel )
+        {
+            ++ cnt.peel;
+            ++ pk;
+            ptau = __fadd_rn( ptau, et );
+            peel_cut = ptau > P.tau_cut;
+            if( ray == RAY_DEPOSIT && ! peel_cut )
+                add_grad< TALLY >( P.g_len, ci, __dmul_rn( -( double ) pG, t ), P.g_scale );
+        }
+        else
+        {
+            ++ cnt.steps;
+            ++ p.n_steps;
+            interact = et >= p.tau;
+        }
+        if( interact )
+        {
+            double ti = ( double ) __fdiv_rn( p.tau, ext );
+            ti = ti > t ? t : ti;
+            if( pass == 1 && R != 0.0 )
+                add_grad< TALLY >( P.g_len, ci, __dmul_rn( -R, ti ), P.g_scale );
+            p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
+            p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
+            p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
+            phase = PH_EVENT;
+            continue;
+        }
+        bool left = false, lost = false;
+        if( ! peel_cut )
+        {
+            if( ! peel )
+            {
+                p.tau = __fsub_rn( p.tau, et );
+                if( pass == 1 && R != 0.0 )
+                    add_grad< TALLY >( P.g_len, ci, __dmul_rn( -R, t ), P.g_scale );
+            }
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a )
+                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
+            const int b_old = p.b;
+            left = ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost );
+            if( ! left && p.b != b_old ) count( sp, KP_CNT_HOPS );
+        }
+        if( peel )
+        {
+            if( !( peel_cut || left || pk >= ( 1 << 20 ) ) )
+                continue;
+            if( ray == RAY_MEASURE )
+            {
+                float G = 0.0f;
+                if( ptau <= P.tau_cut )
+                {
+                    const float att = __fmul_rn( sp.w[ th ],
+                                                 ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    G = score( P, sp.pix[ th ], __fmul_rn( att, sp.I[ th ] ),
+                               __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
+                               __fmul_rn( att, sp.V[ th ] ) );
+                }
+                if( remeasure )
+                {   // pass 1, vertex beyond the stored ones: now deposit along it
+                    remeasure = false;
+                    unpark_walk( sp, p );
+                    if( G != 0.0f )
+                    {
+                        pG = G; ptau = 0.f; pk = 0;
+                        ray = RAY_DEPOSIT;          // the walk position stays parked
+                        continue;
+                    }
+                }
+                else if( nv == 0 )
+                    G0 = G;                          // emission
+                else
+                {
+                    R = __dadd_rn( R, ( double ) G );
+                    if( nv <= ADJ_KMAX ) gk[ nv - 1 ] = G;
+                }
+            }
+            else if( nv > 0 )
+                R = __dsub_rn( R, ( double ) pG );   // deposit ray of vertex nv done
+            unpark_walk( sp, p );
+            ray = RAY_WALK;
+            if( pend )
+                end_packet(  );
+            continue;
+        }
+        if( left || p.n_steps >= P.max_steps )
+        {
+            if( left )
+                count( sp, lost ? KP_CNT_LOST : KP_CNT_ESCAPED );
+            else
+                count( sp, KP_CNT_CAPPED );
+            end_packet(  );
+        }
+    }
+    count( sp, KP_CNT_STEPS, cnt.steps );
+    count( sp, KP_CNT_PEEL_STEPS, cnt.peel );
+    __syncthreads(  );
+    if( P.counters && threadIdx.x < KP_NCOUNTERS && sp.cnt[ threadIdx.x ] )
+        atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );
+}
+
+}   // namespace
+}   // namespace kp
+
+extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                     const float * adj_image, int grad_fx_shift,
+                                     void * grad_len, void * grad_int,
+                                     unsigned long long * counters, void * stream )
+{
+    return kp::guarded( "kp_transport_adjoint", [ & ]
+    {
+        kp::require( mesh && cfg && adj_image && grad_len && grad_int, "null argument" );
+        kp::require( cfg->image_n > 0, "the adjoint needs a peel-off image (image_n > 0)" );
+        kp::require( grad_fx_shift >= 0 && grad_fx_shift <= 48, "grad_fx_shift out of range" );
+        mesh->upload(  );
+        static thread_local kp::fwd_params_t P;
+        kp_tallies_t none {  };
+        none.counters = counters;
+        // the forward's image buffers are not written by the adjoint; any
+        // non-null placeholders pass the configuration checks
+        none.image = grad_len;
+        none.image_batch = grad_len;
+        none.mu = grad_len;
+        kp_transport_cfg_t c = * cfg;
+        c.n_record = 0;
+        kp::make_fwd_params( mesh, c, none, P );
+        P.image = P.img_batch = P.mu_tally = nullptr;
+        P.adj_img = reinterpret_cast< const float4 * >( adj_image );
+        P.g_len = grad_len;
+        P.g_int = grad_int;
+        P.g_scale = std::ldexp( 1.0, grad_fx_shift );
+        P.work = mesh->workspace(  );
+        if( P.n_packets == 0 ) return;
+        auto s = ( cudaStream_t ) stream;
+        const int threads = kp::FWD_THREADS;
+        const void * k = c.tally_mode == KP_TALLY_FIXED
+                       ? ( const void * ) kp::k_adjoint< KP_TALLY_FIXED >
+                       : ( const void * ) kp::k_adjoint< KP_TALLY_FLOAT >;
+        long long grid = kp::persistent_grid( k, threads );
+        grid = std::min< long long >( grid, ( P.n_packets + threads - 1 ) / threads );
+        KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
+        if( c.tally_mode == KP_TALLY_FIXED )
+            kp::k_adjoint< KP_TALLY_FIXED ><<< ( unsigned ) grid, threads, 0, s >>>( P );
+        else
+            kp::k_adjoint< KP_TALLY_FLOAT ><<< ( unsigned ) grid, threads, 0, s >>>( P );
+        KP_CUDA( cudaGetLastError(  ) );
+    } );
+}

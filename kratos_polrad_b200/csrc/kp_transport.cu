@@ -17,50 +17,6 @@ namespace
 {
 namespace cg = cooperative_groups;
 
-// Segment counts stay in registers (32-bit: a thread walks far fewer than
-// 2^32 segments in one launch); rare events are counted in shared memory.
-struct counts32_t
-{
-    unsigned steps = 0, peel = 0;
-};
-
-constexpr int FWD_THREADS = 256;
-
-// Rarely touched per-lane state kept in shared memory (structure of arrays):
-// the parked walk position while a peel-off ray runs, and the pending
-// peel-off contribution.
-struct park_t
-{
-    double x[ 3 ][ FWD_THREADS ];
-    int    c[ 3 ][ FWD_THREADS ];
-    int    b[ FWD_THREADS ];
-    float  w[ FWD_THREADS ], I[ FWD_THREADS ], Q[ FWD_THREADS ], U[ FWD_THREADS ],
-           V[ FWD_THREADS ];
-    int    pix[ FWD_THREADS ];
-    unsigned long long cnt[ KP_NCOUNTERS ];
-};
-
-__device__ __forceinline__ void park_walk( park_t & sp, const packet_t & p )
-{
-    const int t = threadIdx.x;
-    #pragma unroll
-    for( int a = 0; a < 3; ++ a ) { sp.x[ a ][ t ] = p.x[ a ]; sp.c[ a ][ t ] = p.c[ a ]; }
-    sp.b[ t ] = p.b;
-}
-__device__ __forceinline__ void unpark_walk( const park_t & sp, packet_t & p )
-{
-    const int t = threadIdx.x;
-    #pragma unroll
-    for( int a = 0; a < 3; ++ a ) { p.x[ a ] = sp.x[ a ][ t ]; p.c[ a ] = sp.c[ a ][ t ]; }
-    p.b = sp.b[ t ];
-}
-__device__ __forceinline__ void count( park_t & sp, int k, unsigned v = 1u )
-{
-    atomicAdd( sp.cnt + k, ( unsigned long long ) v );
-}
-
-// Lane phases of the forward kernel.
-enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3 };
 
 // Warp-synchronous scheduler.  Each lane carries one packet through a small
 // state machine: EMIT (needs a packet), SEGMENT (advance its active ray by

@@ -63,6 +63,11 @@ struct fwd_params_t
     kp_packet_record_t * records;
     long long   n_record;
     unsigned long long * work;     // scratch: next packet index
+    // adjoint only
+    const float4 * adj_img;        // dL/d(image) [img_n * img_n] (I, Q, U, V)
+    void      * g_len;             // path-length term per cell
+    void      * g_int;             // interaction term per cell (sigma_sca only)
+    double      g_scale;           // fixed point scale of the gradient tallies
     src_dev_t   src[ MAX_SOURCES ];
 };
 
@@ -394,5 +399,55 @@ __device__ __forceinline__ void write_record( const fwd_params_t & P, const pack
     r->rng_draws = p.rng.draw;
     r->n_steps = p.n_steps;
 }
+
+// Lane phases of the warp-synchronous transport kernels.
+enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3 };
+
+// Segment counts stay in registers (32-bit: a thread walks far fewer than
+// 2^32 segments in one launch); rare events are counted in shared memory.
+struct counts32_t
+{
+    unsigned steps = 0, peel = 0;
+};
+
+constexpr int FWD_THREADS = 256;
+
+// Rarely touched per-lane state kept in shared memory (structure of arrays):
+// the parked walk position while a peel-off ray runs, and the pending
+// peel-off contribution.
+struct park_t
+{
+    double x[ 3 ][ FWD_THREADS ];
+    int    c[ 3 ][ FWD_THREADS ];
+    int    b[ FWD_THREADS ];
+    float  w[ FWD_THREADS ], I[ FWD_THREADS ], Q[ FWD_THREADS ], U[ FWD_THREADS ],
+           V[ FWD_THREADS ];
+    int    pix[ FWD_THREADS ];
+    unsigned long long cnt[ KP_NCOUNTERS ];
+};
+
+__device__ __forceinline__ void park_walk( park_t & sp, const packet_t & p )
+{
+    const int t = threadIdx.x;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { sp.x[ a ][ t ] = p.x[ a ]; sp.c[ a ][ t ] = p.c[ a ]; }
+    sp.b[ t ] = p.b;
+}
+__device__ __forceinline__ void unpark_walk( const park_t & sp, packet_t & p )
+{
+    const int t = threadIdx.x;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { p.x[ a ] = sp.x[ a ][ t ]; p.c[ a ] = sp.c[ a ][ t ]; }
+    p.b = sp.b[ t ];
+}
+__device__ __forceinline__ void count( park_t & sp, int k, unsigned v = 1u )
+{
+    atomicAdd( sp.cnt + k, ( unsigned long long ) v );
+}
+
+// Host helpers shared by the transport entry points (kp_transport.cu).
+void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
+                      const kp_tallies_t & t, fwd_params_t & P );
+int  persistent_grid( const void * kernel, int threads );
 
 }   // namespace kp

@@ -447,10 +447,10 @@ static void trecord( const kpo_cfg_t * c, kpo_record_t * rec, const tpk * p, int
     r->rng_draws = p->rng.draw; r->n_steps = p->n_steps;
 }
 
-int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
-                   const int * lookup_n, const kpo_cfg_t * c, long long * mu,
-                   long long * image, long long * img_batch,
-                   unsigned long long * counters, kpo_record_t * rec )
+/* Fills the transport context from the mesh tables and configuration
+ * (the host side of make_fwd_params in the device code). */
+static int tsetup( tctx * tp, const kpo_mesh_t * m, const float * sigma2, const int * lookup,
+                   const int * lookup_n, const kpo_cfg_t * c )
 {
     tctx t;
     memset( & t, 0, sizeof( t ) );
@@ -496,8 +496,18 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
     t.rr_survive = c->rr_survive > 0 ? c->rr_survive : 0.1f;
     t.max_scatter = c->max_scatter;
     t.max_steps = c->max_steps;
-    t.mu = mu; t.image = image; t.img_batch = img_batch;
+    * tp = t;
+    return 0;
+}
 
+int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
+                   const int * lookup_n, const kpo_cfg_t * c, long long * mu,
+                   long long * image, long long * img_batch,
+                   unsigned long long * counters, kpo_record_t * rec )
+{
+    tctx t;
+    if( tsetup( & t, m, sigma2, lookup, lookup_n, c ) ) return -2;
+    t.mu = mu; t.image = image; t.img_batch = img_batch;
     unsigned long long cnt[ 10 ] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
     for( long long k = 0; k < c->n_packets; ++ k )
     {
@@ -640,4 +650,201 @@ void kpo_scatter_sample( long n, uint32_t seed, int kind, float g, float pmax,
         o[ 3 ] = e1.x; o[ 4 ] = e1.y; o[ 5 ] = e1.z;
         o[ 6 ] = S.q; o[ 7 ] = S.u; o[ 8 ] = S.v;
     }
+}
+
+/* ====================================================================== */
+/* Path-replay adjoint restatement (same estimator and operation order as  */
+/* the device kernel; sequential packets; int64 gradient tallies).         */
+
+static void tgadd( long long * base, long i, double v, double sc )
+{
+    base[ i ] += llrint( v * sc );
+}
+
+static float tscore( const float * g, int pix, float I, float Q, float U, float V )
+{
+    const float * q = g + 4 * ( long ) pix;
+    return ( ( q[ 0 ] * I + q[ 1 ] * Q ) + q[ 2 ] * U ) + q[ 3 ] * V;
+}
+
+/* Marches a peel-off ray like tpeel_tau and deposits -G * length per cell. */
+static void tpeel_deposit( const tctx * t, int b, const int * c0, const double * x0, float G,
+                           long long * g_len, double gsc, unsigned long long * steps )
+{
+    int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
+    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
+    float tau = 0.0f;
+    for( int k = 0; k < ( 1 << 20 ); ++ k )
+    {
+        const long ci = tcell( t, b, c );
+        const float ext = t->sig[ 2 * ci ] + t->sig[ 2 * ci + 1 ];
+        int ax;
+        const double tt = texit( t, b, c, x, t->o, t->inv_o, & ax );
+        tau = tau + ext * ( float ) tt;
+        ++ * steps;
+        if( tau > t->tau_cut ) return;
+        tgadd( g_len, ci, -( double ) G * tt, gsc );
+        for( int a = 0; a < 3; ++ a )
+            if( a != ax ) x[ a ] = fma( tt, t->o_d[ a ], x[ a ] );
+        int lost;
+        if( ! tcross( t, & b, c, x, ax, om_comp( t->o, ax ) > 0.0f, & lost ) ) return;
+    }
+}
+
+/* One replay of a packet.  pass 0 fills G0, Gs[] and *R (the sum of the
+ * interaction terms, in vertex order); pass 1 deposits, starting from that
+ * *R and subtracting each vertex's G after its peel-off ray.  Returns the
+ * number of interaction vertices. */
+static int tadjoint_pass( const tctx * t, const kpo_cfg_t * c, long long pid, int pass,
+                          const float * g, float * G0, float * Gs, int gs_cap, double * Rp,
+                          long long * g_len, long long * g_int, double gsc,
+                          unsigned long long * cnt )
+{
+    tpk p;
+    if( ! temit( t, c, pid, & p ) ) return -1;
+    const kpo_source_t * s = c->sources + pid % c->n_sources;
+    p.tau = tsample_tau( & p.rng );
+    double R = pass == 1 ? * Rp : 0.0;
+    int nv = 0;
+    if( t->img_n > 0 && s->kind == 0 && s->emit == 0 )
+    {
+        const int pix = timage_pixel( t, p.x );
+        if( pix >= 0 )
+        {
+            if( pass == 0 )
+            {
+                const float tau = tpeel_tau( t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
+                float G = 0.0f;
+                if( tau <= t->tau_cut )
+                {
+                    const float att = 1.0f * ( float ) om_exp_neg( -( double ) tau );
+                    G = tscore( g, pix, att * 0x1.45f306p-4f, att * 0.0f, att * 0.0f, att * 0.0f );
+                }
+                * G0 = G;
+            }
+            else if( * G0 != 0.0f )
+                tpeel_deposit( t, p.b, p.c, p.x, * G0, g_len, gsc, & cnt[ 1 ] );
+        }
+    }
+    for( ;; )
+    {
+        const long ci = tcell( t, p.b, p.c );
+        const float ss = t->sig[ 2 * ci ], sa = t->sig[ 2 * ci + 1 ];
+        const float ext = ss + sa;
+        int ax;
+        const double tt = texit( t, p.b, p.c, p.x, p.d, p.inv, & ax );
+        const float dtau = ext * ( float ) tt;
+        ++ cnt[ 0 ];
+        ++ p.n_steps;
+        int end = 0;
+        if( dtau >= p.tau )
+        {
+            double ti = ( double ) ( p.tau / ext );
+            ti = ti > tt ? tt : ti;
+            if( pass == 1 && R != 0.0 ) tgadd( g_len, ci, -R * ti, gsc );
+            p.x[ 0 ] = fma( ti, ( double ) p.d.x, p.x[ 0 ] );
+            p.x[ 1 ] = fma( ti, ( double ) p.d.y, p.x[ 1 ] );
+            p.x[ 2 ] = fma( ti, ( double ) p.d.z, p.x[ 2 ] );
+            ++ p.n_scat;
+            ++ cnt[ 2 ];
+            p.w = p.w * ( ss / ext );
+            if( pass == 1 && R != 0.0 ) tgadd( g_int, ci, R / ( double ) ss, gsc );
+            ++ nv;
+            const int pix = t->img_n > 0 ? timage_pixel( t, p.x ) : -1;
+            float pI = 0, pQ = 0, pU = 0, pV = 0, pw = 0;
+            if( pix >= 0 )
+            {
+                pI = om_peel_stokes( t->ph, p.d, p.e1, p.S, t->o, t->ev, t->eh, & pQ, & pU, & pV );
+                pw = p.w;
+            }
+            /* the peel-off ray of this vertex (before roulette and scattering,
+             * whose random numbers it does not use) */
+            if( pix >= 0 )
+            {
+                if( pass == 0 )
+                {
+                    const float tau = tpeel_tau( t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
+                    float G = 0.0f;
+                    if( tau <= t->tau_cut )
+                    {
+                        const float att = pw * ( float ) om_exp_neg( -( double ) tau );
+                        G = tscore( g, pix, att * pI, att * pQ, att * pU, att * pV );
+                    }
+                    R += ( double ) G;
+                    if( nv <= gs_cap ) Gs[ nv - 1 ] = G;
+                    else return -3;
+                }
+                else
+                {
+                    const float G = Gs[ nv - 1 ];
+                    if( G != 0.0f )
+                    {
+                        tpeel_deposit( t, p.b, p.c, p.x, G, g_len, gsc, & cnt[ 1 ] );
+                        R = R - ( double ) G;
+                    }
+                }
+            }
+            if( p.n_scat >= t->max_scatter ) end = ST_SCATTER_CAP;
+            else if( p.w < t->w_min )
+            {
+                const om_u4 r = om_next( & p.rng );
+                if( om_u01( r.x ) < t->rr_survive ) p.w = p.w / t->rr_survive;
+                else end = ST_ABSORBED;
+            }
+            if( ! end )
+            {
+                om_scatter( t->ph, & p.rng, & p.d, & p.e1, & p.S );
+                tset_inv( & p );
+                p.tau = tsample_tau( & p.rng );
+            }
+        }
+        else
+        {
+            p.tau = p.tau - dtau;
+            if( pass == 1 && R != 0.0 ) tgadd( g_len, ci, -R * tt, gsc );
+            for( int a = 0; a < 3; ++ a )
+                if( a != ax ) p.x[ a ] = fma( tt, ( double ) om_comp( p.d, a ), p.x[ a ] );
+            int lost;
+            const int b_old = p.b;
+            if( ! tcross( t, & p.b, p.c, p.x, ax, om_comp( p.d, ax ) > 0.0f, & lost ) )
+                end = lost ? ST_LOST : ST_ESCAPED;
+            else
+                cnt[ 8 ] += p.b != b_old;
+        }
+        if( ! end && p.n_steps >= t->max_steps ) end = ST_STEP_CAP;
+        if( end ) break;
+    }
+    if( pass == 0 ) * Rp = R;
+    return nv;
+}
+
+int kpo_adjoint( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
+                 const int * lookup_n, const kpo_cfg_t * c, const float * adj_img,
+                 int grad_shift, long long * g_len, long long * g_int,
+                 unsigned long long * counters )
+{
+    tctx t;
+    if( tsetup( & t, m, sigma2, lookup, lookup_n, c ) ) return -2;
+    const double gsc = ldexp( 1.0, grad_shift );
+    const int cap = 1 << 16;
+    float * Gs = ( float * ) malloc( sizeof( float ) * cap );
+    unsigned long long cnt[ 10 ] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+    int rc = 0;
+    for( long long k = 0; k < c->n_packets && rc == 0; ++ k )
+    {
+        const long long pid = c->packet_offset + k;
+        float G0 = 0.0f;
+        double R = 0.0;
+        const int n = tadjoint_pass( & t, c, pid, 0, adj_img, & G0, Gs, cap, & R, g_len, g_int,
+                                     gsc, cnt );
+        if( n < 0 ) { rc = n; break; }
+        if( tadjoint_pass( & t, c, pid, 1, adj_img, & G0, Gs, cap, & R, g_len, g_int, gsc,
+                           cnt ) < 0 )
+            rc = -1;
+    }
+    if( counters )
+        for( int k = 0; k < 10; ++ k ) counters[ k ] += cnt[ k ];
+    free( Gs );
+    free( t.inv_dx );
+    return rc;
 }

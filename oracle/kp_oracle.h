@@ -118,3 +118,21 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
 }
 #endif
 #endif
+
+#ifndef KPO_ADJOINT_DECLS
+#define KPO_ADJOINT_DECLS
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* Path-replay adjoint of the peel-off image: adj_img [image_n][image_n][4]
+ * float is dL/dimage; accumulates int64 round(v * 2^grad_shift) of the
+ * path-length term into g_len and of the interaction term into g_int
+ * (dL/dsigma_sca = g_len + g_int, dL/dsigma_abs = g_len). */
+int kpo_adjoint( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
+                 const int * lookup_n, const kpo_cfg_t * c, const float * adj_img,
+                 int grad_shift, long long * g_len, long long * g_int,
+                 unsigned long long * counters );
+#ifdef __cplusplus
+}
+#endif
+#endif

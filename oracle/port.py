@@ -191,3 +191,41 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
         raise RuntimeError(f"kpo_transport failed ({st})")
     out["records"] = rec[:cfg.n_record]
     return out
+
+
+def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, grad_shift=24):
+    """Restated path-replay adjoint; returns int64 (g_len, g_int), counters."""
+    src = (_Source * max(1, len(cfg.sources)))()
+    for k, s in enumerate(cfg.sources):
+        src[k].kind, src[k].emit = int(s.kind), int(s.emit)
+        for a in range(3):
+            src[k].pos[a] = float(s.pos[a])
+        ib, cell = source_cells[k]
+        src[k].ib = int(ib)
+        for a in range(3):
+            src[k].cell[a] = int(cell[a])
+    c = _Cfg()
+    for name, _ in _Cfg._fields_:
+        if name in ("sources", "n_sources", "image_center"):
+            continue
+        setattr(c, name, getattr(cfg, name))
+    c.n_sources = len(cfg.sources)
+    c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
+    for a in range(3):
+        c.image_center[a] = float(cfg.image_center[a])
+    n_cells = tab.n_blocks * tab.cells_per_block
+    g_len, g_int = np.zeros(n_cells, np.int64), np.zeros(n_cells, np.int64)
+    cnt = np.zeros(10, np.uint64)
+    sigma2 = np.ascontiguousarray(sigma2, np.float32)
+    lookup = np.ascontiguousarray(lookup, np.int32)
+    lk_n = np.ascontiguousarray(lookup_n, np.int32)
+    adj = np.ascontiguousarray(adj_img, np.float32)
+    s = tab._struct()
+    L = lib()
+    L.kpo_adjoint.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int] + [ctypes.c_void_p] * 3
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)
+    st = L.kpo_adjoint(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c), p(adj),
+                       grad_shift, p(g_len), p(g_int), p(cnt))
+    if st != 0:
+        raise RuntimeError(f"kpo_adjoint failed ({st})")
+    return g_len, g_int, cnt

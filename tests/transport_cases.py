@@ -73,3 +73,25 @@ def run_oracle(mesh, sig, t):
         else:
             cells.append((0, (0, 0, 0)))
     return port.transport(tab, sig, grid, n, t, cells)
+
+
+def oracle_inputs(mesh, t):
+    """Tables, lookup grid and located source cells for the oracle."""
+    tab = port.Tables.from_mesh(mesh, 8)
+    lev, reg = mesh.blocks()
+    root = [int(round((mesh.x_max[a] - mesh.x_min[a]) / (tab.dx0[0, a] * mesh.nc[a] * 2 ** lev[0])))
+            for a in range(3)]
+    grid, n = port.lookup_grid(lev, reg, root)
+    cells = []
+    for s in t.sources:
+        if s.kind == SOURCE_POINT:
+            ib, cell = mesh.locate(np.array([s.pos]))
+            cells.append((ib[0], cell[0]))
+        else:
+            cells.append((0, (0, 0, 0)))
+    return tab, grid, n, cells
+
+
+def run_oracle_adjoint(mesh, sig, t, adj_img, grad_shift=24):
+    tab, grid, n, cells = oracle_inputs(mesh, t)
+    return port.adjoint(tab, sig, grid, n, t, cells, adj_img, grad_shift)
