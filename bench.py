@@ -297,6 +297,29 @@ def main():
                 "algorithmic_bytes": algorithmic_bytes(c_rank),
                 "kernel_ms": statistics.mean(kern_ms)}
 
+    # ---- adjoint: gradient of an image loss, cost relative to one forward ----
+    from kratos_polrad_b200.adjoint import adjoint as run_adjoint
+    adj_img = torch.randn((cfg.image_n, cfg.image_n, 4), device=dev, generator=torch.Generator(
+        device=dev).manual_seed(7)) * 2.0 ** -cfg.fx_shift
+    adj_cnt = torch.zeros(10, dtype=torch.int64, device=dev)
+    run_adjoint(mesh, cfg, adj_img, 24, adj_cnt)
+    torch.cuda.synchronize()
+    adj_ms = []
+    for k in range(max(1, min(args.steps, 3))):
+        adj_cnt.zero_()
+        flush.fill_(float(k))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        run_adjoint(mesh, cfg, adj_img, 24, adj_cnt)
+        a1.record()
+        torch.cuda.synchronize()
+        adj_ms.append(a0.elapsed_time(a1))
+    ac = adj_cnt.cpu().numpy()
+    adjoint_info = {"ms_per_solve": statistics.mean(adj_ms),
+                    "cost_vs_forward": statistics.mean(adj_ms) / statistics.mean(kern_ms),
+                    "packet_steps_per_s": float(ac[0] + ac[1]) / (statistics.mean(adj_ms) / 1e3),
+                    "note": "two replays per packet (measure, deposit); same packets as the forward"}
+
     # ---- end to end through the C ABI with host buffers ----
     import ctypes
     n_cells = mesh.n_cells
@@ -349,6 +372,7 @@ def main():
                "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
+               "adjoint": adjoint_info,
                "gpu_launches": args.steps, "clocks": clk.summary()}
         print(json.dumps(out), flush=True)
     if world > 1:
