@@ -71,7 +71,14 @@ class TransportImage(torch.autograd.Function):
         (sig2,) = ctx.saved_tensors
         mesh, cfg = ctx.mesh, ctx.cfg
         mesh.set_sigma(sig2)
-        # d(image)/d(tally) = scale / N; the adjoint input is dL/d(tally)
-        scale = (2.0 ** -cfg.fx_shift if cfg.tally_mode == TALLY_FIXED else 1.0) / cfg.n_packets
-        g_sca, g_abs = gradients(mesh, cfg, (g_img * scale).to(torch.float32), ctx.shift)
-        return g_sca.to(sig2.dtype), g_abs.to(sig2.dtype), None, None, None
+        # image = (sum of per-packet contributions C) / N.  The kernel returns
+        # d/dsigma of sum_k <a, C_k> for an adjoint image a; it is called with
+        # a = g / max|g| (order one, so the fixed-point deposits keep their
+        # precision) and the result is scaled back by max|g| / N.
+        gmax = g_img.abs().max()
+        if not torch.isfinite(gmax) or gmax == 0:
+            z = torch.zeros(mesh.n_cells, dtype=torch.float64, device=g_img.device)
+            return z, z.clone(), None, None, None
+        g_sca, g_abs = gradients(mesh, cfg, (g_img / gmax).to(torch.float32), ctx.shift)
+        f = gmax / cfg.n_packets
+        return g_sca * f, g_abs * f, None, None, None

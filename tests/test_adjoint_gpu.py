@@ -40,9 +40,12 @@ def test_adjoint_float_mode_close():
                        dtype=torch.float32, device="cuda")
     a_s, a_a = gradients(mesh, t, adj, 24)
     b_s, b_a = gradients(mesh, dataclasses.replace(t, tally_mode=TALLY_FLOAT), adj, 24)
+    # float atomics vs int64 sums of 2^-24-rounded deposits: both approximate
+    # the exact sum; per cell within 1e-3 of the field's peak, and 1e-4 in L2
     for x, y in ((a_s, b_s), (a_a, b_a)):
         x, y = x.cpu().numpy(), y.cpu().numpy()
-        np.testing.assert_allclose(y, x, rtol=0, atol=1e-4 * np.abs(x).max())
+        np.testing.assert_allclose(y, x, rtol=0, atol=1e-3 * np.abs(x).max())
+        assert np.linalg.norm(y - x) < 1e-4 * np.linalg.norm(x)
 
 
 def test_autograd_backward_is_the_adjoint():
@@ -57,8 +60,9 @@ def test_autograd_backward_is_the_adjoint():
     loss.backward()
     g_img = torch.zeros_like(img)
     g_img[..., 1:3] = 2 * img[..., 1:3]
-    scale = 2.0 ** -t.fx_shift / t.n_packets
-    e_sca, e_abs = gradients(mesh, t, (g_img * scale).float(), 24)
-    torch.testing.assert_close(sca.grad, e_sca, rtol=0, atol=0)
-    torch.testing.assert_close(ab.grad, e_abs, rtol=0, atol=0)
+    gmax = g_img.abs().max()
+    e_sca, e_abs = gradients(mesh, t, (g_img / gmax).float(), 24)
+    f = gmax / t.n_packets
+    torch.testing.assert_close(sca.grad, e_sca * f, rtol=0, atol=0)
+    torch.testing.assert_close(ab.grad, e_abs * f, rtol=0, atol=0)
     assert torch.isfinite(sca.grad).all() and sca.grad.abs().sum() > 0
