@@ -280,6 +280,59 @@ typedef struct kp_tallies
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
+/* ------------------------------------------------------------------ */
+/* Batched solves: many independent scenes in one persistent launch.    */
+/* The reference solves one mesh per process, one cycle at a time       */
+/* (modules/particle/driver.h:59-79); there is no counterpart.  The     */
+/* scenes' block tables are concatenated into one multi-scene mesh; a   */
+/* scene's packets (seed from the cfg, its own stream_id, local ids     */
+/* 0..n-1) are identical to those of a kp_transport_forward of that     */
+/* scene alone with the same seed and stream_id.                        */
+
+typedef struct kp_batch kp_batch_t;
+
+typedef struct kp_scene
+{
+    kp_mesh_t * mesh;          /* uploaded mesh with its coefficients set      */
+    long long   n_packets;
+    uint32_t    stream_id;     /* RNG key word of the scene's packets          */
+    kp_source_t source;        /* point source                                 */
+} kp_scene_t;
+
+typedef struct kp_tune_result
+{
+    int       threads;         /* threads per block (128 or 256)               */
+    int       lane_batch;      /* event batch (see kp_transport_cfg_t)         */
+    int       grid_pct;        /* persistent grid, percent of resident blocks  */
+    float     sample_ms;       /* time of the best candidate on the sample     */
+    long long sample_packets;
+} kp_tune_result_t;
+
+/* Builds the concatenated tables (the scenes must share the cells per block;
+ * their meshes are uploaded and their coefficients copied). */
+int kp_batch_create( int n_scenes, const kp_scene_t * scenes, kp_batch_t ** batch );
+int kp_batch_destroy( kp_batch_t * batch );
+/* Re-copies every scene's coefficients after kp_mesh_set_sigma. */
+int kp_batch_refresh_sigma( kp_batch_t * batch, void * stream );
+/* Synchronizes, returns and clears the batch's device error status. */
+int kp_batch_status( kp_batch_t * batch, void * stream, unsigned * flags );
+/* One launch over all scenes.  cfg gives the physics and tally settings
+ * (n_packets, packet_offset is added to every local id, sources and images
+ * are not used: image_n must be 0).  mu: device [n_scenes][n_batches]
+ * [n_mu_bins][4], accumulated into. */
+int kp_batch_forward( kp_batch_t * batch, const kp_transport_cfg_t * cfg, void * mu,
+                      unsigned long long * counters, void * stream );
+/* Same launch replayed from a CUDA graph: the first call (or one whose
+ * arguments changed) captures the counter reset and the kernel on `stream`
+ * (non-default), later calls replay it. */
+int kp_batch_graph_launch( kp_batch_t * batch, const kp_transport_cfg_t * cfg, void * mu,
+                           unsigned long long * counters, void * stream );
+/* Autotuner: times candidate launch shapes (threads per block, event batch,
+ * grid fill) on `fraction` of every scene's packets, tallying into
+ * mu_scratch (same shape as mu), and keeps the fastest for later launches. */
+int kp_batch_autotune( kp_batch_t * batch, const kp_transport_cfg_t * cfg, double fraction,
+                       void * mu_scratch, void * stream, kp_tune_result_t * result );
+
 /* Path-replay adjoint of the peel-off image.  No reference counterpart (the
  * reference's transport is not differentiable); it differentiates the
  * solve of kp_transport_forward with the same cfg (same seed, packet ids

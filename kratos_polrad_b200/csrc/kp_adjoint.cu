@@ -53,7 +53,7 @@ template< int TALLY >
 __global__ void __launch_bounds__( FWD_THREADS, 3 )
 k_adjoint( const __grid_constant__ fwd_params_t P )
 {
-    __shared__ park_t sp;
+    __shared__ park_t<  > sp;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const int th = threadIdx.x;
@@ -72,7 +72,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
     auto begin_pass1 = [ & ](  )
     {
         const long long pid = p.pid(  );
-        emit_packet( P, pid, p );
+        emit_packet( P, pid, p, P.src[ pid % P.n_src ], P.stream );
         p.tau = sample_tau( p.rng );
         pass = 1;
         nv = 0;
@@ -129,7 +129,8 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                 phase = PH_DONE;
                 continue;
             }
-            if( ! emit_packet( P, P.pid0 + ( long long ) idx, p ) )
+            if( ! emit_packet( P, P.pid0 + ( long long ) idx, p,
+                               P.src[ ( P.pid0 + ( long long ) idx ) % P.n_src ], P.stream ) )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
                 continue;

@@ -31,11 +31,11 @@ namespace cg = cooperative_groups;
 // contribution is deposited and the walk resumes.  Peel-off rays draw no
 // random numbers, so each packet's history equals a sequential walk that
 // marches every peel-off ray at the moment of its interaction.
-template< int TALLY >
-__global__ void __launch_bounds__( FWD_THREADS, 3 )
+template< int TALLY, int NT >
+__global__ void __launch_bounds__( NT, 768 / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
-    __shared__ park_t sp;
+    __shared__ park_t< NT > sp;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     if( threadIdx.x < KP_NCOUNTERS ) sp.cnt[ threadIdx.x ] = 0;
@@ -46,6 +46,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
     bool peel = false;
     float ptau = 0;
     int pk = 0, pend = 0;
+    int si = 0;                                   // scene of a batched launch
 
     for( ;; )
     {
@@ -78,7 +79,23 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 phase = PH_DONE;
                 continue;
             }
-            if( ! emit_packet( P, P.pid0 + ( long long ) idx, p ) )
+            bool ok;
+            if( P.n_scenes > 0 )
+            {   // batched launch: scene of this packet index, then its local id
+                int lo = 0, hi = P.n_scenes;
+                while( hi - lo > 1 )
+                {
+                    const int mid = ( lo + hi ) >> 1;
+                    if( ( long long ) idx >= P.scene_prefix[ mid ] ) lo = mid; else hi = mid;
+                }
+                si = lo;
+                const long long pid = P.pid0 + ( ( long long ) idx - P.scene_prefix[ si ] );
+                ok = emit_packet( P, pid, p, P.scenes[ si ].src, P.scenes[ si ].stream );
+            }
+            else
+                ok = emit_packet( P, P.pid0 + ( long long ) idx, p,
+                                  P.src[ ( P.pid0 + ( long long ) idx ) % P.n_src ], P.stream );
+            if( ! ok )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
                 continue;
@@ -86,7 +103,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             count( sp, KP_CNT_EMITTED );
             p.tau = sample_tau( p.rng );
             phase = PH_SEGMENT;
-            const src_dev_t & s = P.src[ p.pid(  ) % P.n_src ];
+            const src_dev_t & s = P.n_scenes > 0 ? P.scenes[ si ].src : P.src[ p.pid(  ) % P.n_src ];
             if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
             {   // direct light of an isotropic, unpolarized point source
                 const int pix = image_pixel( P, p.x );
@@ -245,7 +262,8 @@ k_forward( const __grid_constant__ fwd_params_t P )
             else
             {
                 end = PK_ESCAPED;
-                if( tally_escape< TALLY >( P, p ) ) count( sp, KP_CNT_DEPOSITS );
+                if( tally_escape< TALLY >( P, ( char * ) P.mu_tally + ( size_t ) si * P.mu_scene_stride
+                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), p ) ) count( sp, KP_CNT_DEPOSITS );
             }
         }
         else if( p.n_steps >= P.max_steps )
@@ -270,13 +288,12 @@ k_forward( const __grid_constant__ fwd_params_t P )
 ////////////////////////////////////////////////////////////
 // Host side
 
-// Fills the launch parameters from the C configuration (host work only).
-void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
-                      const kp_tallies_t & t, fwd_params_t & P )
+// Fills the launch parameters that do not depend on the mesh or the
+// sources (host work only).
+void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
+                         fwd_params_t & P )
 {
     require( c.n_packets >= 0 && c.packet_offset >= 0, "negative packet count" );
-    require( c.n_sources >= 1 && c.n_sources <= MAX_SOURCES && c.sources,
-             "need 1..KP_MAX_SOURCES sources", KP_ERR_CAPACITY );
     require( c.phase == KP_PHASE_RAYLEIGH || c.phase == KP_PHASE_HG_POL, "unknown phase" );
     require( c.tally_mode == KP_TALLY_FIXED || c.tally_mode == KP_TALLY_FLOAT, "unknown tally mode" );
     require( c.fx_shift >= 0 && c.fx_shift <= 48, "fx_shift out of range" );
@@ -289,30 +306,15 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
              "bad image" );
     require( c.n_record >= 0 && ( c.n_record == 0 || t.records ), "bad records" );
     require( c.max_scatter >= 1 && c.max_steps >= 1, "caps must be positive" );
-    const auto & tab = mesh->tree->tables(  );
+    require( c.image_n == 0 || ( c.image_batch_n >= 1 && c.image_batch_n <= c.image_n ),
+             "image_batch_n must be in 1..image_n" );
+    require( c.lane_batch >= 0 && c.lane_batch <= 32, "lane_batch must be in 0..32" );
     std::memset( & P, 0, sizeof( P ) );
-    P.m = mesh->view(  );
     P.n_packets = c.n_packets;
     P.pid0 = c.packet_offset;
     P.seed = c.seed;
     P.stream = c.stream_id;
     P.ph = phys::phase_t { c.phase, c.hg_g, c.pol_max };
-    P.n_src = c.n_sources;
-    for( int k = 0; k < c.n_sources; ++ k )
-    {
-        const auto & s = c.sources[ k ];
-        require( s.kind == KP_SOURCE_POINT || s.kind == KP_SOURCE_PLANE_BASE, "unknown source" );
-        require( s.emit == KP_EMIT_ISOTROPIC || s.emit == KP_EMIT_UP_UNIFORM, "unknown emission" );
-        auto & d = P.src[ k ];
-        d.kind = s.kind;
-        d.emit = s.emit;
-        for( int a = 0; a < 3; ++ a ) d.pos[ a ] = s.pos[ a ];
-        d.ib = 0;
-        d.cell[ 0 ] = d.cell[ 1 ] = d.cell[ 2 ] = 0;
-        if( s.kind == KP_SOURCE_POINT )
-            require( mesh->tree->locate( s.pos, d.ib, d.cell ), "source outside the mesh",
-                     KP_ERR_CONFIG );
-    }
     P.n_mu = c.n_mu_bins;
     P.mu_lo = c.mu_lo;
     P.mu_inv_w = c.n_mu_bins > 0 ? ( float ) ( c.n_mu_bins / ( ( double ) c.mu_hi - c.mu_lo ) ) : 0.f;
@@ -339,20 +341,16 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
         P.eh_d[ a ] = eh[ a ];
         P.inv_o[ a ] = o[ a ] != 0.0f ? 1.0 / ( double ) o[ a ] : 0.0;
         P.img_c[ a ] = c.image_center[ a ];
-        P.lk_inv[ a ] = tab.lookup_n[ a ] / tab.l_box_d[ a ];
     }
     P.img_inv_pix = c.image_n > 0 ? c.image_n / ( 2.0 * c.image_half_width ) : 0.0;
     P.tau_cut = c.tau_peel_max > 0 ? c.tau_peel_max : 40.0f;
     P.fx_scale = std::ldexp( 1.0, c.fx_shift );
     P.n_batch = c.n_batches;
-    require( c.image_n == 0 || ( c.image_batch_n >= 1 && c.image_batch_n <= c.image_n ),
-             "image_batch_n must be in 1..image_n" );
     P.img_bn = c.image_batch_n >= 1 ? c.image_batch_n : 1;
     P.w_min = c.w_min;
     P.rr_survive = c.rr_survive > 0 ? c.rr_survive : 0.1f;
     P.max_scatter = c.max_scatter;
     P.max_steps = std::min< long long >( c.max_steps, 0x7fffffff );
-    require( c.lane_batch >= 0 && c.lane_batch <= 32, "lane_batch must be in 0..32" );
     P.ev_batch = c.lane_batch > 0 ? c.lane_batch : 6;
     P.mu_tally = t.mu;
     P.image = t.image;
@@ -360,6 +358,38 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
     P.counters = t.counters;
     P.records = t.records;
     P.n_record = c.n_record;
+}
+
+// Converts one C source to its device form; point sources are located in
+// `mesh` (block id, cell).
+void make_source( kp_mesh_t * mesh, const kp_source_t & s, src_dev_t & d )
+{
+    require( s.kind == KP_SOURCE_POINT || s.kind == KP_SOURCE_PLANE_BASE, "unknown source" );
+    require( s.emit == KP_EMIT_ISOTROPIC || s.emit == KP_EMIT_UP_UNIFORM, "unknown emission" );
+    d.kind = s.kind;
+    d.emit = s.emit;
+    for( int a = 0; a < 3; ++ a ) d.pos[ a ] = s.pos[ a ];
+    d.ib = 0;
+    d.cell[ 0 ] = d.cell[ 1 ] = d.cell[ 2 ] = 0;
+    if( s.kind == KP_SOURCE_POINT )
+        require( mesh->tree->locate( s.pos, d.ib, d.cell ), "source outside the mesh",
+                 KP_ERR_CONFIG );
+}
+
+// Fills the launch parameters of a single-mesh solve (host work only).
+void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
+                      const kp_tallies_t & t, fwd_params_t & P )
+{
+    require( c.n_sources >= 1 && c.n_sources <= MAX_SOURCES && c.sources,
+             "need 1..KP_MAX_SOURCES sources", KP_ERR_CAPACITY );
+    fill_common_params( c, t, P );
+    const auto & tab = mesh->tree->tables(  );
+    P.m = mesh->view(  );
+    P.n_src = c.n_sources;
+    for( int k = 0; k < c.n_sources; ++ k )
+        make_source( mesh, c.sources[ k ], P.src[ k ] );
+    for( int a = 0; a < 3; ++ a )
+        P.lk_inv[ a ] = tab.lookup_n[ a ] / tab.l_box_d[ a ];
 }
 
 int persistent_grid( const void * kernel, int threads )
@@ -371,21 +401,33 @@ int persistent_grid( const void * kernel, int threads )
     return n_sm * std::max( per_sm, 1 );
 }
 
-void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s )
+template< int NT >
+void launch_forward_nt( const fwd_params_t & P, int tally_mode, cudaStream_t s, int grid_pct )
 {
-    if( P.n_packets == 0 ) return;
-    const int threads = FWD_THREADS;
-    const void * k = tally_mode == KP_TALLY_FIXED ? ( const void * ) k_forward< KP_TALLY_FIXED >
-                                                  : ( const void * ) k_forward< KP_TALLY_FLOAT >;
-    long long grid = persistent_grid( k, threads );
-    grid = std::min< long long >( grid, ( P.n_packets + threads - 1 ) / threads );
+    const void * k = tally_mode == KP_TALLY_FIXED ? ( const void * ) k_forward< KP_TALLY_FIXED, NT >
+                                                  : ( const void * ) k_forward< KP_TALLY_FLOAT, NT >;
+    long long grid = persistent_grid( k, NT );
+    grid = std::max< long long >( 1, grid * grid_pct / 100 );
+    grid = std::min< long long >( grid, ( P.n_packets + NT - 1 ) / NT );
     KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
     // whole warps only: the scheduler ballots over full warps
     if( tally_mode == KP_TALLY_FIXED )
-        k_forward< KP_TALLY_FIXED ><<< ( unsigned ) grid, threads, 0, s >>>( P );
+        k_forward< KP_TALLY_FIXED, NT ><<< ( unsigned ) grid, NT, 0, s >>>( P );
     else
-        k_forward< KP_TALLY_FLOAT ><<< ( unsigned ) grid, threads, 0, s >>>( P );
+        k_forward< KP_TALLY_FLOAT, NT ><<< ( unsigned ) grid, NT, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
+}
+
+// Launches the forward kernel with `threads` per block (128 or 256) and a
+// persistent grid of grid_pct percent of the resident-block capacity.
+void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int threads,
+                     int grid_pct )
+{
+    if( P.n_packets == 0 ) return;
+    if( threads == 128 )
+        launch_forward_nt< 128 >( P, tally_mode, s, grid_pct );
+    else
+        launch_forward_nt< 256 >( P, tally_mode, s, grid_pct );
 }
 
 }   // namespace kp
@@ -400,7 +442,7 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = mesh->workspace(  );
-        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream );
+        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
     } );
 }
 
@@ -463,6 +505,6 @@ extern "C" int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transpor
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = static_cast< unsigned long long * >( kp::noalloc_scratch(  ) );
-        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream );
+        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
     } );
 }

@@ -31,6 +31,14 @@ struct src_dev_t
     int    emit;
 };
 
+// One scene of a batched launch (all scenes share one concatenated mesh).
+struct scene_dev_t
+{
+    src_dev_t src;
+    uint32_t  stream;          // RNG key word 2 of the scene's packets
+    uint32_t  pad;
+};
+
 // Everything a transport launch reads, passed by value.
 struct fwd_params_t
 {
@@ -68,6 +76,11 @@ struct fwd_params_t
     void      * g_len;             // path-length term per cell
     void      * g_int;             // interaction term per cell (sigma_sca only)
     double      g_scale;           // fixed point scale of the gradient tallies
+    // batched launch only (n_scenes > 0)
+    int         n_scenes;
+    const long long   * scene_prefix;   // [n_scenes + 1] packet index prefix
+    const scene_dev_t * scenes;         // [n_scenes]
+    long long   mu_scene_stride;        // mu tally elements per scene
     src_dev_t   src[ MAX_SOURCES ];
 };
 
@@ -290,7 +303,8 @@ __device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel
 // Escape tally: mu = d.z bins, Stokes in the meridian frame (Q > 0 in the
 // plane of d and +z).
 template< int TALLY >
-__device__ __forceinline__ bool tally_escape( const fwd_params_t & P, const packet_t & p )
+__device__ __forceinline__ bool tally_escape( const fwd_params_t & P, void * mu_base,
+                                              const packet_t & p )
 {
     if( P.n_mu <= 0 ) return false;
     const float fb = floorf( __fmul_rn( __fsub_rn( p.d.z, P.mu_lo ), P.mu_inv_w ) );
@@ -303,10 +317,10 @@ __device__ __forceinline__ bool tally_escape( const fwd_params_t & P, const pack
     phys::rotate( q, u, c2, s2 );
     const int batch = ( int ) ( p.pid(  ) % P.n_batch );
     const size_t i = ( ( size_t ) batch * P.n_mu + bin ) * 4;
-    add_tally< TALLY >( P.mu_tally, i + 0, p.w, P.fx_scale );
-    add_tally< TALLY >( P.mu_tally, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
-    add_tally< TALLY >( P.mu_tally, i + 2, __fmul_rn( p.w, u ), P.fx_scale );
-    add_tally< TALLY >( P.mu_tally, i + 3, __fmul_rn( p.w, p.S.v ), P.fx_scale );
+    add_tally< TALLY >( mu_base, i + 0, p.w, P.fx_scale );
+    add_tally< TALLY >( mu_base, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
+    add_tally< TALLY >( mu_base, i + 2, __fmul_rn( p.w, u ), P.fx_scale );
+    add_tally< TALLY >( mu_base, i + 3, __fmul_rn( p.w, p.S.v ), P.fx_scale );
     return true;
 }
 
@@ -335,12 +349,12 @@ __device__ __forceinline__ phys::v3 sample_emission_dir( phys::rng_t & rng, int 
     return phys::dir_from( mu, __fdiv_rn( a, rr ), __fdiv_rn( b, rr ) );
 }
 
-// Creates packet `pid` (global id) at its source.  Returns false if the
-// source position lies outside the mesh.
-__device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long pid, packet_t & p )
+// Creates packet `pid` at source `s` with RNG key (seed, stream).  Returns
+// false if the source position lies outside the mesh.
+__device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long pid, packet_t & p,
+                                             const src_dev_t & s, uint32_t stream )
 {
-    p.rng = phys::rng_t { P.seed, P.stream, ( uint32_t ) pid, ( uint32_t ) ( pid >> 32 ), 0u };
-    const src_dev_t & s = P.src[ pid % P.n_src ];
+    p.rng = phys::rng_t { P.seed, stream, ( uint32_t ) pid, ( uint32_t ) ( pid >> 32 ), 0u };
     if( s.kind == KP_SOURCE_POINT )
     {
         #pragma unroll
@@ -415,32 +429,35 @@ constexpr int FWD_THREADS = 256;
 // Rarely touched per-lane state kept in shared memory (structure of arrays):
 // the parked walk position while a peel-off ray runs, and the pending
 // peel-off contribution.
+template< int NT = FWD_THREADS >
 struct park_t
 {
-    double x[ 3 ][ FWD_THREADS ];
-    int    c[ 3 ][ FWD_THREADS ];
-    int    b[ FWD_THREADS ];
-    float  w[ FWD_THREADS ], I[ FWD_THREADS ], Q[ FWD_THREADS ], U[ FWD_THREADS ],
-           V[ FWD_THREADS ];
-    int    pix[ FWD_THREADS ];
+    double x[ 3 ][ NT ];
+    int    c[ 3 ][ NT ];
+    int    b[ NT ];
+    float  w[ NT ], I[ NT ], Q[ NT ], U[ NT ], V[ NT ];
+    int    pix[ NT ];
     unsigned long long cnt[ KP_NCOUNTERS ];
 };
 
-__device__ __forceinline__ void park_walk( park_t & sp, const packet_t & p )
+template< class SP >
+__device__ __forceinline__ void park_walk( SP & sp, const packet_t & p )
 {
     const int t = threadIdx.x;
     #pragma unroll
     for( int a = 0; a < 3; ++ a ) { sp.x[ a ][ t ] = p.x[ a ]; sp.c[ a ][ t ] = p.c[ a ]; }
     sp.b[ t ] = p.b;
 }
-__device__ __forceinline__ void unpark_walk( const park_t & sp, packet_t & p )
+template< class SP >
+__device__ __forceinline__ void unpark_walk( const SP & sp, packet_t & p )
 {
     const int t = threadIdx.x;
     #pragma unroll
     for( int a = 0; a < 3; ++ a ) { p.x[ a ] = sp.x[ a ][ t ]; p.c[ a ] = sp.c[ a ][ t ]; }
     p.b = sp.b[ t ];
 }
-__device__ __forceinline__ void count( park_t & sp, int k, unsigned v = 1u )
+template< class SP >
+__device__ __forceinline__ void count( SP & sp, int k, unsigned v = 1u )
 {
     atomicAdd( sp.cnt + k, ( unsigned long long ) v );
 }
@@ -448,6 +465,11 @@ __device__ __forceinline__ void count( park_t & sp, int k, unsigned v = 1u )
 // Host helpers shared by the transport entry points (kp_transport.cu).
 void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
                       const kp_tallies_t & t, fwd_params_t & P );
+void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
+                         fwd_params_t & P );
+void make_source( kp_mesh_t * mesh, const kp_source_t & s, src_dev_t & d );
 int  persistent_grid( const void * kernel, int threads );
+void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int threads,
+                     int grid_pct );
 
 }   // namespace kp

@@ -114,3 +114,30 @@ def batch_rel_error(batch_images: np.ndarray) -> tuple[float, float]:
     tot = tangential_polarization(batch_images.sum(0))
     err = p.std(ddof=1) / math.sqrt(len(p))
     return tot, (err / abs(tot) if tot != 0 else float("inf"))
+
+
+def batched_cubes(n_scenes=256, sides=(16, 32, 48, 64, 96), tau=(0.1, 20.0), albedo=(0.3, 1.0),
+                  packets=(100_000, 1_000_000), seed=3, n_mu=32, block=16):
+    """Independent uniform cubes for a batched solve: side drawn uniformly from
+    ``sides`` (cells), centre-to-face extinction depth log-uniform in ``tau``,
+    albedo uniform in ``albedo`` (seed ``seed``), a central isotropic point
+    source, and packets in proportion to tau, clipped to ``packets``.
+    Returns (scenes, cfg): scenes is a list of (mesh, sigma2, n_packets,
+    stream_id, Source); cfg the common TransportConfig (32-bin mu tallies)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        side = int(rng.choice(sides))
+        t = float(np.exp(rng.uniform(np.log(tau[0]), np.log(tau[1]))))
+        alb = float(rng.uniform(*albedo))
+        n = int(np.clip(round(packets[1] * t / tau[1]), packets[0], packets[1]))
+        mesh = Mesh(MeshConfig((0, 0, 0), (1, 1, 1), (side,) * 3, (block,) * 3, (False,) * 3))
+        ext = 2.0 * t                      # unit box: centre-to-face depth t
+        sigma2 = np.empty((mesh.n_cells, 2), np.float32)
+        sigma2[:, 0] = ext * alb
+        sigma2[:, 1] = ext * (1.0 - alb)
+        out.append((mesh, sigma2, n, k, Source(SOURCE_POINT, EMIT_ISOTROPIC, (0.5, 0.5, 0.5))))
+    cfg = TransportConfig(n_packets=0, sources=[Source()], seed=seed, phase=PHASE_RAYLEIGH,
+                          n_mu_bins=n_mu, mu_lo=-1.0, mu_hi=1.0, n_batches=32, w_min=0.01,
+                          fx_shift=32)
+    return out, cfg
