@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--packets", type=float, default=1e7)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="clump", choices=["clump", "batched"])
+    p.add_argument("--workload", default="clump", choices=["clump", "batched", "diff", "large"])
     return p.parse_args()
 
 
@@ -274,10 +274,118 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed(fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def run_diff(args):
+    """Differentiable workload: 96^3 lognormal field (std of ln rho 1.0,
+    k^-11/3, seed 4), albedo 0.9, Rayleigh, 64x64 Q/U image at 60 deg; loss =
+    L2 distance (Q, U) to the image of the field perturbed by 5% Gaussian
+    noise.  Times the forward and the path-replay gradient, then checks the
+    gradient against common-random-number central differences on 32 cells
+    drawn at random among the 2000 with the largest |dL/dsigma_sca|."""
+    import numpy as np
+    import torch
+    from kratos_polrad_b200 import scenes
+    from kratos_polrad_b200.adjoint import TransportImage
+    n_pk = int(args.packets) if args.packets != 1e7 else 100_000_000
+    mesh, sig, cfg, _ = scenes.lognormal_cube(n_packets=n_pk)
+    rng = np.random.default_rng(4)
+    sig_t = (sig * (1 + 0.05 * rng.normal(size=sig.shape))).astype(np.float32)
+    dev = torch.device("cuda")
+    with torch.no_grad():
+        target = TransportImage.apply(torch.tensor(sig_t[:, 0], device=dev, dtype=torch.float64),
+                                      torch.tensor(sig_t[:, 1], device=dev, dtype=torch.float64),
+                                      mesh, cfg)
+
+    def loss_of(s):
+        img = TransportImage.apply(s[:, 0], s[:, 1], mesh, cfg)
+        return ((img - target)[..., 1:3] ** 2).sum()
+
+    s = torch.tensor(sig, device=dev, dtype=torch.float64)
+    for _ in range(max(1, args.warmup)):
+        x = s.clone().requires_grad_(True)
+        loss_of(x).backward()
+    x = s.clone().requires_grad_(True)
+    L, t_fwd = _timed(lambda: loss_of(x))
+    _, t_bwd = _timed(lambda: L.backward())
+    g = x.grad[:, 0].detach().cpu().numpy()
+    top = np.argsort(-np.abs(g))[:2000]
+    cells = rng.choice(top, 32, replace=False)
+    rel = []
+    with torch.no_grad():
+        for c in cells:
+            h = 0.1 * float(sig[c, 0])
+            sp, sm = s.clone(), s.clone()
+            sp[c, 0] += h
+            sm[c, 0] -= h
+            fd = (float(loss_of(sp)) - float(loss_of(sm))) / (2 * h)
+            rel.append(abs(fd - g[c]) / max(abs(g[c]), 1e-300))
+    rel = np.array(rel)
+    line = {"metric": "path-replay gradient, 96^3 lognormal, Q/U image loss", "unit": "ms",
+            "value": t_bwd, "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": "lognormal_96_diff", "packets": n_pk, "cells": mesh.n_cells},
+            "forward_ms": t_fwd, "gradient_ms": t_bwd, "gradient_cost_vs_forward": t_bwd / t_fwd,
+            "fd_check": {"cells": 32, "median_rel_diff": float(np.median(rel)),
+                         "frac_within_2pct": float(np.mean(rel < 0.02)),
+                         "frac_within_10pct": float(np.mean(rel < 0.10)),
+                         "max_rel_diff": float(rel.max()), "h": "10% of sigma_sca(cell)",
+                         "note": "common random numbers: same packets for both sides"}}
+    print(json.dumps(line), flush=True)
+
+
+def run_large(args):
+    """Large workload: 256^3 root, 3 levels on a lognormal field (std of ln
+    rho 1.5, seed 5; ~2e7 cells, 166 MB of coefficients: beyond L2), HG g=0.6
+    with polarization, 64 random point sources, 256^2 IQUV image; one forward
+    solve and one path-replay gradient of `--packets` packets (default 1e9)."""
+    import torch
+    from kratos_polrad_b200 import scenes
+    from kratos_polrad_b200.adjoint import adjoint
+    from kratos_polrad_b200.transport import Tallies, forward
+    n_pk = int(args.packets) if args.packets != 1e7 else 1_000_000_000
+    mesh, sig, cfg = scenes.large_amr(n_packets=n_pk)
+    mesh.set_sigma(sig)
+    warm = dataclasses.replace(cfg, n_packets=min(n_pk, 2_000_000))
+    forward(mesh, warm)
+    torch.cuda.synchronize()
+    tal = Tallies(cfg)
+    with ClockSampler(0) as clk:
+        _, t_fwd = _timed(lambda: forward(mesh, cfg, tal))
+    c = tal.counts()
+    p_tan, rel = scenes.batch_rel_error(tal.image_batch.cpu().numpy() * tal.scale())
+    g_img = torch.randn((cfg.image_n, cfg.image_n, 4), device="cuda",
+                        generator=torch.Generator(device="cuda").manual_seed(5))
+    acnt = torch.zeros(10, dtype=torch.int64, device="cuda")
+    _, t_adj = _timed(lambda: adjoint(mesh, cfg, g_img, 24, acnt))
+    ac = acnt.cpu().numpy()
+    line = {"metric": "packet-steps/s, 3-level AMR lognormal, 64 sources", "unit": UNIT,
+            "value": (c["steps"] + c["peel_steps"]) / (t_fwd / 1e3), "higher_is_better": True,
+            "n_gpus": 1, "config": {"workload": "large_amr_3level", "packets": n_pk,
+                                    "blocks": mesh.n_blocks, "cells": mesh.n_cells,
+                                    "sigma_MB": sig.nbytes / 1e6, "image": cfg.image_n},
+            "forward_ms": t_fwd, "counts": c, "pol_tangential": p_tan, "pol_rel_std_err": rel,
+            "adjoint_ms": t_adj, "adjoint_cost_vs_forward": t_adj / t_fwd,
+            "adjoint_packet_steps_per_s": float(ac[0] + ac[1]) / (t_adj / 1e3),
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "diff":
+        return run_diff(args)
+    if args.workload == "large":
+        return run_large(args)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))

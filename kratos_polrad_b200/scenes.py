@@ -141,3 +141,90 @@ def batched_cubes(n_scenes=256, sides=(16, 32, 48, 64, 96), tau=(0.1, 20.0), alb
                           n_mu_bins=n_mu, mu_lo=-1.0, mu_hi=1.0, n_batches=32, w_min=0.01,
                           fx_shift=32)
     return out, cfg
+
+
+def lognormal_field(n, sigma_ln, slope=-11.0 / 3.0, seed=4):
+    """Periodic lognormal density on an n^3 grid: exp of a Gaussian random
+    field with power spectrum P(k) ~ k^slope (FFT-filtered white noise,
+    seed), scaled to std(ln rho) = sigma_ln and mean(rho) = 1.  Axis order
+    [z, y, x]."""
+    rng = np.random.default_rng(seed)
+    w = rng.normal(size=(n, n, n))
+    k = np.fft.fftfreq(n) * n
+    kr = np.fft.rfftfreq(n) * n
+    K = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + kr[None, None, :] ** 2)
+    amp = np.where(K > 0, K, 1.0) ** (slope / 2.0)
+    amp[0, 0, 0] = 0.0
+    g = np.fft.irfftn(np.fft.rfftn(w) * amp, s=(n, n, n))
+    g = (g - g.mean()) / g.std()
+    rho = np.exp(sigma_ln * g)
+    return rho / rho.mean()
+
+
+def _sample(grid, x):
+    """Nearest-cell sample of a periodic [z, y, x] grid on the unit box at points x [..., 3]."""
+    n = grid.shape[0]
+    i = np.clip((np.asarray(x) * n).astype(np.int64), 0, n - 1)
+    return grid[i[..., 2], i[..., 1], i[..., 0]]
+
+
+def lognormal_cube(n_packets=1_000_000, n=96, sigma_ln=1.0, albedo=0.9, tau_mean=2.0, seed=4,
+                   image_n=64, inclination=60.0):
+    """Uniform n^3 grid (16^3 blocks) holding a lognormal density (std of
+    ln rho sigma_ln, k^-11/3 spectrum, seed); sigma_sca proportional to rho with
+    the given albedo; mean centre-to-face extinction depth tau_mean; Rayleigh
+    matrix; central isotropic point source; n x n peel-off image at the given
+    inclination.  Returns (mesh, sigma2, cfg, rho_grid)."""
+    rho = lognormal_field(n, sigma_ln, seed=seed)
+    mesh = Mesh(MeshConfig((0, 0, 0), (1, 1, 1), (n,) * 3, (16,) * 3, (False,) * 3))
+    r = _sample(rho, cell_centers(mesh))
+    ext = 2.0 * tau_mean * r
+    sigma2 = np.stack([albedo * ext, (1.0 - albedo) * ext], 1).astype(np.float32)
+    cfg = TransportConfig(n_packets=n_packets, seed=seed,
+                          sources=[Source(SOURCE_POINT, EMIT_ISOTROPIC, (0.5, 0.5, 0.5))],
+                          phase=PHASE_RAYLEIGH, image_n=image_n, inclination_deg=inclination,
+                          image_center=(0.5, 0.5, 0.5), image_half_width=0.75, image_batch_n=8,
+                          n_batches=32, w_min=0.01, fx_shift=32)
+    return mesh, sigma2, cfg, rho
+
+
+def large_amr(n_packets=1_000_000_000, n_root=256, block=16, sigma_ln=1.5, levels=3, seed=5,
+              target_cells=20_000_000, n_sources=64, image_n=256, tau_mean=2.0):
+    """Large AMR scene: root n_root^3 in block^3, refined up to `levels`
+    levels on a lognormal density (std of ln rho sigma_ln, k^-11/3, seed)
+    with thresholds chosen so that the mesh holds about target_cells cells;
+    HG (g = 0.6) with a Rayleigh-like polarization (peak 0.5 at 90 deg); albedo
+    0.9; n_sources isotropic point sources placed uniformly at random;
+    image_n^2 IQUV peel-off.  Returns (mesh, sigma2, cfg)."""
+    rho = lognormal_field(n_root, sigma_ln, seed=seed)
+    nb = n_root // block
+    bmax = rho.reshape(nb, block, nb, block, nb, block).max(axis=(1, 3, 5))
+    order = np.sort(bmax.ravel())[::-1]
+    # choose the level-1 and level-2 block counts so that cells ~ target:
+    # each refined block adds 7 blocks per level
+    extra = max(0, target_cells // (block ** 3) - nb ** 3)
+    n1 = min(len(order) // 4, max(1, int(extra / 7 * 0.7)))
+    n2 = max(1, int(extra / 49 * 0.3 / 1.0)) if levels >= 3 else 0
+    n2 = min(n2, n1 // 2)
+    t1 = order[n1 - 1]
+    t2 = order[n2 - 1] if n2 else np.inf
+    boxes = []
+    h = 1.0 / nb
+    for lvl, thr in ((1, t1), (2, t2)):
+        if lvl >= levels or not np.isfinite(thr):
+            continue
+        for kz, ky, kx in zip(*np.nonzero(bmax >= thr)):
+            lo = tuple((np.array([kx, ky, kz]) + 0.25) * h)
+            hi = tuple((np.array([kx, ky, kz]) + 0.75) * h)
+            boxes.append(RefineRegion(lvl, lo, hi))
+    mesh = Mesh(MeshConfig((0, 0, 0), (1, 1, 1), (n_root,) * 3, (block,) * 3, (False,) * 3, boxes))
+    r = _sample(rho, cell_centers(mesh))
+    ext = 2.0 * tau_mean * r
+    sigma2 = np.stack([0.9 * ext, 0.1 * ext], 1).astype(np.float32)
+    rng = np.random.default_rng(seed)
+    srcs = [Source(SOURCE_POINT, EMIT_ISOTROPIC, tuple(p)) for p in rng.uniform(0.05, 0.95, (n_sources, 3))]
+    cfg = TransportConfig(n_packets=n_packets, seed=seed, sources=srcs, phase=PHASE_HG_POL,
+                          hg_g=0.6, pol_max=0.5, image_n=image_n, inclination_deg=60.0,
+                          image_center=(0.5, 0.5, 0.5), image_half_width=0.75, image_batch_n=8,
+                          n_batches=32, w_min=0.01, fx_shift=30)
+    return mesh, sigma2, cfg
