@@ -656,9 +656,21 @@ void kpo_scatter_sample( long n, uint32_t seed, int kind, float g, float pmax,
 /* Path-replay adjoint restatement (same estimator and operation order as  */
 /* the device kernel; sequential packets; int64 gradient tallies).         */
 
+/* Optional per-cell sum of |term| and count of gradient deposits (both
+ * tallies): what a float-atomic accumulation's rounding error is bounded by.
+ * Set by kpo_set_abs_sink; process-global, for sequential test use. */
+static double * s_abs_sink = NULL;
+
+void kpo_set_abs_sink( double * sink ) { s_abs_sink = sink; }
+
 static void tgadd( long long * base, long i, double v, double sc )
 {
     base[ i ] += llrint( v * sc );
+    if( s_abs_sink )
+    {
+        s_abs_sink[ 2 * i ] += fabs( v );
+        s_abs_sink[ 2 * i + 1 ] += 1.0;
+    }
 }
 
 static float tscore( const float * g, int pix, float I, float Q, float U, float V )

@@ -132,6 +132,10 @@ int kpo_adjoint( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
                  const int * lookup_n, const kpo_cfg_t * c, const float * adj_img,
                  int grad_shift, long long * g_len, long long * g_int,
                  unsigned long long * counters );
+/* While non-null, every adjoint deposit of value v into cell i also adds
+ * |v| to sink[2 i] and 1 to sink[2 i + 1] (2 n_cells doubles); NULL switches
+ * it off. */
+void kpo_set_abs_sink( double * sink );
 #ifdef __cplusplus
 }
 #endif

@@ -193,8 +193,11 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
     return out
 
 
-def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, grad_shift=24):
-    """Restated path-replay adjoint; returns int64 (g_len, g_int), counters."""
+def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, grad_shift=24,
+            abs_sum=False):
+    """Restated path-replay adjoint; returns int64 (g_len, g_int), counters,
+    and with ``abs_sum`` also the per-cell sum of |deposit| over both
+    tallies and the per-cell deposit count ([n_cells, 2] float64)."""
     src = (_Source * max(1, len(cfg.sources)))()
     for k, s in enumerate(cfg.sources):
         src[k].kind, src[k].emit = int(s.kind), int(s.emit)
@@ -224,8 +227,14 @@ def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, g
     L = lib()
     L.kpo_adjoint.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int] + [ctypes.c_void_p] * 3
     p = lambda a: ctypes.c_void_p(a.ctypes.data)
-    st = L.kpo_adjoint(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c), p(adj),
-                       grad_shift, p(g_len), p(g_int), p(cnt))
+    sink = np.zeros((n_cells, 2), np.float64) if abs_sum else None
+    L.kpo_set_abs_sink.argtypes = [ctypes.c_void_p]
+    L.kpo_set_abs_sink(p(sink) if abs_sum else None)
+    try:
+        st = L.kpo_adjoint(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
+                           p(adj), grad_shift, p(g_len), p(g_int), p(cnt))
+    finally:
+        L.kpo_set_abs_sink(None)
     if st != 0:
         raise RuntimeError(f"kpo_adjoint failed ({st})")
-    return g_len, g_int, cnt
+    return (g_len, g_int, cnt, sink) if abs_sum else (g_len, g_int, cnt)

@@ -40,13 +40,23 @@ def test_adjoint_float_mode_close():
                        dtype=torch.float32, device="cuda")
     a_s, a_a = gradients(mesh, t, adj, 24)
     b_s, b_a = gradients(mesh, dataclasses.replace(t, tally_mode=TALLY_FLOAT), adj, 24)
-    # float atomics vs int64 sums of 2^-24-rounded deposits: both approximate
-    # the exact sum of thousands of terms of either sign per cell; per cell
-    # within 1e-3 of the field's peak, and 2e-3 relative in L2
+    # Per cell, the float32 atomic sum of n deposits v_k (each first rounded to
+    # float) differs from the exact sum by at most (gamma_n + u) * sum|v_k|,
+    # gamma_n = n u / (1 - n u), u = 2^-24, in any order; the int64 sum of
+    # round(v_k 2^24) differs by at most n 2^-25.  Cells crossed by every
+    # packet (around the source) sum thousands of terms that nearly cancel,
+    # so the bound is taken per cell from the oracle's |v| sums and counts.
+    rl, ri, _, S = run_oracle_adjoint(mesh, sig, t, adj.cpu().numpy(), 24, abs_sum=True)
+    np.testing.assert_array_equal(a_a.cpu().numpy(), rl * 2.0 ** -24)
+    A, n = S[:, 0], S[:, 1]
+    u = 2.0 ** -24
+    tol = (n * u / (1 - n * u) + u) * A + n * 2.0 ** -25
     for x, y in ((a_s, b_s), (a_a, b_a)):
         x, y = x.cpu().numpy(), y.cpu().numpy()
-        np.testing.assert_allclose(y, x, rtol=0, atol=1e-3 * np.abs(x).max())
-        assert np.linalg.norm(y - x) < 2e-3 * np.linalg.norm(x)
+        err = np.abs(y - x)
+        assert np.all(err <= tol), (err - tol).max()
+        # and in all but a few heavy cells, far inside the peak's 1e-3
+        assert np.mean(err > 1e-3 * np.abs(x).max()) < 1e-3
 
 
 def test_autograd_backward_is_the_adjoint():

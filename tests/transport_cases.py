@@ -92,6 +92,6 @@ def oracle_inputs(mesh, t):
     return tab, grid, n, cells
 
 
-def run_oracle_adjoint(mesh, sig, t, adj_img, grad_shift=24):
+def run_oracle_adjoint(mesh, sig, t, adj_img, grad_shift=24, abs_sum=False):
     tab, grid, n, cells = oracle_inputs(mesh, t)
-    return port.adjoint(tab, sig, grid, n, t, cells, adj_img, grad_shift)
+    return port.adjoint(tab, sig, grid, n, t, cells, adj_img, grad_shift, abs_sum)
