@@ -206,12 +206,18 @@ def run_batched(args):
     {16,32,48,64,96}, tau log-uniform [0.1,20], albedo uniform [0.3,1], seed 3,
     1e5-1e6 packets in proportion to tau, 32-bin mu tallies) in one autotuned,
     graph-replayed persistent launch, against 256 sequential single-scene
-    launches of the same packets (same tallies, bit for bit)."""
+    launches of the same packets (same tallies, bit for bit).  Under torchrun
+    each rank solves a contiguous range of the scenes (no collective in the
+    data path); the per-scene tallies are gathered on rank 0."""
     import torch
-    from kratos_polrad_b200 import scenes
+    import torch.distributed as dist
+    from kratos_polrad_b200 import scenes, shard
     from kratos_polrad_b200.batch import Batch
     from kratos_polrad_b200.transport import Tallies, forward
-    sc, cfg = scenes.batched_cubes()
+    rank, world, _ = _init_ranks()
+    sc_all, cfg = scenes.batched_cubes()
+    lo, hi = shard.scene_range(len(sc_all), rank, world)
+    sc = sc_all[lo:hi]
     for mesh, sig, *_ in sc:
         mesh.set_sigma(sig)
     b = Batch([(m, n, sid, src) for m, _, n, sid, src in sc])
@@ -225,7 +231,9 @@ def run_batched(args):
             b.forward(cfg, mu=mu, graph=True, stream=s.cuda_stream)
     s.synchronize()
     times = []
-    with ClockSampler(0) as clk:
+    if world > 1:
+        dist.barrier()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         for k in range(args.steps):
             mu.zero_()
             cnt.zero_()
@@ -236,9 +244,15 @@ def run_batched(args):
                 e1.record(s)
             s.synchronize()
             times.append(e0.elapsed_time(e1))
+    if world > 1:
+        dist.barrier()
+    red = torch.tensor([statistics.mean(times)], dtype=torch.float64, device="cuda")
+    shard_max(red)
+    batched_ms = float(red.item())
+    shard.reduce_tallies([cnt])
     c = cnt.cpu().numpy()
     steps = int(c[0] + c[1])
-    batched_ms = statistics.mean(times)
+    mu_all = shard.gather_scene_tallies(mu, len(sc_all), rank, world)
     # sequential plain launches of the same scenes
     seq_mu = torch.zeros_like(mu)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -255,23 +269,64 @@ def run_batched(args):
         forward(mesh, cc, tl)
     e1.record()
     torch.cuda.synchronize()
-    seq_ms = e0.elapsed_time(e1)
+    red = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    shard_max(red)
+    seq_ms = float(red.item())
     for k, tl in enumerate(tals):
         seq_mu[k] = tl.mu
-    same = bool(torch.equal(seq_mu, mu))
+    differs = torch.tensor([0 if torch.equal(seq_mu, mu) else 1], dtype=torch.int64, device="cuda")
+    shard_max(differs)                                   # any rank whose scenes differ
+    same = bool(differs.item() == 0)
+    if rank != 0:
+        _finish_ranks(world)
+        return
     line = {"metric": "packet-steps/s, 256-scene batched solve", "value": steps / (batched_ms / 1e3),
-            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 positions / f32 Stokes", "data": "synthetic",
-            "config": {"workload": "batched_cubes_256", "scenes": len(sc),
-                       "packets": int(sum(n for _, _, n, _, _ in sc)),
-                       "cells": int(sum(m.n_cells for m, *_ in sc)), "tallies": "int64 fixed point",
-                       "launch": "one persistent launch replayed from a CUDA graph"},
+            "config": {"workload": "batched_cubes_256", "scenes": len(sc_all),
+                       "packets": int(sum(n for _, _, n, _, _ in sc_all)),
+                       "cells": int(sum(m.n_cells for m, *_ in sc_all)),
+                       "tallies": "int64 fixed point",
+                       "launch": "one persistent launch replayed from a CUDA graph",
+                       "split": "contiguous scene ranges per rank, tallies gathered on rank 0"},
+            "gathered_scenes": int(mu_all.shape[0]),
             "autotune": tune, "sequential_ms": seq_ms,
             "sequential_value": steps / (seq_ms / 1e3),
             "batched_over_sequential": seq_ms / batched_ms,
             "tallies_identical_to_sequential": same, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
+    _finish_ranks(world)
+
+
+def _init_ranks():
+    """(rank, world, local rank); initialises NCCL under torchrun."""
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def _finish_ranks(world):
+    import torch.distributed as dist
+    if world > 1 and dist.is_initialized():
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def shard_max(t):
+    """In-place max over the ranks (no-op with one rank)."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t
 
 
 def _timed(fn):
@@ -447,38 +502,28 @@ def main():
         return run_diff(args)
     if args.workload == "large":
         return run_large(args)
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":     # host cores only: rank 0 runs, the others exit
+        run_reference(args, int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)))
+        return
     import torch
     import torch.distributed as dist
-    if world > 1:
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        if world > 1:
-            dist.destroy_process_group()
-        return
+    rank, world, local = _init_ranks()
 
-    from kratos_polrad_b200 import scenes
+    from kratos_polrad_b200 import scenes, shard
     from kratos_polrad_b200._lib import call, ptr
     from kratos_polrad_b200.transport import Tallies, forward
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     n_pk = int(args.packets)
     mesh, sigma2, cfg = scenes.clump_amr(n_packets=n_pk)
-    cfg = dataclasses.replace(cfg, packet_offset=rank * n_pk)
+    cfg = shard.shard_config(cfg, rank, world, weak=True)
     mesh.set_sigma(sigma2)
     tal = Tallies(cfg)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    rank_counts = torch.zeros(10, dtype=torch.int64, device=dev)
 
     def allreduce():
-        if world > 1:
-            for t in (tal.image, tal.mu, tal.image_batch, tal.counters):
-                dist.all_reduce(t)
+        rank_counts.copy_(tal.counters)               # this rank's own counts
+        shard.reduce_tallies([tal.image, tal.mu, tal.image_batch, tal.counters])
 
     for _ in range(args.warmup):
         tal.zero_()
@@ -529,9 +574,7 @@ def main():
     p_tan, rel_err = scenes.batch_rel_error(tal.image_batch.cpu().numpy() * scale)
 
     # roofline of the transport kernel (per launch, this rank)
-    c_rank = {k: int(v) for k, v in zip(tal.counts().keys(), counts[-1].cpu().numpy())}
-    if world > 1:
-        c_rank = {k: v // world for k, v in c_rank.items()}
+    c_rank = {k: int(v) for k, v in zip(tal.counts().keys(), rank_counts.cpu().numpy())}
     kern_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = measured_peak()
     ach = algorithmic_bytes(c_rank) / kern_s / 1e9
@@ -600,7 +643,7 @@ def main():
     t2 = torch.tensor([e2e_ms / 1e3], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_value = (e2e_steps if world > 1 else e2e_steps) / float(t2.item())
+    e2e_value = e2e_steps / float(t2.item())
 
     out = None
     if rank == 0:
