@@ -1,0 +1,89 @@
+"""Generates the golden fixtures of the geometric walk from the reference's
+own code compiled for the host (oracle/_ref: tree_t, meshgen, proxy_base_t
+::setup and photon::cart_t::proc built from the reference sources).
+
+Each fixture holds the reference's block tables and the final packet states
+and flux sums of a seeded packet set, in the reference's block order, so
+tests can pin the product tables, the oracle restatement and the GPU walk
+without the reference present.  Run from the repository root after
+`make -C oracle ref REF=<reference tree>`:
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [ROOT, os.path.dirname(HERE)]
+
+from kratos_polrad_b200 import Mesh                      # noqa: E402
+from meshcases import CASES                              # noqa: E402
+from oracle import refharness                            # noqa: E402
+
+FIXTURES = [("amr_box", 1), ("amr_periodic", 1), ("amr_periodic", 2), ("three_level", 2),
+            ("slab", 1)]
+N_PACKETS, BUDGET, FX_SHIFT = 256, 120, 30
+
+
+def packets(mesh, n, ftype, seed):
+    """Seeded packets: random interior points and directions, plus axis-aligned
+    and in-plane directions, starts on a cell face and short budgets."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.array(mesh.x_min), np.array(mesh.x_max)
+    x = (lo + rng.random((n, 3)) * (hi - lo)).astype(ftype)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = d.astype(ftype)
+    k = n // 8
+    d[:k, :] = 0
+    d[:k, 0] = np.where(rng.random(k) < 0.5, 1, -1)
+    d[k:2 * k, 2] = 0
+    xf0, dx0, _, _ = mesh.geometry(4 if ftype == np.float32 else 8)
+    ib, cell = mesh.locate(x.astype(np.float64))
+    m = slice(2 * k, 3 * k)
+    x[m, 1] = (xf0[ib[m], 1] + cell[m, 1] * dx0[ib[m], 1]).astype(ftype)
+    ib, cell = mesh.locate(x.astype(np.float64))
+    proper = rng.random(n).astype(ftype) + ftype(0.5)
+    steps = np.full(n, BUDGET, np.int32)
+    steps[3 * k:4 * k] = rng.integers(0, 40, k)
+    return x, d, cell, ib, proper, steps
+
+
+def make(name, precision):
+    cfg = CASES[name]
+    ftype = np.float32 if precision == 1 else np.float64
+    mesh = Mesh(cfg)
+    ref = refharness.RefMesh(cfg.to_ini(), precision)
+    rl, rr = ref.blocks()
+    pl, pr = mesh.blocks()
+    key = {(int(l), *map(int, r)): i for i, (l, r) in enumerate(zip(pl, pr))}
+    perm = np.array([key[(int(l), *map(int, r))] for l, r in zip(rl, rr)])   # ref -> product
+    inv = np.argsort(perm)
+    x, d, cell, ib, proper, steps = packets(mesh, N_PACKETS, ftype, seed=100 + precision)
+    ib_ref = inv[ib].astype(np.int32)
+    r = ref.trace(x, d, cell, ib_ref, proper, steps, fx_shift=FX_SHIFT)
+    xf0, dx0, vol0, pb = ref.geometry()
+    ids, sh, dl = ref.neighbors()
+    xlim, lbox, per = ref.box()
+    nz = np.nonzero((r["flux"] != 0) | (r["flux_fx"] != 0))[0]
+    out = dict(ini=np.array(cfg.to_ini()), precision=np.int32(precision),
+               ref_levels=rl, ref_regions=rr, xf0=xf0, dx0=dx0, vol0=vol0, phybnd=pb,
+               nb_ids=ids, nb_shift=sh, nb_dlvl=dl, xlim=xlim, lbox=lbox, periodic=per,
+               in_x=x, in_dir=d, in_cell=cell.astype(np.int32), in_ib=ib_ref, in_proper=proper,
+               in_steps=steps, fx_shift=np.int32(FX_SHIFT),
+               out_x=r["x"], out_cell=r["cell"], out_ib=r["ib"], out_step=r["step"],
+               out_todo=r["todo"], flux_idx=nz.astype(np.int32), flux=r["flux"][nz],
+               flux_fx=r["flux_fx"][nz])
+    path = os.path.join(HERE, f"trace_{name}_p{precision}.npz")
+    np.savez_compressed(path, **out)
+    return path, os.path.getsize(path)
+
+
+if __name__ == "__main__":
+    if not refharness.available(1):
+        sys.exit("oracle/_ref not built: make -C oracle ref REF=<reference tree>")
+    for name, prec in FIXTURES:
+        print(*make(name, prec))
