@@ -369,6 +369,44 @@ int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
 int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                                   const kp_tallies_t * tallies, void * stream );
 
+/* ------------------------------------------------------------------ */
+/* Binary container of the reference's binary_io (io/binary/            */
+/* binary_io.h:6-32; save/load in binary_io_base.cpp:89-131): a byte of */
+/* (little-endian | sizeof(size_t)), the header size, a tag-sorted map  */
+/* tag -> (size, unit size, offset), then the data.  Files written here */
+/* are byte-identical to binary_io::base_t::save's for the same entries */
+/* and readable by the reference's visual/binary_io.py:31-55; the       */
+/* reader takes either writer's files.  Host memory only.  Replaces     */
+/* mesh_t::save / the restart load (mesh/mesh.cpp:63-69,99-112) for the */
+/* transport's fields and tallies.                                      */
+
+typedef struct kp_bio_entry
+{
+    const char *       tag;
+    const void *       data;       /* host pointer                          */
+    unsigned long long count;      /* elements                              */
+    int                unit_size;  /* bytes per element, 1..127             */
+} kp_bio_entry_t;
+
+/* Writes (truncates) `path`; a later entry with the same tag replaces an
+ * earlier one, as binary_io::base_t::write does. */
+int kp_bio_write( const char * path, int n_entries, const kp_bio_entry_t * entries );
+
+typedef struct kp_bio kp_bio_t;
+/* Opens a container and reads its header (checks size_t and endianness as
+ * binary_io::base_t::load_header does, and every entry against the file). */
+int kp_bio_open( const char * path, kp_bio_t ** file );
+int kp_bio_close( kp_bio_t * file );
+int kp_bio_n_entries( const kp_bio_t * file, int * n );
+/* Entry i in file order: tag (NUL-terminated into tag[tag_cap]), size in
+ * bytes, unit size.  Any output may be NULL. */
+int kp_bio_entry( const kp_bio_t * file, int i, char * tag, size_t tag_cap,
+                  unsigned long long * size, int * unit_size );
+/* Copies entry `tag` into dst (cap bytes available; KP_ERR_ARG if the tag
+ * is missing or the entry is larger); *size receives its size in bytes. */
+int kp_bio_read( const kp_bio_t * file, const char * tag, void * dst, unsigned long long cap,
+                 unsigned long long * size );
+
 #ifdef __cplusplus
 }
 #endif

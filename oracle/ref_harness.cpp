@@ -32,6 +32,7 @@
 #include "mesh/tree/tree.h"
 #include "mesh/mesh.h"
 #include "io/args/input.h"
+#include "io/binary/binary_io_base.h"
 #include "utilities/mapping/loop.h"
 
 #include <atomic>
@@ -432,6 +433,53 @@ int kpref_trace( long n, const double * x, const double * dir,
     if( flux_fx_out )
         std::copy( h.flux_fx.begin(  ), h.flux_fx.end(  ), flux_fx_out );
     return 0;
+}
+
+// The reference's binary container: binary_io::base_t::write for every entry
+// (copied into its buffers), then save (io/binary/binary_io_base.cpp:89-131).
+int kpref_bio_write( const char * path, int n, const char * const * tags,
+                     const void * const * data, const unsigned long long * counts,
+                     const int * unit_sizes )
+{
+    try
+    {
+        binary_io::base_t b;
+        b.open( path, "w" );
+        for( int i = 0; i < n; ++ i )
+            b.write( data[ i ], ( size_t ) counts[ i ], ( size_t ) unit_sizes[ i ], tags[ i ],
+                     true );
+        b.save(  );
+        b.close(  );
+        return 0;
+    }
+    catch( const std::exception & )
+    {
+        return -1;
+    }
+}
+
+// Loads a container with binary_io::base_t::load and reads one entry:
+// returns its element count (base_t::read), or -1 if it cannot.
+long long kpref_bio_read( const char * path, const char * tag, void * dst,
+                          unsigned long long * size, int * unit_size )
+{
+    try
+    {
+        binary_io::base_t b;
+        b.open( path, "r" );
+        b.load(  );
+        const auto & in = b.info( tag );
+        if( size ) * size = in.size;
+        if( unit_size ) * unit_size = in.u_size;
+        long long n = 0;
+        if( dst ) n = ( long long ) b.read( dst, tag );
+        b.close(  );
+        return n;
+    }
+    catch( const std::exception & )
+    {
+        return -1;
+    }
 }
 
 }   // extern "C"

@@ -28,13 +28,17 @@ class RefMesh:
 
     _libs: dict = {}
 
-    def __init__(self, ini_text: str, precision: int = 1):
-        if precision not in self._libs:
+    @classmethod
+    def _lib_for(cls, precision):
+        if precision not in cls._libs:
             path = os.path.join(REF_DIR, f"libkpref_p{precision}.so")
             if not os.path.exists(path):
                 raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
-            self._libs[precision] = ctypes.CDLL(path)
-        self.lib = L = self._libs[precision]
+            cls._libs[precision] = ctypes.CDLL(path)
+        return cls._libs[precision]
+
+    def __init__(self, ini_text: str, precision: int = 1):
+        self.lib = L = self._lib_for(precision)
         self.precision = precision
         self.ftype = np.float32 if precision == 1 else np.float64
         with tempfile.NamedTemporaryFile("w", suffix=".ini", delete=False) as f:
@@ -100,3 +104,35 @@ class RefMesh:
         if st != 0:
             raise RuntimeError("kpref_trace failed")
         return out
+
+
+def bio_write(path: str, entries, precision: int = 2) -> None:
+    """Writes (tag, numpy array) pairs with the reference's own
+    binary_io::base_t (write with copy, then save)."""
+    L = RefMesh._lib_for(precision)
+    n = len(entries)
+    arrs = [np.ascontiguousarray(a).reshape(-1) for _, a in entries]
+    tags = (ctypes.c_char_p * n)(*[t.encode("ascii") for t, _ in entries])
+    data = (ctypes.c_void_p * n)(*[a.ctypes.data for a in arrs])
+    counts = (ctypes.c_ulonglong * n)(*[a.size for a in arrs])
+    units = (ctypes.c_int * n)(*[a.dtype.itemsize for a in arrs])
+    L.kpref_bio_write.argtypes = [ctypes.c_char_p, ctypes.c_int] + [ctypes.c_void_p] * 4
+    if L.kpref_bio_write(path.encode(), n, tags, data, counts, units) != 0:
+        raise RuntimeError("reference binary_io rejected the entries")
+
+
+def bio_read(path: str, tag: str, precision: int = 2):
+    """(bytes, unit size) of one entry, read by the reference's
+    binary_io::base_t (load, then read)."""
+    L = RefMesh._lib_for(precision)
+    L.kpref_bio_read.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p,
+                                 ctypes.c_void_p, ctypes.c_void_p]
+    L.kpref_bio_read.restype = ctypes.c_longlong
+    size, unit = ctypes.c_ulonglong(), ctypes.c_int()
+    if L.kpref_bio_read(path.encode(), tag.encode(), None, ctypes.byref(size),
+                        ctypes.byref(unit)) < 0:
+        raise KeyError(tag)
+    buf = np.zeros(max(1, size.value), np.uint8)
+    if L.kpref_bio_read(path.encode(), tag.encode(), buf.ctypes.data, None, None) < 0:
+        raise KeyError(tag)
+    return buf[:size.value].tobytes(), unit.value

@@ -8,7 +8,10 @@ tests can pin the product tables, the oracle restatement and the GPU walk
 without the reference present.  Run from the repository root after
 `make -C oracle ref REF=<reference tree>`:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [reference tree]
+
+It also writes two binary-container fixtures, one with the reference's C++
+binary_io and one with its Python writer (visual/binary_io.py).
 """
 import os
 import sys
@@ -82,8 +85,39 @@ def make(name, precision):
     return path, os.path.getsize(path)
 
 
+def bio_entries():
+    """Entries of the binary-container fixtures: unsorted tags (the writer
+    sorts them), every unit size the transport stores, a block-key tag."""
+    rng = np.random.default_rng(12)
+    return [("zeta|tally", rng.integers(-2 ** 40, 2 ** 40, 24, dtype=np.int64)),
+            ("block_10|level", np.int32([2])),
+            ("block_2|i_logic", np.int32([1, 0, 3])),
+            ("alpha", rng.random(7).astype(np.float32)),
+            ("kp|grad", rng.normal(size=5)),
+            ("kp|config", np.frombuffer(b'{"seed": 4}', np.uint8))]
+
+
+def make_bio(reference_tree):
+    """bio_reference.bin: the reference's C++ binary_io::base_t; bio_reference_py.bin:
+    the reference's Python writer (visual/binary_io.py), which keeps insertion order."""
+    ent = bio_entries()
+    p1 = os.path.join(HERE, "bio_reference.bin")
+    refharness.bio_write(p1, ent)
+    sys.path.insert(0, os.path.join(reference_tree, "visual"))
+    from binary_io import binary_io as py_writer        # the reference's own reader/writer
+    p2 = os.path.join(HERE, "bio_reference_py.bin")
+    w = py_writer(p2)
+    for tag, a in ent:
+        w.cache(tag, a)
+    w.save()
+    return [(p, os.path.getsize(p)) for p in (p1, p2)]
+
+
 if __name__ == "__main__":
     if not refharness.available(1):
         sys.exit("oracle/_ref not built: make -C oracle ref REF=<reference tree>")
+    ref_tree = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     for name, prec in FIXTURES:
         print(*make(name, prec))
+    for p in make_bio(ref_tree):
+        print(*p)
