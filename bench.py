@@ -118,14 +118,20 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_packet():
-    """DRAM bytes per packet of the transport kernel from the committed ncu
-    summary (profiles/k_forward_clump_traffic.json), or None."""
-    p = os.path.join(ROOT, "profiles", "k_forward_clump_traffic.json")
+def ncu_traffic(n_packets):
+    """DRAM bytes (read + write) of one transport launch from the committed
+    ncu summary (profiles/k_forward_clump_traffic.txt), when it was captured on
+    this packet count (the traffic does not scale with packets), else None."""
+    p = os.path.join(ROOT, "profiles", "k_forward_clump_traffic.txt")
     try:
-        with open(p) as f:
-            d = json.load(f)
-        return float(d["dram_bytes"]) / float(d["packets"])
+        kv = {}
+        for ln in open(p):
+            if "=" in ln and not ln.lstrip().startswith("#"):
+                k, v = ln.split("=", 1)
+                kv[k.strip()] = float(v)
+        if int(kv["packets"]) != int(n_packets):
+            return None
+        return kv["dram_read_bytes"] + kv["dram_write_bytes"]
     except (OSError, KeyError, ValueError):
         return None
 
@@ -578,10 +584,9 @@ def main():
     kern_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = measured_peak()
     ach = algorithmic_bytes(c_rank) / kern_s / 1e9
-    tpp = ncu_traffic_per_packet()
     roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_source": peak_kind, "kernel": "k_forward",
-                "traffic": (tpp * n_pk) if tpp else None,
+                "traffic": ncu_traffic(n_pk),
                 "algorithmic_bytes": algorithmic_bytes(c_rank),
                 "kernel_ms": statistics.mean(kern_ms)}
 
