@@ -31,17 +31,24 @@ namespace cg = cooperative_groups;
 // contribution is deposited and the walk resumes.  Peel-off rays draw no
 // random numbers, so each packet's history equals a sequential walk that
 // marches every peel-off ray at the moment of its interaction.
+#ifndef KP_FWD_RESIDENT
+#define KP_FWD_RESIDENT 768          // resident threads per SM the register budget targets
+#endif
+
 template< int TALLY, int NT >
-__global__ void __launch_bounds__( NT, 768 / NT )
+__global__ void __launch_bounds__( NT, KP_FWD_RESIDENT / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
     __shared__ park_t< NT > sp;
+    __shared__ dir_park_t< NT > sd;
+    __shared__ cold_park_t< NT > sc;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     if( threadIdx.x < KP_NCOUNTERS ) sp.cnt[ threadIdx.x ] = 0;
     __syncthreads(  );
     counts32_t cnt;
     packet_t p;
+    double fx[ 3 ];                               // face cache of the active ray
     int  phase = PH_EMIT;
     bool peel = false;
     float ptau = 0;
@@ -115,15 +122,19 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sp.pix[ t ] = pix;
                     pend = 0; ptau = 0.0f; pk = 0;
                     park_walk( sp, p );
+                    park_dir( sd, p, P.o, P.inv_o );
                     peel = true;
                 }
             }
+            faces_all( P.m, p.b, p.c, p.d, fx );
+            store_cold( sc, p );
             continue;
         }
 
         if( run == PH_EVENT )
         {
             if( phase != PH_EVENT ) continue;
+            load_cold( sc, p, P.seed );
             // interaction at p.x (already moved there by its segment)
             ++ p.n_scat;
             count( sp, KP_CNT_SCATTER );
@@ -168,6 +179,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             if( do_peel )
             {
                 park_walk( sp, p );
+                park_dir( sd, p, P.o, P.inv_o );
                 ptau = 0.0f; pk = 0; pend = end;
                 peel = true;
                 phase = PH_SEGMENT;
@@ -180,19 +192,22 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             else
                 phase = PH_SEGMENT;
+            if( phase == PH_SEGMENT )
+            {
+                faces_all( P.m, p.b, p.c, p.d, fx );
+                store_cold( sc, p );
+            }
             continue;
         }
 
         // ---- PH_SEGMENT: one segment of the active ray ----
         if( phase != PH_SEGMENT ) continue;
+        // the active ray's direction is in p.d / p.inv (a peel-off ray holds
+        // them while the walk's are parked)
         const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
         const float ext = __fadd_rn( sg.x, sg.y );
-        const phys::v3 dd = peel ? P.o : p.d;
-        const double inv[ 3 ] = { peel ? P.inv_o[ 0 ] : p.inv[ 0 ],
-                                  peel ? P.inv_o[ 1 ] : p.inv[ 1 ],
-                                  peel ? P.inv_o[ 2 ] : p.inv[ 2 ] };
         int ax;
-        const double t = exit_dist( P.m, p.b, p.c, p.x, dd, inv, ax );
+        const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
         const float et = __fmul_rn( ext, ( float ) t );
         bool interact = false, peel_cut = false;
         if( peel )
@@ -224,9 +239,9 @@ k_forward( const __grid_constant__ fwd_params_t P )
             if( ! peel ) p.tau = __fsub_rn( p.tau, et );
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
-                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
+                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
             const int b_old = p.b;
-            left = ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost );
+            left = ! cross_cached( P.m, p.b, p.c, p.x, fx, ax, p.d, lost );
             if( ! left && p.b != b_old ) count( sp, KP_CNT_HOPS );
         }
         if( peel )
@@ -238,15 +253,18 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     const int th = threadIdx.x;
                     const float att = __fmul_rn( sp.w[ th ],
                                                  ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                    deposit_pixel< TALLY >( P, sp.pix[ th ], p.pid(  ), __fmul_rn( att, sp.I[ th ] ),
+                    deposit_pixel< TALLY >( P, sp.pix[ th ], cold_pid( sc ), __fmul_rn( att, sp.I[ th ] ),
                                             __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
                                             __fmul_rn( att, sp.V[ th ] ) );
                     count( sp, KP_CNT_DEPOSITS );
                 }
                 unpark_walk( sp, p );
+                unpark_dir( sd, p );
+                faces_all( P.m, p.b, p.c, p.d, fx );
                 peel = false;
                 if( pend )
                 {
+                    load_cold( sc, p, P.seed );
                     write_record( P, p, pend );
                     count( sp, pend == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
                     phase = PH_EMIT;
@@ -257,6 +275,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
         int end = 0;
         if( left )
         {
+            load_cold( sc, p, P.seed );
             if( lost )
                 end = PK_LOST;
             else
@@ -267,7 +286,10 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
         }
         else if( p.n_steps >= P.max_steps )
+        {
+            load_cold( sc, p, P.seed );
             end = PK_STEP_CAP;
+        }
         if( end )
         {
             write_record( P, p, end );

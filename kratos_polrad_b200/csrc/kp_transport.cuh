@@ -217,6 +217,134 @@ __device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int 
     return true;
 }
 
+// Face cache of the active ray (forward kernel).  fx[a] is the coordinate of
+// the face through which the ray leaves cell c along axis a, computed with
+// exit_dist's expression, so distances from the cache are bit-identical to
+// exit_dist's while a segment loads no geometry.  Refreshed for all axes when
+// the direction or the block changes, for one axis after an in-block step.
+__device__ __forceinline__ void faces_all( const mesh_view_t & m, int b, const int c[ 3 ],
+                                           const phys::v3 & d, double fx[ 3 ] )
+{
+    const double * g = m.geo_d + 16 * ( size_t ) b;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+        fx[ a ] = __fma_rn( ( double ) ( c[ a ] + ( comp( d, a ) > 0.0f ? 1 : 0 ) ), g[ 3 + a ],
+                            g[ a ] );
+}
+
+// exit_dist from the face cache.
+__device__ __forceinline__ double exit_cached( const double x[ 3 ], const double fx[ 3 ],
+                                               const phys::v3 & d, const double inv[ 3 ], int & ax )
+{
+    double t = 1e300;
+    ax = 0;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        if( comp( d, a ) == 0.0f ) continue;
+        double ta = __dmul_rn( __dsub_rn( fx[ a ], x[ a ] ), inv[ a ] );
+        ta = ta < 0.0 ? 0.0 : ta;
+        if( ta < t ) { t = ta; ax = a; }
+    }
+    return t;
+}
+
+// cross_face with the face cache: inside the block the crossed face is the
+// cached one (x snaps to it) and only that axis's next face is computed;
+// a hand-off to a neighbour block refreshes all three.
+__device__ __forceinline__ bool cross_cached( const mesh_view_t & m, int & b, int c[ 3 ],
+                                              double x[ 3 ], double fx[ 3 ], int ax,
+                                              const phys::v3 & d, bool & lost )
+{
+    const bool pos = comp( d, ax ) > 0.0f;
+    const int cax = ax == 0 ? c[ 0 ] : ( ax == 1 ? c[ 1 ] : c[ 2 ] );
+    const int cn = cax + ( pos ? 1 : -1 );
+    if( cn >= 0 && cn < m.nc[ ax ] )
+    {
+        lost = false;
+        const double * g = m.geo_d + 16 * ( size_t ) b;
+        const double nf = __fma_rn( ( double ) ( cn + ( pos ? 1 : 0 ) ), g[ 3 + ax ], g[ ax ] );
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+            if( a == ax ) { c[ a ] = cn; x[ a ] = fx[ a ]; fx[ a ] = nf; }
+        return true;
+    }
+    if( ! cross_face( m, b, c, x, ax, pos, lost ) )
+        return false;
+    faces_all( m, b, c, d, fx );
+    return true;
+}
+
+// Direction of the parked walk while a peel-off ray holds the direction
+// registers (forward kernel).
+template< int NT >
+struct dir_park_t
+{
+    float  d[ 3 ][ NT ];
+    double inv[ 3 ][ NT ];
+};
+
+template< class SD >
+__device__ __forceinline__ void park_dir( SD & sd, packet_t & p, const phys::v3 & o,
+                                          const double inv_o[ 3 ] )
+{
+    const int t = threadIdx.x;
+    sd.d[ 0 ][ t ] = p.d.x; sd.d[ 1 ][ t ] = p.d.y; sd.d[ 2 ][ t ] = p.d.z;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) { sd.inv[ a ][ t ] = p.inv[ a ]; p.inv[ a ] = inv_o[ a ]; }
+    p.d = o;
+}
+template< class SD >
+__device__ __forceinline__ void unpark_dir( const SD & sd, packet_t & p )
+{
+    const int t = threadIdx.x;
+    p.d = phys::v3 { sd.d[ 0 ][ t ], sd.d[ 1 ][ t ], sd.d[ 2 ][ t ] };
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) p.inv[ a ] = sd.inv[ a ][ t ];
+}
+
+// Packet state that only interactions, emissions, tallies and records use
+// (forward kernel): the Stokes frame, Stokes vector, weight, interaction
+// count and RNG counter words live in shared memory between those events,
+// so the segment loop keeps only the ray's geometry in registers.
+template< int NT >
+struct cold_park_t
+{
+    float    e1[ 3 ][ NT ];
+    float    S[ 3 ][ NT ];
+    float    w[ NT ];
+    int      n_scat[ NT ];
+    uint32_t k1[ NT ], pid_lo[ NT ], pid_hi[ NT ], draw[ NT ];
+};
+
+template< class SC >
+__device__ __forceinline__ void store_cold( SC & sc, const packet_t & p )
+{
+    const int t = threadIdx.x;
+    sc.e1[ 0 ][ t ] = p.e1.x; sc.e1[ 1 ][ t ] = p.e1.y; sc.e1[ 2 ][ t ] = p.e1.z;
+    sc.S[ 0 ][ t ] = p.S.q; sc.S[ 1 ][ t ] = p.S.u; sc.S[ 2 ][ t ] = p.S.v;
+    sc.w[ t ] = p.w;
+    sc.n_scat[ t ] = p.n_scat;
+    sc.k1[ t ] = p.rng.k1; sc.pid_lo[ t ] = p.rng.pid_lo; sc.pid_hi[ t ] = p.rng.pid_hi;
+    sc.draw[ t ] = p.rng.draw;
+}
+template< class SC >
+__device__ __forceinline__ void load_cold( const SC & sc, packet_t & p, uint32_t seed )
+{
+    const int t = threadIdx.x;
+    p.e1 = phys::v3 { sc.e1[ 0 ][ t ], sc.e1[ 1 ][ t ], sc.e1[ 2 ][ t ] };
+    p.S = phys::stokes_t { sc.S[ 0 ][ t ], sc.S[ 1 ][ t ], sc.S[ 2 ][ t ] };
+    p.w = sc.w[ t ];
+    p.n_scat = sc.n_scat[ t ];
+    p.rng = phys::rng_t { seed, sc.k1[ t ], sc.pid_lo[ t ], sc.pid_hi[ t ], sc.draw[ t ] };
+}
+template< class SC >
+__device__ __forceinline__ long long cold_pid( const SC & sc )
+{
+    const int t = threadIdx.x;
+    return ( long long ) ( ( ( unsigned long long ) sc.pid_hi[ t ] << 32 ) | sc.pid_lo[ t ] );
+}
+
 // Optical depth from x to the domain boundary along the observer direction;
 // stops early (returns > tau_cut) once tau_cut is exceeded.
 __device__ __forceinline__ float peel_tau( const fwd_params_t & P, int b, const int c0[ 3 ],
