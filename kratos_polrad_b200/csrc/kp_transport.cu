@@ -108,6 +108,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             count( sp, KP_CNT_EMITTED );
+            sc.batch[ threadIdx.x ] = ( int ) ( p.pid(  ) % P.n_batch );
             p.tau = sample_tau( p.rng );
             phase = PH_SEGMENT;
             const src_dev_t & s = P.n_scenes > 0 ? P.scenes[ si ].src : P.src[ p.pid(  ) % P.n_src ];
@@ -120,6 +121,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sp.w[ t ] = 1.0f; sp.I[ t ] = 0x1.45f306p-4f;     // 1 / (4 pi)
                     sp.Q[ t ] = sp.U[ t ] = sp.V[ t ] = 0.0f;
                     sp.pix[ t ] = pix;
+                    sd.cpix[ t ] = coarse_pixel( P, pix, sc.batch[ t ] );
                     pend = 0; ptau = 0.0f; pk = 0;
                     park_walk( sp, p );
                     park_dir( sd, p, P.o, P.inv_o );
@@ -154,6 +156,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sp.Q[ t ] = Q; sp.U[ t ] = U; sp.V[ t ] = V;
                     sp.w[ t ] = p.w;
                     sp.pix[ t ] = pix;
+                    sd.cpix[ t ] = coarse_pixel( P, pix, sc.batch[ t ] );
                     do_peel = true;
                 }
             }
@@ -253,7 +256,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     const int th = threadIdx.x;
                     const float att = __fmul_rn( sp.w[ th ],
                                                  ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                    deposit_pixel< TALLY >( P, sp.pix[ th ], cold_pid( sc ), __fmul_rn( att, sp.I[ th ] ),
+                    deposit_pixel< TALLY >( P, sp.pix[ th ], sd.cpix[ th ], __fmul_rn( att, sp.I[ th ] ),
                                             __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
                                             __fmul_rn( att, sp.V[ th ] ) );
                     count( sp, KP_CNT_DEPOSITS );
@@ -282,7 +285,9 @@ k_forward( const __grid_constant__ fwd_params_t P )
             {
                 end = PK_ESCAPED;
                 if( tally_escape< TALLY >( P, ( char * ) P.mu_tally + ( size_t ) si * P.mu_scene_stride
-                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), p ) ) count( sp, KP_CNT_DEPOSITS );
+                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), p,
+                                             sc.batch[ threadIdx.x ] ) )
+                    count( sp, KP_CNT_DEPOSITS );
             }
         }
         else if( p.n_steps >= P.max_steps )
@@ -331,6 +336,9 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     require( c.image_n == 0 || ( c.image_batch_n >= 1 && c.image_batch_n <= c.image_n ),
              "image_batch_n must be in 1..image_n" );
     require( c.lane_batch >= 0 && c.lane_batch <= 32, "lane_batch must be in 0..32" );
+    require( c.image_n == 0 || ( long long ) c.n_batches * c.image_batch_n * c.image_batch_n
+                                  < ( 1ll << 31 ), "per-batch image too large",
+             KP_ERR_CAPACITY );
     std::memset( & P, 0, sizeof( P ) );
     P.n_packets = c.n_packets;
     P.pid0 = c.packet_offset;

@@ -282,6 +282,7 @@ struct dir_park_t
 {
     float  d[ 3 ][ NT ];
     double inv[ 3 ][ NT ];
+    int    cpix[ NT ];             // coarse per-batch pixel of the pending deposit
 };
 
 template< class SD >
@@ -315,6 +316,7 @@ struct cold_park_t
     float    w[ NT ];
     int      n_scat[ NT ];
     uint32_t k1[ NT ], pid_lo[ NT ], pid_hi[ NT ], draw[ NT ];
+    int      batch[ NT ];          // pid % n_batches, set at emission
 };
 
 template< class SC >
@@ -409,19 +411,25 @@ __device__ __forceinline__ int image_pixel( const fwd_params_t & P, const double
 // Adds a peel-off contribution (intensity per steradian I and image-frame
 // Q, U, V, already weighted) to image pixel `pix` (>= 0) and to the packet's
 // batch image.
-template< int TALLY >
-__device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel,
-                                               long long pid, float I, float Q, float U, float V )
+// Index of pixel `pixel` in the coarse per-batch image of batch `batch`
+// (pixel i -> i * bn / n on each axis); computed once when a peel-off ray
+// starts, so the deposit at its end is atomics only.
+__device__ __forceinline__ int coarse_pixel( const fwd_params_t & P, int pixel, int batch )
 {
     const int ix = pixel % P.img_n, iy = pixel / P.img_n;
+    return ( batch * P.img_bn + iy * P.img_bn / P.img_n ) * P.img_bn + ix * P.img_bn / P.img_n;
+}
+
+template< int TALLY >
+__device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel, int cpix,
+                                               float I, float Q, float U, float V )
+{
     const size_t pix = ( size_t ) pixel * 4;
     add_tally< TALLY >( P.image, pix + 0, I, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 1, Q, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 2, U, P.fx_scale );
     add_tally< TALLY >( P.image, pix + 3, V, P.fx_scale );
-    const int batch = ( int ) ( pid % P.n_batch );
-    const size_t bp = ( ( ( size_t ) batch * P.img_bn + iy * P.img_bn / P.img_n ) * P.img_bn
-                        + ix * P.img_bn / P.img_n ) * 4;
+    const size_t bp = ( size_t ) cpix * 4;
     add_tally< TALLY >( P.img_batch, bp + 0, I, P.fx_scale );
     add_tally< TALLY >( P.img_batch, bp + 1, Q, P.fx_scale );
     add_tally< TALLY >( P.img_batch, bp + 2, U, P.fx_scale );
@@ -432,7 +440,7 @@ __device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel
 // plane of d and +z).
 template< int TALLY >
 __device__ __forceinline__ bool tally_escape( const fwd_params_t & P, void * mu_base,
-                                              const packet_t & p )
+                                              const packet_t & p, int batch )
 {
     if( P.n_mu <= 0 ) return false;
     const float fb = floorf( __fmul_rn( __fsub_rn( p.d.z, P.mu_lo ), P.mu_inv_w ) );
@@ -443,7 +451,6 @@ __device__ __forceinline__ bool tally_escape( const fwd_params_t & P, void * mu_
     phys::double_angle( p.e1.z, e2.z, c2, s2 );
     float q = p.S.q, u = p.S.u;
     phys::rotate( q, u, c2, s2 );
-    const int batch = ( int ) ( p.pid(  ) % P.n_batch );
     const size_t i = ( ( size_t ) batch * P.n_mu + bin ) * 4;
     add_tally< TALLY >( mu_base, i + 0, p.w, P.fx_scale );
     add_tally< TALLY >( mu_base, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
