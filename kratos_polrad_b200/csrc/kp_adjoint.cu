@@ -54,6 +54,8 @@ __global__ void __launch_bounds__( FWD_THREADS, 3 )
 k_adjoint( const __grid_constant__ fwd_params_t P )
 {
     __shared__ park_t<  > sp;
+    __shared__ dir_park_t< FWD_THREADS > sd;
+    __shared__ cold_park_t< FWD_THREADS > sc;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const int th = threadIdx.x;
@@ -61,6 +63,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
     __syncthreads(  );
     counts32_t cnt;
     packet_t p;
+    double fx[ 3 ];                               // face cache of the active ray
     int   phase = PH_EMIT, ray = RAY_WALK, pass = 0;
     float ptau = 0.f, pG = 0.f, G0 = 0.f;
     int   pk = 0, pend = 0, nv = 0;
@@ -71,9 +74,10 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
     // Starts pass 1 of the lane's packet (same id, RNG from its start).
     auto begin_pass1 = [ & ](  )
     {
-        const long long pid = p.pid(  );
+        const long long pid = cold_pid( sc );
         emit_packet( P, pid, p, P.src[ pid % P.n_src ], P.stream );
         p.tau = sample_tau( p.rng );
+        store_cold( sc, p );
         pass = 1;
         nv = 0;
         phase = PH_SEGMENT;
@@ -82,9 +86,11 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC && G0 != 0.0f )
         {
             park_walk( sp, p );
+            park_dir( sd, p, P.o, P.inv_o );
             pG = G0; ptau = 0.f; pk = 0; pend = 0;
             ray = RAY_DEPOSIT;
         }
+        faces_all( P.m, p.b, p.c, p.d, fx );
     };
     // The lane's packet has ended (in the current pass).
     auto end_packet = [ & ](  )
@@ -137,6 +143,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             }
             count( sp, KP_CNT_EMITTED );
             p.tau = sample_tau( p.rng );
+            store_cold( sc, p );
             pass = 0; nv = 0; R = 0.0; G0 = 0.f;
             phase = PH_SEGMENT;
             ray = RAY_WALK;
@@ -151,15 +158,18 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                     sp.pix[ th ] = pix;
                     pend = 0; ptau = 0.0f; pk = 0;
                     park_walk( sp, p );
+                    park_dir( sd, p, P.o, P.inv_o );
                     ray = RAY_MEASURE;
                 }
             }
+            faces_all( P.m, p.b, p.c, p.d, fx );
             continue;
         }
 
         if( run == PH_EVENT )
         {
             if( phase != PH_EVENT ) continue;
+            load_cold( sc, p, P.seed );
             ++ p.n_scat;
             count( sp, KP_CNT_SCATTER );
             const size_t ci = cell_index( P.m, p.b, p.c );
@@ -203,6 +213,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             }
             if( ! end && p.n_steps >= P.max_steps )
                 end = PK_STEP_CAP;
+            store_cold( sc, p );
             phase = PH_SEGMENT;
             if( do_peel )
             {
@@ -211,6 +222,8 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                 if( pass == 0 || nv > ADJ_KMAX )
                 {
                     park_walk( sp, p );
+                    park_dir( sd, p, P.o, P.inv_o );
+                    faces_all( P.m, p.b, p.c, p.d, fx );
                     ray = RAY_MEASURE;
                     remeasure = pass == 1;
                     continue;
@@ -219,12 +232,16 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                 if( pG != 0.0f )
                 {
                     park_walk( sp, p );
+                    park_dir( sd, p, P.o, P.inv_o );
+                    faces_all( P.m, p.b, p.c, p.d, fx );
                     ray = RAY_DEPOSIT;
                     continue;
                 }
             }
             if( end )
                 end_packet(  );
+            else
+                faces_all( P.m, p.b, p.c, p.d, fx );
             continue;
         }
 
@@ -234,12 +251,8 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         const size_t ci = cell_index( P.m, p.b, p.c );
         const float2 sg = P.m.sigma[ ci ];
         const float ext = __fadd_rn( sg.x, sg.y );
-        const phys::v3 dd = peel ? P.o : p.d;
-        const double inv[ 3 ] = { peel ? P.inv_o[ 0 ] : p.inv[ 0 ],
-                                  peel ? P.inv_o[ 1 ] : p.inv[ 1 ],
-                                  peel ? P.inv_o[ 2 ] : p.inv[ 2 ] };
-        int ax;
-        const double t = exit_dist( P.m, p.b, p.c, p.x, dd, inv, ax );
+        int ax;                                   // p.d / p.inv: the active ray's
+        const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
         const float et = __fmul_rn( ext, ( float ) t );
         bool interact = false, peel_cut = false;
         if( peel )
@@ -280,9 +293,9 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             }
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
-                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( dd, a ), p.x[ a ] );
+                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
             const int b_old = p.b;
-            left = ! cross_face( P.m, p.b, p.c, p.x, ax, comp( dd, ax ) > 0.0f, lost );
+            left = ! cross_cached( P.m, p.b, p.c, p.x, fx, ax, p.d, lost );
             if( ! left && p.b != b_old ) count( sp, KP_CNT_HOPS );
         }
         if( peel )
@@ -308,6 +321,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                     {
                         pG = G; ptau = 0.f; pk = 0;
                         ray = RAY_DEPOSIT;          // the walk position stays parked
+                        faces_all( P.m, p.b, p.c, p.d, fx );   // p.d is still o
                         continue;
                     }
                 }
@@ -322,9 +336,12 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             else if( nv > 0 )
                 R = __dsub_rn( R, ( double ) pG );   // deposit ray of vertex nv done
             unpark_walk( sp, p );
+            unpark_dir( sd, p );
             ray = RAY_WALK;
             if( pend )
                 end_packet(  );
+            else
+                faces_all( P.m, p.b, p.c, p.d, fx );
             continue;
         }
         if( left || p.n_steps >= P.max_steps )
