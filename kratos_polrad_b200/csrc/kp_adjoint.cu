@@ -104,21 +104,104 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         }
     };
 
+    // After the active ray crossed a face (or stopped): the end of a peel-off
+    // ray (measure / deposit bookkeeping, walk resumes) or of the walk.
+    // Shared by the segment phase and the hand-off phase.
+    auto after_crossing = [ & ]( bool peel_cut, bool left, bool lost )
+    {
+        if( ray != RAY_WALK )
+        {
+            if( !( peel_cut || left || pk >= ( 1 << 20 ) ) )
+                return;
+            if( ray == RAY_MEASURE )
+            {
+                float G = 0.0f;
+                if( ptau <= P.tau_cut )
+                {
+                    const float att = __fmul_rn( sp.w[ th ],
+                                                 ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    G = score( P, sp.pix[ th ], __fmul_rn( att, sp.I[ th ] ),
+                               __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
+                               __fmul_rn( att, sp.V[ th ] ) );
+                }
+                if( remeasure )
+                {   // pass 1, vertex beyond the stored ones: now deposit along it
+                    remeasure = false;
+                    unpark_walk( sp, p );
+                    if( G != 0.0f )
+                    {
+                        pG = G; ptau = 0.f; pk = 0;
+                        ray = RAY_DEPOSIT;          // the walk position stays parked
+                        faces_all( P.m, p.b, p.c, p.d, fx );   // p.d is still o
+                        return;
+                    }
+                }
+                else if( nv == 0 )
+                    G0 = G;                          // emission
+                else
+                {
+                    R = __dadd_rn( R, ( double ) G );
+                    if( nv <= ADJ_KMAX ) gk[ nv - 1 ] = G;
+                }
+            }
+            else if( nv > 0 )
+                R = __dsub_rn( R, ( double ) pG );   // deposit ray of vertex nv done
+            unpark_walk( sp, p );
+            unpark_dir( sd, p );
+            ray = RAY_WALK;
+            if( pend )
+                end_packet(  );
+            else
+                faces_all( P.m, p.b, p.c, p.d, fx );
+            return;
+        }
+        if( left || p.n_steps >= P.max_steps )
+        {
+            if( left )
+                count( sp, lost ? KP_CNT_LOST : KP_CNT_ESCAPED );
+            else
+                count( sp, KP_CNT_CAPPED );
+            end_packet(  );
+        }
+    };
+    int hop_ax = 0;                               // face axis of a pending hand-off
+
     for( ;; )
     {
         const unsigned m_emit = __ballot_sync( FULL, phase == PH_EMIT );
         const unsigned m_seg  = __ballot_sync( FULL, phase == PH_SEGMENT );
         const unsigned m_ev   = __ballot_sync( FULL, phase == PH_EVENT );
-        if( ( m_emit | m_seg | m_ev ) == 0u )
+        const unsigned m_hop  = __ballot_sync( FULL, phase == PH_HOP );
+        if( ( m_emit | m_seg | m_ev | m_hop ) == 0u )
             break;
         const int n_seg = __popc( m_seg ), n_ev = __popc( m_ev ), n_emit = __popc( m_emit );
+        const int n_hop = __popc( m_hop );
         int run;
         if( n_ev > 0 && ( n_ev >= P.ev_batch || n_seg == 0 ) )
             run = PH_EVENT;
         else if( n_emit > 0 && ( n_emit >= P.ev_batch || n_seg == 0 ) )
             run = PH_EMIT;
+        else if( n_hop > 0 && ( n_hop >= P.hop_batch || n_seg == 0 ) )
+            run = PH_HOP;
         else
             run = PH_SEGMENT;
+
+        if( run == PH_HOP )
+        {   // batched block hand-offs (see k_forward)
+            if( phase != PH_HOP ) continue;
+            const int b_old = p.b;
+            bool lost;
+            const bool left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax,
+                                            comp( p.d, hop_ax ) > 0.0f, lost );
+            if( ! left )
+            {
+                faces_all( P.m, p.b, p.c, p.d, fx );
+                if( p.b != b_old ) count( sp, KP_CNT_HOPS );
+            }
+            phase = PH_SEGMENT;
+            after_crossing( false, left, lost );
+            continue;
+        }
 
         if( run == PH_EMIT )
         {
@@ -282,7 +365,6 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             phase = PH_EVENT;
             continue;
         }
-        bool left = false, lost = false;
         if( ! peel_cut )
         {
             if( ! peel )
@@ -294,64 +376,14 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
                 if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
-            const int b_old = p.b;
-            left = ! cross_cached( P.m, p.b, p.c, p.x, fx, ax, p.d, lost );
-            if( ! left && p.b != b_old ) count( sp, KP_CNT_HOPS );
-        }
-        if( peel )
-        {
-            if( !( peel_cut || left || pk >= ( 1 << 20 ) ) )
+            if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
+            {   // leaves the block: wait for a batched hand-off
+                hop_ax = ax;
+                phase = PH_HOP;
                 continue;
-            if( ray == RAY_MEASURE )
-            {
-                float G = 0.0f;
-                if( ptau <= P.tau_cut )
-                {
-                    const float att = __fmul_rn( sp.w[ th ],
-                                                 ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                    G = score( P, sp.pix[ th ], __fmul_rn( att, sp.I[ th ] ),
-                               __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
-                               __fmul_rn( att, sp.V[ th ] ) );
-                }
-                if( remeasure )
-                {   // pass 1, vertex beyond the stored ones: now deposit along it
-                    remeasure = false;
-                    unpark_walk( sp, p );
-                    if( G != 0.0f )
-                    {
-                        pG = G; ptau = 0.f; pk = 0;
-                        ray = RAY_DEPOSIT;          // the walk position stays parked
-                        faces_all( P.m, p.b, p.c, p.d, fx );   // p.d is still o
-                        continue;
-                    }
-                }
-                else if( nv == 0 )
-                    G0 = G;                          // emission
-                else
-                {
-                    R = __dadd_rn( R, ( double ) G );
-                    if( nv <= ADJ_KMAX ) gk[ nv - 1 ] = G;
-                }
             }
-            else if( nv > 0 )
-                R = __dsub_rn( R, ( double ) pG );   // deposit ray of vertex nv done
-            unpark_walk( sp, p );
-            unpark_dir( sd, p );
-            ray = RAY_WALK;
-            if( pend )
-                end_packet(  );
-            else
-                faces_all( P.m, p.b, p.c, p.d, fx );
-            continue;
         }
-        if( left || p.n_steps >= P.max_steps )
-        {
-            if( left )
-                count( sp, lost ? KP_CNT_LOST : KP_CNT_ESCAPED );
-            else
-                count( sp, KP_CNT_CAPPED );
-            end_packet(  );
-        }
+        after_crossing( peel_cut, false, false );
     }
     count( sp, KP_CNT_STEPS, cnt.steps );
     count( sp, KP_CNT_PEEL_STEPS, cnt.peel );

@@ -21,11 +21,15 @@ namespace cg = cooperative_groups;
 // Warp-synchronous scheduler.  Each lane carries one packet through a small
 // state machine: EMIT (needs a packet), SEGMENT (advance its active ray by
 // one cell segment: the packet's own walk, or a peel-off ray toward the
-// observer), EVENT (an interaction to process).  Every iteration the warp
-// ballots the lane phases and runs ONE phase for all lanes in it: events and
-// emissions, which are long and rare, wait until at least `ev_batch` lanes
-// need them (or no lane can step), so their code runs with many lanes
-// active; segments, which are short and frequent, run otherwise.  A peel-off
+// observer), EVENT (an interaction to process), HOP (its ray left the block:
+// neighbour lookup and the new block's geometry).  Every iteration the warp
+// ballots the lane phases and runs ONE phase for all lanes in it: events,
+// emissions and hand-offs, which are long and rare, wait until at least
+// `ev_batch` (hand-offs: `hop_batch`) lanes need them, or no lane can step,
+// so their code runs with many lanes active and their dependent loads are
+// paid once per batch; segments, which are short and frequent, run
+// otherwise.  A hand-off left inline cost as much as 11 segments, because
+// the whole warp waited on one lane's chain of dependent loads.  A peel-off
 // ray starts at an emission or interaction point: the walk position is
 // parked, the ray marches to the boundary (or beyond tau_cut), its
 // contribution is deposited and the walk resumes.  Peel-off rays draw no
@@ -54,22 +58,107 @@ k_forward( const __grid_constant__ fwd_params_t P )
     float ptau = 0;
     int pk = 0, pend = 0;
     int si = 0;                                   // scene of a batched launch
+    int hop_ax = 0;                               // face axis of a pending hand-off
+
+    // After the active ray crossed a face (or stopped): the end of a peel-off
+    // ray (deposit, walk resumes) or of the packet's walk (escape, step cap).
+    // Shared by the segment phase and the hand-off phase.
+    auto after_crossing = [ & ]( bool peel_cut, bool left, bool lost )
+    {
+        if( peel )
+        {
+            if( peel_cut || left || pk >= ( 1 << 20 ) )
+            {
+                if( ptau <= P.tau_cut )
+                {
+                    const int th = threadIdx.x;
+                    const float att = __fmul_rn( sp.w[ th ],
+                                                 ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    deposit_pixel< TALLY >( P, sp.pix[ th ], sd.cpix[ th ], __fmul_rn( att, sp.I[ th ] ),
+                                            __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
+                                            __fmul_rn( att, sp.V[ th ] ) );
+                    count( sp, KP_CNT_DEPOSITS );
+                }
+                unpark_walk( sp, p );
+                unpark_dir( sd, p );
+                faces_all( P.m, p.b, p.c, p.d, fx );
+                peel = false;
+                if( pend )
+                {
+                    load_cold( sc, p, P.seed );
+                    write_record( P, p, pend );
+                    count( sp, pend == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
+                    phase = PH_EMIT;
+                }
+            }
+            return;
+        }
+        int end = 0;
+        if( left )
+        {
+            load_cold( sc, p, P.seed );
+            if( lost )
+                end = PK_LOST;
+            else
+            {
+                end = PK_ESCAPED;
+                if( tally_escape< TALLY >( P, ( char * ) P.mu_tally + ( size_t ) si * P.mu_scene_stride
+                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), p,
+                                             sc.batch[ threadIdx.x ] ) )
+                    count( sp, KP_CNT_DEPOSITS );
+            }
+        }
+        else if( p.n_steps >= P.max_steps )
+        {
+            load_cold( sc, p, P.seed );
+            end = PK_STEP_CAP;
+        }
+        if( end )
+        {
+            write_record( P, p, end );
+            count( sp, end == PK_ESCAPED ? KP_CNT_ESCAPED
+                     : ( end == PK_LOST ? KP_CNT_LOST : KP_CNT_CAPPED ) );
+            phase = PH_EMIT;
+        }
+    };
 
     for( ;; )
     {
         const unsigned m_emit = __ballot_sync( FULL, phase == PH_EMIT );
         const unsigned m_seg  = __ballot_sync( FULL, phase == PH_SEGMENT );
         const unsigned m_ev   = __ballot_sync( FULL, phase == PH_EVENT );
-        if( ( m_emit | m_seg | m_ev ) == 0u )
+        const unsigned m_hop  = __ballot_sync( FULL, phase == PH_HOP );
+        if( ( m_emit | m_seg | m_ev | m_hop ) == 0u )
             break;
         const int n_seg = __popc( m_seg ), n_ev = __popc( m_ev ), n_emit = __popc( m_emit );
+        const int n_hop = __popc( m_hop );
         int run;
         if( n_ev > 0 && ( n_ev >= P.ev_batch || n_seg == 0 ) )
             run = PH_EVENT;
         else if( n_emit > 0 && ( n_emit >= P.ev_batch || n_seg == 0 ) )
             run = PH_EMIT;
+        else if( n_hop > 0 && ( n_hop >= P.hop_batch || n_seg == 0 ) )
+            run = PH_HOP;
         else
             run = PH_SEGMENT;
+
+        if( run == PH_HOP )
+        {   // block hand-offs of the lanes that left their block, together:
+            // neighbour lookup and the new block's geometry in one batch
+            if( phase != PH_HOP ) continue;
+            const int b_old = p.b;
+            bool lost;
+            const bool left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax,
+                                            comp( p.d, hop_ax ) > 0.0f, lost );
+            if( ! left )
+            {
+                faces_all( P.m, p.b, p.c, p.d, fx );
+                if( p.b != b_old ) count( sp, KP_CNT_HOPS );
+            }
+            phase = PH_SEGMENT;
+            after_crossing( false, left, lost );
+            continue;
+        }
 
         if( run == PH_EMIT )
         {
@@ -226,7 +315,6 @@ k_forward( const __grid_constant__ fwd_params_t P )
             ++ p.n_steps;
             interact = et >= p.tau;
         }
-        bool left = false, lost = false;
         if( interact )
         {
             double ti = ( double ) __fdiv_rn( p.tau, ext );
@@ -243,65 +331,14 @@ k_forward( const __grid_constant__ fwd_params_t P )
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
                 if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
-            const int b_old = p.b;
-            left = ! cross_cached( P.m, p.b, p.c, p.x, fx, ax, p.d, lost );
-            if( ! left && p.b != b_old ) count( sp, KP_CNT_HOPS );
-        }
-        if( peel )
-        {
-            if( peel_cut || left || pk >= ( 1 << 20 ) )
-            {
-                if( ptau <= P.tau_cut )
-                {
-                    const int th = threadIdx.x;
-                    const float att = __fmul_rn( sp.w[ th ],
-                                                 ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                    deposit_pixel< TALLY >( P, sp.pix[ th ], sd.cpix[ th ], __fmul_rn( att, sp.I[ th ] ),
-                                            __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
-                                            __fmul_rn( att, sp.V[ th ] ) );
-                    count( sp, KP_CNT_DEPOSITS );
-                }
-                unpark_walk( sp, p );
-                unpark_dir( sd, p );
-                faces_all( P.m, p.b, p.c, p.d, fx );
-                peel = false;
-                if( pend )
-                {
-                    load_cold( sc, p, P.seed );
-                    write_record( P, p, pend );
-                    count( sp, pend == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
-                    phase = PH_EMIT;
-                }
-            }
-            continue;
-        }
-        int end = 0;
-        if( left )
-        {
-            load_cold( sc, p, P.seed );
-            if( lost )
-                end = PK_LOST;
-            else
-            {
-                end = PK_ESCAPED;
-                if( tally_escape< TALLY >( P, ( char * ) P.mu_tally + ( size_t ) si * P.mu_scene_stride
-                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), p,
-                                             sc.batch[ threadIdx.x ] ) )
-                    count( sp, KP_CNT_DEPOSITS );
+            if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
+            {   // leaves the block: wait for a batched hand-off
+                hop_ax = ax;
+                phase = PH_HOP;
+                continue;
             }
         }
-        else if( p.n_steps >= P.max_steps )
-        {
-            load_cold( sc, p, P.seed );
-            end = PK_STEP_CAP;
-        }
-        if( end )
-        {
-            write_record( P, p, end );
-            count( sp, end == PK_ESCAPED ? KP_CNT_ESCAPED
-                     : ( end == PK_LOST ? KP_CNT_LOST : KP_CNT_CAPPED ) );
-            phase = PH_EMIT;
-        }
+        after_crossing( peel_cut, false, false );
     }
     count( sp, KP_CNT_STEPS, cnt.steps );
     count( sp, KP_CNT_PEEL_STEPS, cnt.peel );
@@ -382,6 +419,10 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     P.max_scatter = c.max_scatter;
     P.max_steps = std::min< long long >( c.max_steps, 0x7fffffff );
     P.ev_batch = c.lane_batch > 0 ? c.lane_batch : 6;
+    // Block hand-offs wait for 8 lanes (measured best on AMR and on uniform
+    // scenes, whatever the event batch): the neighbour lookup and the new
+    // block's geometry are dependent loads, paid once per batch.
+    P.hop_batch = 8;
     P.mu_tally = t.mu;
     P.image = t.image;
     P.img_batch = t.image_batch;

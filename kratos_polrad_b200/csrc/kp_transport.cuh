@@ -63,6 +63,7 @@ struct fwd_params_t
     int         max_scatter;
     long long   max_steps;
     int         ev_batch;          // lanes that must wait for an event batch
+    int         hop_batch;         // lanes that must wait for a hand-off batch
     double      lk_inv[ 3 ];       // lookup cells per unit length
     void      * mu_tally;
     void      * image;
@@ -176,8 +177,11 @@ __device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int 
             }
         return true;
     }
-    const blk_meta_t md = m.meta[ b ];
     const int side = pos ? 1 : 0;
+    // the face's four neighbour slots (16-byte aligned: 24 ints per block),
+    // loaded together with the meta record, not after it
+    const int4 q = reinterpret_cast< const int4 * >( m.nb + 24 * ( size_t ) b )[ ax * 2 + side ];
+    const blk_meta_t md = m.meta[ b ];
     if( ( md.phybnd >> ( 2 * ax + side ) ) & 1 )
         return false;
     const int a1 = ax == 2 ? 0 : ax + 1;
@@ -191,7 +195,8 @@ __device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int 
         j0 = ca1 >= m.nc[ a1 ] / 2;
         j1 = ca2 >= m.nc[ a2 ] / 2;
     }
-    const int nid = m.nb[ 24 * ( size_t ) b + ( ( ax * 2 + side ) * 2 + j0 ) * 2 + j1 ];
+    const int js = j0 * 2 + j1;
+    const int nid = js == 0 ? q.x : ( js == 1 ? q.y : ( js == 2 ? q.z : q.w ) );
     if( nid < 0 || nid >= m.n_blocks )
     {
         lost = true;
@@ -247,6 +252,27 @@ __device__ __forceinline__ double exit_cached( const double x[ 3 ], const double
         if( ta < t ) { t = ta; ax = a; }
     }
     return t;
+}
+
+// The in-block half of cross_cached: steps into the next cell across face
+// `ax` when it lies in the same block (x snaps to the cached face, one new
+// face is computed) and returns true; returns false, changing nothing, when
+// the step leaves the block.
+__device__ __forceinline__ bool step_in_block( const mesh_view_t & m, int b, int c[ 3 ],
+                                               double x[ 3 ], double fx[ 3 ], int ax,
+                                               const phys::v3 & d )
+{
+    const bool pos = comp( d, ax ) > 0.0f;
+    const int cax = ax == 0 ? c[ 0 ] : ( ax == 1 ? c[ 1 ] : c[ 2 ] );
+    const int cn = cax + ( pos ? 1 : -1 );
+    if( cn < 0 || cn >= m.nc[ ax ] )
+        return false;
+    const double * g = m.geo_d + 16 * ( size_t ) b;
+    const double nf = __fma_rn( ( double ) ( cn + ( pos ? 1 : 0 ) ), g[ 3 + ax ], g[ ax ] );
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+        if( a == ax ) { c[ a ] = cn; x[ a ] = fx[ a ]; fx[ a ] = nf; }
+    return true;
 }
 
 // cross_face with the face cache: inside the block the crossed face is the
@@ -550,7 +576,8 @@ __device__ __forceinline__ void write_record( const fwd_params_t & P, const pack
 }
 
 // Lane phases of the warp-synchronous transport kernels.
-enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3 };
+enum lane_phase { PH_EMIT = 0, PH_SEGMENT = 1, PH_EVENT = 2, PH_DONE = 3,
+                  PH_HOP = 4 };          // waits for a batched block hand-off
 
 // Segment counts stay in registers (32-bit: a thread walks far fewer than
 // 2^32 segments in one launch); rare events are counted in shared memory.
