@@ -146,6 +146,33 @@ int kp_mesh_sigma_ptr( kp_mesh_t * mesh, float ** sigma );
 int kp_mesh_status( kp_mesh_t * mesh, void * stream, unsigned * flags );
 
 /* ------------------------------------------------------------------ */
+/* Runtime refinement.  The reference declares the hook and leaves it   */
+/* empty: mesh_t::changed (mesh/mesh.cpp:86-89), meshgen::base_t::update */
+/* (mesh/meshgen/meshgen.cpp:443-446); block_map_t::update              */
+/* (modules/particle/types/block_map.h:53-103) would rebuild the        */
+/* neighbour tables.                                                    */
+
+/* Per-block flags (device int[n_blocks]) from the mesh's coefficients:  */
+/* +1 where some cell's extinction depth across the block's widest cell */
+/* side exceeds tau_refine, -1 where every cell's stays below           */
+/* tau_coarsen, else 0. */
+int kp_mesh_flag_tau( kp_mesh_t * mesh, float tau_refine, float tau_coarsen, int * flags,
+                      void * stream );
+/* New mesh (*out, coefficients not set) from `mesh` and host flags
+ * int[n_blocks]: blocks flagged > 0 are replaced by their eight children,
+ * families whose eight blocks are leaves flagged < 0 by their parent; the
+ * 2:1 balance of static refinement is then restored, a refinement winning
+ * over a coarsening it would break.  The result equals the mesh built from
+ * one [refine_region*] box per resulting leaf. */
+int kp_mesh_adapt( const kp_mesh_t * mesh, const int * flags, kp_mesh_t ** out );
+/* Per-cell field of n_comp floats (device, block-id order) from mesh `from`
+ * to mesh `to` of the same domain: a `to` cell inside one `from` cell takes
+ * its value; a `to` cell covering several (coarsened) takes the mean of the
+ * eight octant samples.  E.g. n_comp = 2 for the coefficients. */
+int kp_mesh_remap( kp_mesh_t * from, kp_mesh_t * to, int n_comp, const float * src, float * dst,
+                   void * stream );
+
+/* ------------------------------------------------------------------ */
 /* Geometric walk with the path-length flux estimator.  Replaces        */
 /* integrate::base_t::intg / ker_itg (modules/particle/evolve/          */
 /* integrator.h:11-17,47-63,80-106) running photon::cart_t::proc        */

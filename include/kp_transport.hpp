@@ -179,6 +179,24 @@ public:
                              cell.data(  )->data(  ) ) );
     }
     void upload(  ) { api( kp_mesh_upload( m_ ) ); }
+    // Runtime refinement: host flags per block (+1 refine, -1 coarsen a whole
+    // family, 0 keep) -> a new mesh with the 2:1 balance restored.
+    mesh_t adapt( const std::vector< int > & flags ) const
+    {
+        kp_mesh_t * out = nullptr;
+        api( kp_mesh_adapt( m_, flags.data(  ), & out ) );
+        return mesh_t( out );
+    }
+    // Device flags from the coefficients (optical depth across a cell).
+    void flag_tau( float tau_refine, float tau_coarsen, int * d_flags, stream_t s = nullptr )
+    {
+        api( kp_mesh_flag_tau( m_, tau_refine, tau_coarsen, d_flags, s ) );
+    }
+    // Per-cell device field (n_comp floats per cell) of this mesh onto `to`.
+    void remap_to( mesh_t & to, int n_comp, const float * src, float * dst, stream_t s = nullptr )
+    {
+        api( kp_mesh_remap( m_, to.m_, n_comp, src, dst, s ) );
+    }
     // (sigma_sca, sigma_abs) per cell, block-id order, x fastest
     void set_sigma( const float * src, long long n_values, bool on_device = false,
                     stream_t s = nullptr )
@@ -197,6 +215,7 @@ public:
     }
 
 private:
+    explicit mesh_t( kp_mesh_t * m ) : m_( m ) {  }
     kp_mesh_t * m_ = nullptr;
 };
 

@@ -95,6 +95,9 @@ _SIGS = {
     "kp_mesh_set_sigma": [c_void_p, c_void_p, c_ll, c_int, c_void_p],
     "kp_mesh_sigma_ptr": [c_void_p, P(c_void_p)],
     "kp_mesh_status": [c_void_p, c_void_p, P(ctypes.c_uint)],
+    "kp_mesh_flag_tau": [c_void_p, c_float, c_float, c_void_p, c_void_p],
+    "kp_mesh_adapt": [c_void_p, c_void_p, P(c_void_p)],
+    "kp_mesh_remap": [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p],
     "kp_trace": [c_void_p, c_int, c_ll, c_void_p, c_void_p, c_void_p, c_void_p,
                  c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p],
 }

@@ -50,8 +50,9 @@ mesh_desc_t mesh_desc_from_ini( const ini_t & ini )
 ////////////////////////////////////////////////////////////
 // Tree construction
 
-block_tree_t::block_tree_t( const mesh_desc_t & desc ) : desc_( desc )
+void block_tree_t::init_domain(  )
 {
+    const mesh_desc_t & desc = desc_;
     n_dim_ = 0;
     for( int a = 0; a < 3; ++ a )
         if( desc.n_cell_global[ a ] > 1 )
@@ -69,7 +70,11 @@ block_tree_t::block_tree_t( const mesh_desc_t & desc ) : desc_( desc )
             throw std::runtime_error( "x_max must exceed x_min" );
         lim_[ a ] = ng / nb;
     }
+}
 
+block_tree_t::block_tree_t( const mesh_desc_t & desc ) : desc_( desc )
+{
+    init_domain(  );
     // Static refinement: every block of every box is forced to the box's
     // level (meshgen.cpp:144-163); insert() keeps the 2:1 balance.
     for( const auto & r : desc.refine )
@@ -90,6 +95,29 @@ block_tree_t::block_tree_t( const mesh_desc_t & desc ) : desc_( desc )
             for( int j = lo[ 1 ]; j <= hi[ 1 ]; ++ j )
                 for( int i = lo[ 0 ]; i <= hi[ 0 ]; ++ i )
                     insert( { r.level, { i, j, k } } );
+    }
+    for( int k = 0; k < lim_[ 2 ]; ++ k )
+        for( int j = 0; j < lim_[ 1 ]; ++ j )
+            for( int i = 0; i < lim_[ 0 ]; ++ i )
+                nodes_[ { 0, { i, j, k } } ];
+    build_tables(  );
+}
+
+block_tree_t::block_tree_t( const mesh_desc_t & desc, const std::vector< region_key_t > & keys )
+    : desc_( desc )
+{
+    desc_.refine.clear(  );
+    init_domain(  );
+    for( const auto & k0 : keys )
+    {
+        if( k0.level < 0 || k0.level > 20 )
+            throw std::runtime_error( "refinement level outside 0..20" );
+        region_key_t k = k0;
+        for( int a = 0; a < 3; ++ a )
+            if( k.i[ a ] < 0 || k.i[ a ] >= blocks_at( k.level, a ) )
+                throw std::runtime_error( "block index outside the domain" );
+        if( k.level > 0 )
+            insert( k );
     }
     for( int k = 0; k < lim_[ 2 ]; ++ k )
         for( int j = 0; j < lim_[ 1 ]; ++ j )
@@ -299,6 +327,12 @@ void block_tree_t::build_tables(  )
         }
     }
     const int L = t.max_level;
+    double n_lookup = 1.0;
+    for( int a = 0; a < 3; ++ a )
+        n_lookup *= std::ldexp( ( double ) lim_[ a ], L );
+    if( n_lookup > ( double ) ( 1 << 28 ) )
+        throw std::runtime_error( "finest-level lookup grid too large (more than 2^28 "
+                                  "block positions): too many refinement levels" );
     for( int a = 0; a < 3; ++ a )
         t.lookup_n[ a ] = blocks_at( L, a );
     t.lookup.assign( ( size_t ) t.lookup_n[ 0 ] * t.lookup_n[ 1 ] * t.lookup_n[ 2 ], -1 );

@@ -93,6 +93,10 @@ class block_tree_t
 {
 public:
     explicit block_tree_t( const mesh_desc_t & desc );
+    // Tree whose leaves include `keys` (each inserted with the 2:1 closure,
+    // as a refine box covering one block at its level would insert it);
+    // desc.refine is not used.  The runtime refinement path.
+    block_tree_t( const mesh_desc_t & desc, const std::vector< region_key_t > & keys );
 
     const block_tables_t & tables(  ) const { return tab_; }
     const mesh_desc_t    & desc  (  ) const { return desc_; }
@@ -108,6 +112,7 @@ public:
 private:
     struct node_t { bool refined = false; int id = -1; };
 
+    void   init_domain(  );                          // checks desc_, sets lim_
     void   insert( const region_key_t & k );
     bool   inside( region_key_t & k ) const;         // wraps periodic axes
     int    blocks_at( int level, int a ) const;      // blocks per axis

@@ -54,9 +54,12 @@ class MeshConfig:
 class Mesh:
     """Owns a ``kp_mesh_t``; building needs no GPU."""
 
-    def __init__(self, cfg: MeshConfig | None = None, ini_path: str | None = None):
+    def __init__(self, cfg: MeshConfig | None = None, ini_path: str | None = None,
+                 _handle: ctypes.c_void_p | None = None):
         h = ctypes.c_void_p()
-        if ini_path is not None:
+        if _handle is not None:
+            h = _handle
+        elif ini_path is not None:
             call("kp_mesh_create_ini", ini_path.encode(), ctypes.byref(h))
         else:
             d = _lib.MeshDesc()
@@ -137,7 +140,49 @@ class Mesh:
         n = int(np.prod(sigma2.shape))
         call("kp_mesh_set_sigma", self.handle, ptr(sigma2), n, on_dev, None)
 
+    # ---- runtime refinement ----
+    def flag_tau(self, tau_refine: float, tau_coarsen: float = 0.0, stream=None):
+        """Per-block flags on the device (int32 tensor): +1 where a cell's
+        extinction depth across the widest cell side exceeds ``tau_refine``,
+        -1 where all stay below ``tau_coarsen``, else 0."""
+        import torch
+        flags = torch.empty(self.n_blocks, dtype=torch.int32, device="cuda")
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        call("kp_mesh_flag_tau", self.handle, float(tau_refine), float(tau_coarsen), ptr(flags), s)
+        return flags
+
+    def adapt(self, flags) -> "Mesh":
+        """New mesh: blocks flagged > 0 refined, families of eight leaves all
+        flagged < 0 coarsened, 2:1 balance restored (host; needs no GPU)."""
+        f = np.ascontiguousarray(_host(flags), np.int32).reshape(-1)
+        if f.size != self.n_blocks:
+            raise ValueError(f"need {self.n_blocks} flags, got {f.size}")
+        h = ctypes.c_void_p()
+        call("kp_mesh_adapt", self.handle, ptr(f), ctypes.byref(h))
+        return Mesh(_handle=h)
+
+    def remap_to(self, other: "Mesh", field, stream=None):
+        """Per-cell field [n_cells, n_comp] (CUDA tensor, float32) of this mesh
+        carried onto ``other`` (same domain): copy where a cell of ``other``
+        lies in one cell here, mean of eight octant samples where it covers
+        several."""
+        import torch
+        src = field.to(torch.float32).contiguous()
+        n_comp = 1 if src.dim() == 1 else src.shape[1]
+        if src.shape[0] != self.n_cells:
+            raise ValueError("field must have n_cells rows")
+        dst = torch.empty((other.n_cells, n_comp), dtype=torch.float32, device=src.device)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        call("kp_mesh_remap", self.handle, other.handle, n_comp, ptr(src), ptr(dst), s)
+        return dst if src.dim() > 1 else dst[:, 0]
+
     def status(self, stream=None) -> int:
         flags = ctypes.c_uint()
         call("kp_mesh_status", self.handle, stream, ctypes.byref(flags))
         return flags.value
+
+
+def _host(a):
+    if hasattr(a, "detach"):
+        return a.detach().cpu().numpy()
+    return np.asarray(a)
