@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--packets", type=float, default=1e7)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="clump", choices=["clump", "batched", "diff", "large"])
+    p.add_argument("--workload", default="clump", choices=["clump", "batched", "diff", "large", "decomp"])
     return p.parse_args()
 
 
@@ -463,6 +463,51 @@ def run_diff(args):
     print(json.dumps(line), flush=True)
 
 
+def run_decomp(args):
+    """Domain-decomposed solve of the clump scene: the blocks split over 4
+    ranks (Z-order runs), each holding only its own coefficients, emulated one
+    after another on this GPU with the out-queues moved by device copies;
+    against the replicated solve of the same packets (tallies must agree bit
+    for bit).  Under torchrun each process is one rank (NCCL all-to-all)."""
+    import torch
+    import torch.distributed as dist
+    from kratos_polrad_b200 import decomp, scenes, shard
+    from kratos_polrad_b200.transport import Tallies, forward
+    rank, world, _ = _init_ranks()
+    n_pk = int(args.packets)
+    mesh, sig, cfg = scenes.clump_amr(n_packets=n_pk)
+    mesh.set_sigma(sig)
+    ref = forward(mesh, cfg, Tallies(cfg))
+    torch.cuda.synchronize()
+    _, t_rep = _timed(lambda: forward(mesh, cfg, Tallies(cfg)))
+    n_ranks = 4 if world == 1 else world
+    if world == 1:
+        decomp.solve_emulated(mesh, sig, dataclasses.replace(cfg, n_packets=min(n_pk, 100_000)),
+                              n_ranks)
+        (tal, rounds), t_dd = _timed(lambda: decomp.solve_emulated(mesh, sig, cfg, n_ranks))
+    else:
+        dist.barrier()
+        (tal, rounds), t_dd = _timed(lambda: decomp.solve_distributed(mesh, sig, cfg))
+        t = torch.tensor([t_dd], dtype=torch.float64, device="cuda")
+        shard_max(t)
+        t_dd = float(t.item())
+        shard.reduce_tallies([ref.image, ref.mu, ref.image_batch, ref.counters])
+    same = all(bool(torch.equal(getattr(tal, k), getattr(ref, k)))
+               for k in ("mu", "image", "image_batch", "counters"))
+    c = tal.counts()
+    if rank == 0:
+        line = {"metric": "packet-steps/s, decomposed clump solve", "unit": UNIT,
+                "value": (c["steps"] + c["peel_steps"]) / (t_dd / 1e3), "higher_is_better": True,
+                "n_gpus": world, "config": {"workload": "clump_amr_2level_decomposed",
+                                            "packets": n_pk, "ranks": n_ranks,
+                                            "ranks_emulated_on_one_gpu": world == 1,
+                                            "blocks": mesh.n_blocks},
+                "rounds": rounds, "decomposed_ms": t_dd, "replicated_ms": t_rep,
+                "tallies_identical_to_replicated": same}
+        print(json.dumps(line), flush=True)
+    _finish_ranks(world)
+
+
 def run_large(args):
     """Large workload: 256^3 root, 3 levels on a lognormal field (std of ln
     rho 1.5, seed 5; ~2e7 cells, 166 MB of coefficients: beyond L2), HG g=0.6
@@ -508,6 +553,8 @@ def main():
         return run_diff(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "decomp":
+        return run_decomp(args)
     if args.impl == "reference":     # host cores only: rank 0 runs, the others exit
         run_reference(args, int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)))
         return

@@ -397,6 +397,56 @@ int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transport_cfg_t * c
                                   const kp_tallies_t * tallies, void * stream );
 
 /* ------------------------------------------------------------------ */
+/* Domain-decomposed solve: packet migration between ranks that each    */
+/* own part of the blocks, for meshes too large to replicate.  Replaces */
+/* the reference's off-rank registration and exchange loop              */
+/* (modules/particle/boundary/comm.h:118-239, comm_t::reg/proc/cpy_d)   */
+/* with device queues exchanged between rounds (kratos_polrad_b200/     */
+/* decomp.py: NCCL all-to-all, or device copies for ranks emulated on   */
+/* one GPU).  Every rank holds the block tables of the whole mesh and   */
+/* the coefficients of its own blocks.                                  */
+
+#define KP_DD_WALK_BYTES 128   /* one migrating walk (full packet state)       */
+#define KP_DD_PEEL_BYTES 96    /* one migrating peel-off ray (and its deposit) */
+
+typedef struct kp_dd_round
+{
+    int         rank, n_ranks;
+    const int * owner;          /* device int[n_blocks]: owning rank            */
+    const int * block_local;    /* device int[n_blocks]: index among this rank's
+                                   blocks, -1 for other ranks' blocks           */
+    const float * sigma_local;  /* device: (sigma_sca, sigma_abs) of this rank's
+                                   blocks, local block order, x fastest         */
+    const void * in_walk;       /* device records arriving from other ranks     */
+    long long    n_in_walk;
+    const void * in_peel;
+    long long    n_in_peel;
+    int          emit;          /* 1 in the first round: emit this rank's share  */
+    void *       out_walk;      /* device [cap_walk] records leaving this rank   */
+    int *        out_walk_rank; /* device [cap_walk] destination rank of each    */
+    long long    cap_walk;
+    void *       out_peel;      /* device [cap_peel] records                     */
+    int *        out_peel_rank; /* device [cap_peel]                             */
+    long long    cap_peel;
+    unsigned long long * out_count;  /* device [2] (walks, peel-off rays written,
+                                        in any order), zeroed by the caller; a
+                                        count above its capacity means lost
+                                        records (kp_mesh_status: queue overflow) */
+} kp_dd_round_t;
+
+/* One round on this rank: processes the incoming records and (emit) the
+ * rank's emissions of cfg's packets (the same cfg on every rank: point-source
+ * packets are emitted by the rank owning the source's block, plane-source
+ * packets by the rank pid % n_ranks), and writes every ray that crosses into
+ * another rank's block to that rank's out-queue.  Tallies accumulate on this
+ * rank; summed over the ranks after the last round (no records left
+ * anywhere) they equal kp_transport_forward's, bit for bit in fixed point.
+ * cfg->n_record must be 0. */
+int kp_transport_forward_dd( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                             const kp_dd_round_t * round, const kp_tallies_t * tallies,
+                             void * stream );
+
+/* ------------------------------------------------------------------ */
 /* Binary container of the reference's binary_io (io/binary/            */
 /* binary_io.h:6-32; save/load in binary_io_base.cpp:89-131): a byte of */
 /* (little-endian | sizeof(size_t)), the header size, a tag-sorted map  */

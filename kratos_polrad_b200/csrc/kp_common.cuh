@@ -133,7 +133,9 @@ struct kp_mesh
     unsigned long long * d_work = nullptr;   // scratch: packet counters
 
     kp::mesh_view_t view(  ) const;
-    unsigned long long * workspace(  ) { upload(  ); return d_work; }
-    void upload(  );
+    unsigned long long * workspace(  ) { upload( false ); return d_work; }
+    // Copies the tables to the current device; with_sigma also allocates the
+    // (zeroed) coefficient array, which a decomposed rank does not hold.
+    void upload( bool with_sigma = true );
     void release(  );
 };

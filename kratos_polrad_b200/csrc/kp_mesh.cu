@@ -39,7 +39,7 @@ kp::mesh_view_t kp_mesh::view(  ) const
     return v;
 }
 
-void kp_mesh::upload(  )
+void kp_mesh::upload( bool with_sigma )
 {
     int dev = 0;
     KP_CUDA( cudaGetDevice( & dev ) );
@@ -47,6 +47,13 @@ void kp_mesh::upload(  )
     {
         kp::require( dev == device, "mesh was uploaded to another device",
                      KP_ERR_CONFIG );
+        if( with_sigma && d_sigma == nullptr )
+        {
+            const auto & t = tree->tables(  );
+            const size_t n = ( size_t ) t.n_blocks * t.cells_per_block;
+            KP_CUDA( cudaMalloc( & d_sigma, n * sizeof( float2 ) ) );
+            KP_CUDA( cudaMemset( d_sigma, 0, n * sizeof( float2 ) ) );
+        }
         return;
     }
     const auto & t = tree->tables(  );
@@ -85,7 +92,8 @@ void kp_mesh::upload(  )
         KP_CUDA( cudaMemcpy( d_lookup, t.lookup.data(  ), t.lookup.size(  ) * sizeof( int ),
                              cudaMemcpyHostToDevice ) );
         KP_CUDA( cudaMalloc( & d_geo_f,  nb * 8 * sizeof( float ) ) );
-        KP_CUDA( cudaMalloc( & d_sigma,  n_cells * sizeof( float2 ) ) );
+        if( with_sigma )
+            KP_CUDA( cudaMalloc( & d_sigma,  n_cells * sizeof( float2 ) ) );
         KP_CUDA( cudaMalloc( & d_status, 4 * sizeof( unsigned ) ) );
         KP_CUDA( cudaMalloc( & d_work, 32 * sizeof( unsigned long long ) ) );
         KP_CUDA( cudaMemset( d_work, 0, 32 * sizeof( unsigned long long ) ) );
@@ -97,7 +105,8 @@ void kp_mesh::upload(  )
                              cudaMemcpyHostToDevice ) );
         KP_CUDA( cudaMemcpy( d_geo_f, gf.data(  ), gf.size(  ) * sizeof( float ),
                              cudaMemcpyHostToDevice ) );
-        KP_CUDA( cudaMemset( d_sigma, 0, n_cells * sizeof( float2 ) ) );
+        if( with_sigma )
+            KP_CUDA( cudaMemset( d_sigma, 0, n_cells * sizeof( float2 ) ) );
         KP_CUDA( cudaMemset( d_status, 0, 4 * sizeof( unsigned ) ) );
     }
     catch( ... )

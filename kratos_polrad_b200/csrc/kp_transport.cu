@@ -39,7 +39,12 @@ namespace cg = cooperative_groups;
 #define KP_FWD_RESIDENT 768          // resident threads per SM the register budget targets
 #endif
 
-template< int TALLY, int NT >
+// DD: one round of a domain-decomposed solve.  Work items are, in order, the
+// incoming walks, the incoming peel-off rays (run alone: no walk parked) and
+// this rank's emissions; a ray handed off into a block of another rank is
+// written to that rank's out-queue instead of continuing.  Each packet's
+// arithmetic is that of the replicated solve.
+template< int TALLY, int NT, bool DD = false >
 __global__ void __launch_bounds__( NT, KP_FWD_RESIDENT / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
@@ -59,6 +64,25 @@ k_forward( const __grid_constant__ fwd_params_t P )
     int pk = 0, pend = 0;
     int si = 0;                                   // scene of a batched launch
     int hop_ax = 0;                               // face axis of a pending hand-off
+    bool solo = false;                            // DD: peel-off ray without a parked walk
+
+    // coefficients of cell c of block b (DD: owned blocks stored compactly)
+    auto sigma_at = [ & ]( int b, const int c[ 3 ] ) -> float2
+    {
+        if constexpr( DD )
+        {
+            const int l = P.dd_loc[ b ];
+            if( l < 0 )
+            {   // a block of another rank: never read here by construction
+                atomicOr( P.m.status, ST_BAD_BLOCK );
+                return make_float2( 0.0f, 0.0f );
+            }
+            return P.m.sigma[ ( size_t ) l * P.m.cpb + c[ 0 ]
+                              + P.m.nc[ 0 ] * ( c[ 1 ] + P.m.nc[ 1 ] * c[ 2 ] ) ];
+        }
+        else
+            return P.m.sigma[ cell_index( P.m, b, c ) ];
+    };
 
     // After the active ray crossed a face (or stopped): the end of a peel-off
     // ray (deposit, walk resumes) or of the packet's walk (escape, step cap).
@@ -78,6 +102,15 @@ k_forward( const __grid_constant__ fwd_params_t P )
                                             __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
                                             __fmul_rn( att, sp.V[ th ] ) );
                     count( sp, KP_CNT_DEPOSITS );
+                }
+                if constexpr( DD )
+                {
+                    if( solo )
+                    {
+                        peel = false; solo = false;
+                        phase = PH_EMIT;
+                        return;
+                    }
                 }
                 unpark_walk( sp, p );
                 unpark_dir( sd, p );
@@ -152,8 +185,70 @@ k_forward( const __grid_constant__ fwd_params_t P )
                                             comp( p.d, hop_ax ) > 0.0f, lost );
             if( ! left )
             {
-                faces_all( P.m, p.b, p.c, p.d, fx );
                 if( p.b != b_old ) count( sp, KP_CNT_HOPS );
+                if constexpr( DD )
+                {
+                    const int r = P.dd_owner[ p.b ];
+                    // a ray that used its last segment ends here, as in the
+                    // replicated solve (after_crossing below): no hand-over
+                    const bool capped = peel ? pk >= ( 1 << 20 ) : p.n_steps >= P.max_steps;
+                    if( r != P.dd_rank && ! capped )
+                    {   // the ray continues on rank r
+                        const int t = threadIdx.x;
+                        if( peel )
+                        {
+                            const unsigned long long k = atomicAdd( P.dd_out_count + 1, 1ull );
+                            if( k < ( unsigned long long ) P.dd_cap_peel )
+                            {
+                                P.dd_out_peel_rank[ k ] = r;
+                                dd_peel_t & o = P.dd_out_peel[ k ];
+                                for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+                                o.b = p.b; o.ptau = ptau; o.pk = pk;
+                                o.w = sp.w[ t ]; o.I = sp.I[ t ]; o.Q = sp.Q[ t ]; o.U = sp.U[ t ];
+                                o.V = sp.V[ t ]; o.pix = sp.pix[ t ]; o.cpix = sd.cpix[ t ];
+                            }
+                            else
+                                atomicOr( P.m.status, ST_QUEUE_FULL );
+                            peel = false;
+                            if( solo )
+                            {
+                                solo = false;
+                                phase = PH_EMIT;
+                                continue;
+                            }
+                            unpark_walk( sp, p );
+                            unpark_dir( sd, p );
+                            faces_all( P.m, p.b, p.c, p.d, fx );
+                            phase = PH_SEGMENT;
+                            if( pend )
+                            {
+                                count( sp, pend == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
+                                phase = PH_EMIT;
+                            }
+                            continue;
+                        }
+                        const unsigned long long k = atomicAdd( P.dd_out_count, 1ull );
+                        if( k < ( unsigned long long ) P.dd_cap_walk )
+                        {
+                            load_cold( sc, p, P.seed );
+                            P.dd_out_walk_rank[ k ] = r;
+                            dd_walk_t & o = P.dd_out_walk[ k ];
+                            for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+                            o.d[ 0 ] = p.d.x; o.d[ 1 ] = p.d.y; o.d[ 2 ] = p.d.z;
+                            o.e1[ 0 ] = p.e1.x; o.e1[ 1 ] = p.e1.y; o.e1[ 2 ] = p.e1.z;
+                            o.S[ 0 ] = p.S.q; o.S[ 1 ] = p.S.u; o.S[ 2 ] = p.S.v;
+                            o.w = p.w; o.tau = p.tau; o.b = p.b;
+                            o.n_scat = p.n_scat; o.n_steps = p.n_steps;
+                            o.k1 = p.rng.k1; o.pid_lo = p.rng.pid_lo; o.pid_hi = p.rng.pid_hi;
+                            o.draw = p.rng.draw; o.batch = sc.batch[ t ];
+                        }
+                        else
+                            atomicOr( P.m.status, ST_QUEUE_FULL );
+                        phase = PH_EMIT;
+                        continue;
+                    }
+                }
+                faces_all( P.m, p.b, p.c, p.d, fx );
             }
             phase = PH_SEGMENT;
             after_crossing( false, left, lost );
@@ -169,8 +264,60 @@ k_forward( const __grid_constant__ fwd_params_t P )
             if( ( int ) lane == leader )
                 base = atomicAdd( P.work, ( unsigned long long ) n_emit );
             base = __shfl_sync( m_emit, base, leader );
-            const unsigned long long idx = base + rank;
-            if( idx >= ( unsigned long long ) P.n_packets )
+            unsigned long long idx = base + rank;
+            if constexpr( DD )
+            {
+                const unsigned long long nw = P.dd_n_walk, npl = P.dd_n_peel;
+                if( idx >= nw + npl + ( P.dd_emit ? ( unsigned long long ) P.n_packets : 0ull ) )
+                {
+                    phase = PH_DONE;
+                    continue;
+                }
+                const int t = threadIdx.x;
+                if( idx < nw )
+                {   // a walk arriving from another rank
+                    const dd_walk_t & o = P.dd_in_walk[ idx ];
+                    for( int a = 0; a < 3; ++ a ) { p.x[ a ] = o.x[ a ]; p.c[ a ] = o.c[ a ]; }
+                    p.d = phys::v3 { o.d[ 0 ], o.d[ 1 ], o.d[ 2 ] };
+                    p.e1 = phys::v3 { o.e1[ 0 ], o.e1[ 1 ], o.e1[ 2 ] };
+                    p.S = phys::stokes_t { o.S[ 0 ], o.S[ 1 ], o.S[ 2 ] };
+                    p.w = o.w; p.tau = o.tau; p.b = o.b;
+                    p.n_scat = o.n_scat; p.n_steps = o.n_steps;
+                    p.rng = phys::rng_t { P.seed, o.k1, o.pid_lo, o.pid_hi, o.draw };
+                    sc.batch[ t ] = o.batch;
+                    set_inv( p );
+                    store_cold( sc, p );
+                    faces_all( P.m, p.b, p.c, p.d, fx );
+                    peel = false; solo = false;
+                    phase = PH_SEGMENT;
+                    continue;
+                }
+                if( idx < nw + npl )
+                {   // a peel-off ray arriving from another rank
+                    const dd_peel_t & o = P.dd_in_peel[ idx - nw ];
+                    for( int a = 0; a < 3; ++ a )
+                    {
+                        p.x[ a ] = o.x[ a ]; p.c[ a ] = o.c[ a ]; p.inv[ a ] = P.inv_o[ a ];
+                    }
+                    p.b = o.b; p.d = P.o;
+                    ptau = o.ptau; pk = o.pk;
+                    sp.w[ t ] = o.w; sp.I[ t ] = o.I; sp.Q[ t ] = o.Q; sp.U[ t ] = o.U;
+                    sp.V[ t ] = o.V; sp.pix[ t ] = o.pix; sd.cpix[ t ] = o.cpix;
+                    faces_all( P.m, p.b, p.c, p.d, fx );
+                    peel = true; solo = true; pend = 0;
+                    phase = PH_SEGMENT;
+                    continue;
+                }
+                idx -= nw + npl;
+                // each packet is emitted once over the ranks: point sources by
+                // the owner of the source's block, plane sources by pid modulo
+                const long long pid = P.pid0 + ( long long ) idx;
+                const src_dev_t & s0 = P.src[ pid % P.n_src ];
+                if( s0.kind == KP_SOURCE_POINT ? P.dd_owner[ s0.ib ] != P.dd_rank
+                                               : ( int ) ( pid % P.dd_ranks ) != P.dd_rank )
+                    continue;
+            }
+            else if( idx >= ( unsigned long long ) P.n_packets )
             {
                 phase = PH_DONE;
                 continue;
@@ -200,6 +347,31 @@ k_forward( const __grid_constant__ fwd_params_t P )
             sc.batch[ threadIdx.x ] = ( int ) ( p.pid(  ) % P.n_batch );
             p.tau = sample_tau( p.rng );
             phase = PH_SEGMENT;
+            if constexpr( DD )
+            {
+                const int r = P.dd_owner[ p.b ];
+                if( r != P.dd_rank )
+                {   // emitted into a block of rank r (plane sources): hand it over
+                    const unsigned long long k = atomicAdd( P.dd_out_count, 1ull );
+                    if( k < ( unsigned long long ) P.dd_cap_walk )
+                    {
+                        P.dd_out_walk_rank[ k ] = r;
+                        dd_walk_t & o = P.dd_out_walk[ k ];
+                        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+                        o.d[ 0 ] = p.d.x; o.d[ 1 ] = p.d.y; o.d[ 2 ] = p.d.z;
+                        o.e1[ 0 ] = p.e1.x; o.e1[ 1 ] = p.e1.y; o.e1[ 2 ] = p.e1.z;
+                        o.S[ 0 ] = p.S.q; o.S[ 1 ] = p.S.u; o.S[ 2 ] = p.S.v;
+                        o.w = p.w; o.tau = p.tau; o.b = p.b;
+                        o.n_scat = p.n_scat; o.n_steps = p.n_steps;
+                        o.k1 = p.rng.k1; o.pid_lo = p.rng.pid_lo; o.pid_hi = p.rng.pid_hi;
+                        o.draw = p.rng.draw; o.batch = sc.batch[ threadIdx.x ];
+                    }
+                    else
+                        atomicOr( P.m.status, ST_QUEUE_FULL );
+                    phase = PH_EMIT;
+                    continue;
+                }
+            }
             const src_dev_t & s = P.n_scenes > 0 ? P.scenes[ si ].src : P.src[ p.pid(  ) % P.n_src ];
             if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
             {   // direct light of an isotropic, unpolarized point source
@@ -230,7 +402,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             ++ p.n_scat;
             count( sp, KP_CNT_SCATTER );
             {
-                const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
+                const float2 sg = sigma_at( p.b, p.c );
                 p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, __fadd_rn( sg.x, sg.y ) ) );
             }   // survival weighting by the albedo
             bool do_peel = false;
@@ -296,7 +468,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
         if( phase != PH_SEGMENT ) continue;
         // the active ray's direction is in p.d / p.inv (a peel-off ray holds
         // them while the walk's are parked)
-        const float2 sg = P.m.sigma[ cell_index( P.m, p.b, p.c ) ];
+        const float2 sg = sigma_at( p.b, p.c );
         const float ext = __fadd_rn( sg.x, sg.y );
         int ax;
         const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
@@ -518,6 +690,63 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
 }
 
 ////////////////////////////////////////////////////////////
+// One round of a domain-decomposed solve (k_forward<..., DD = true>).
+
+static_assert( sizeof( kp::dd_walk_t ) == KP_DD_WALK_BYTES, "walk record size" );
+static_assert( sizeof( kp::dd_peel_t ) == KP_DD_PEEL_BYTES, "peel-off record size" );
+
+extern "C" int kp_transport_forward_dd( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                        const kp_dd_round_t * r, const kp_tallies_t * tallies,
+                                        void * stream )
+{
+    return kp::guarded( "kp_transport_forward_dd", [ & ]
+    {
+        kp::require( mesh && cfg && r && tallies, "null argument" );
+        kp::require( cfg->n_record == 0, "records are not kept in decomposed solves" );
+        kp::require( r->n_ranks >= 1 && r->rank >= 0 && r->rank < r->n_ranks, "bad rank" );
+        kp::require( r->owner && r->block_local && r->sigma_local && r->out_count,
+                     "null decomposition array" );
+        kp::require( r->n_in_walk >= 0 && r->n_in_peel >= 0 && r->cap_walk >= 0
+                     && r->cap_peel >= 0, "negative queue size" );
+        kp::require( ( r->n_in_walk == 0 || r->in_walk ) && ( r->n_in_peel == 0 || r->in_peel )
+                     && ( r->cap_walk == 0 || ( r->out_walk && r->out_walk_rank ) )
+                     && ( r->cap_peel == 0 || ( r->out_peel && r->out_peel_rank ) ),
+                     "null queue" );
+        mesh->upload( false );                    // tables only: sigma is per rank
+        static thread_local kp::fwd_params_t P;
+        kp::make_fwd_params( mesh, * cfg, * tallies, P );
+        P.m.sigma = reinterpret_cast< const float2 * >( r->sigma_local );
+        P.work = mesh->workspace(  );
+        P.dd_rank = r->rank; P.dd_ranks = r->n_ranks;
+        P.dd_owner = r->owner; P.dd_loc = r->block_local;
+        P.dd_in_walk = static_cast< const kp::dd_walk_t * >( r->in_walk );
+        P.dd_in_peel = static_cast< const kp::dd_peel_t * >( r->in_peel );
+        P.dd_n_walk = r->n_in_walk; P.dd_n_peel = r->n_in_peel;
+        P.dd_emit = r->emit != 0;
+        P.dd_out_walk = static_cast< kp::dd_walk_t * >( r->out_walk );
+        P.dd_out_peel = static_cast< kp::dd_peel_t * >( r->out_peel );
+        P.dd_out_walk_rank = r->out_walk_rank;
+        P.dd_out_peel_rank = r->out_peel_rank;
+        P.dd_cap_walk = r->cap_walk; P.dd_cap_peel = r->cap_peel;
+        P.dd_out_count = r->out_count;
+        const long long items = r->n_in_walk + r->n_in_peel + ( r->emit ? cfg->n_packets : 0 );
+        if( items == 0 ) return;
+        cudaStream_t s = ( cudaStream_t ) stream;
+        const void * k = cfg->tally_mode == KP_TALLY_FIXED
+                       ? ( const void * ) kp::k_forward< KP_TALLY_FIXED, 256, true >
+                       : ( const void * ) kp::k_forward< KP_TALLY_FLOAT, 256, true >;
+        long long grid = kp::persistent_grid( k, 256 );
+        grid = std::min< long long >( grid, ( items + 255 ) / 256 );
+        KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
+        if( cfg->tally_mode == KP_TALLY_FIXED )
+            kp::k_forward< KP_TALLY_FIXED, 256, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+        else
+            kp::k_forward< KP_TALLY_FLOAT, 256, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+        KP_CUDA( cudaGetLastError(  ) );
+    } );
+}
+
+////////////////////////////////////////////////////////////
 // No-allocation entry point: the forward solve with its packet counter in a
 // static device array instead of the mesh's workspace.
 
@@ -564,7 +793,8 @@ extern "C" int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transpor
     return kp::guarded( "kp_transport_forward_noalloc", [ & ]
     {
         kp::require( mesh && cfg && tallies, "null argument" );
-        kp::require( mesh->uploaded, "mesh is not on the device: call kp_mesh_upload at set-up",
+        kp::require( mesh->uploaded && mesh->d_sigma != nullptr,
+                     "mesh is not on the device: call kp_mesh_upload at set-up",
                      KP_ERR_CONFIG );
         int dev = 0;
         KP_CUDA( cudaGetDevice( & dev ) );

@@ -82,7 +82,48 @@ struct fwd_params_t
     const long long   * scene_prefix;   // [n_scenes + 1] packet index prefix
     const scene_dev_t * scenes;         // [n_scenes]
     long long   mu_scene_stride;        // mu tally elements per scene
+    // domain-decomposed rounds only (kp_transport_forward_dd)
+    int         dd_rank, dd_ranks;
+    const int * dd_owner;               // [n_blocks] rank owning the block
+    const int * dd_loc;                 // [n_blocks] local block index, -1 if foreign
+    const struct dd_walk_t * dd_in_walk;
+    const struct dd_peel_t * dd_in_peel;
+    long long   dd_n_walk, dd_n_peel;   // incoming records
+    int         dd_emit;                // emit this rank's packets in this round
+    struct dd_walk_t * dd_out_walk;     // [dd_cap_walk] records leaving this rank
+    struct dd_peel_t * dd_out_peel;     // [dd_cap_peel]
+    int       * dd_out_walk_rank;       // destination rank of each record
+    int       * dd_out_peel_rank;
+    long long   dd_cap_walk, dd_cap_peel;
+    unsigned long long * dd_out_count;  // [2]: walks, peel-off rays
     src_dev_t   src[ MAX_SOURCES ];
+};
+
+// A packet's walk crossing into a block of another rank (it has entered the
+// block: position snapped to the face, cell and block set).  The inverse
+// direction and the face cache are rebuilt from it, bit for bit.
+struct __align__( 16 ) dd_walk_t
+{
+    double   x[ 3 ];
+    float    d[ 3 ], e1[ 3 ], S[ 3 ];
+    float    w, tau;
+    int      b, c[ 3 ];
+    int      n_scat, n_steps;
+    uint32_t k1, pid_lo, pid_hi, draw;
+    int      batch, pad[ 3 ];
+};
+
+// A peel-off ray crossing into a block of another rank, with its pending
+// contribution (the deposit happens where the ray ends).
+struct __align__( 16 ) dd_peel_t
+{
+    double x[ 3 ];
+    int    b, c[ 3 ];
+    float  ptau;
+    int    pk;
+    float  w, I, Q, U, V;
+    int    pix, cpix;
+    int    pad[ 3 ];
 };
 
 enum pk_status { PK_ESCAPED = 1, PK_ABSORBED = 2, PK_SCATTER_CAP = 3, PK_STEP_CAP = 4,
