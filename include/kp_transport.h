@@ -146,6 +146,29 @@ int kp_mesh_sigma_ptr( kp_mesh_t * mesh, float ** sigma );
 int kp_mesh_status( kp_mesh_t * mesh, void * stream, unsigned * flags );
 
 /* ------------------------------------------------------------------ */
+/* Spherical-polar meshes (axes r, theta, phi): meshgen::sph_t on       */
+/* cyl_t's radial spacing (mesh/meshgen/spherical.h, cylindrical.h),    */
+/* same tree and neighbour tables.  r_ratio as [mesh] r_ratio: 1 for    */
+/* uniform radial cells, a ratio of successive radial widths, or < 0   */
+/* for the ratio (r_max / r_min)^(1/n_r).                               */
+int kp_mesh_create_sph( const kp_mesh_desc_t * desc, double r_ratio, kp_mesh_t ** mesh );
+/* Same from an INI file ([mesh] r_ratio read as cyl_t::read does). */
+int kp_mesh_create_sph_ini( const char * path, kp_mesh_t ** mesh );
+/* Radial faces [n_blocks][nc0 + 1] (the block's dx0[0] is -1 when they are
+ * not uniform) and cell volumes [n_cells], as geo_t holds them for float_t of
+ * `precision` bytes, widened to double (sph_t::set_coord_axes, sph_t::volume). */
+int kp_mesh_geometry_sph( const kp_mesh_t * mesh, int precision, double * r_faces,
+                          double * vol );
+/* photon::sph_t::proc (modules/particle/radiation/photon_sph.h) over a
+ * packet pool on a spherical mesh, like kp_trace: x[3n] (r, theta, phi) and
+ * x_car[3n] (its Cartesian copy), both updated, dir[3n], and the other
+ * arrays as kp_trace's.  The walk evaluates cosf, sinf, sqrtf, acosf and
+ * atan2f per step as the reference does, with CUDA's functions. */
+int kp_trace_sph( kp_mesh_t * mesh, int precision, long long n, void * x, void * x_car,
+                  const void * dir, int * cell, int * ib, const void * proper, int * step,
+                  int8_t * todo, int flux_mode, int fx_shift, void * flux, void * stream );
+
+/* ------------------------------------------------------------------ */
 /* Runtime refinement.  The reference declares the hook and leaves it   */
 /* empty: mesh_t::changed (mesh/mesh.cpp:86-89), meshgen::base_t::update */
 /* (mesh/meshgen/meshgen.cpp:443-446); block_map_t::update              */

@@ -96,6 +96,11 @@ _SIGS = {
     "kp_mesh_sigma_ptr": [c_void_p, P(c_void_p)],
     "kp_mesh_status": [c_void_p, c_void_p, P(ctypes.c_uint)],
     "kp_mesh_flag_tau": [c_void_p, c_float, c_float, c_void_p, c_void_p],
+    "kp_mesh_create_sph": [c_void_p, c_double, P(c_void_p)],
+    "kp_mesh_create_sph_ini": [ctypes.c_char_p, P(c_void_p)],
+    "kp_mesh_geometry_sph": [c_void_p, c_int, c_void_p, c_void_p],
+    "kp_trace_sph": [c_void_p, c_int, c_ll] + [c_void_p] * 8 + [c_int, c_int, c_void_p,
+                                                                 c_void_p],
     "kp_mesh_adapt": [c_void_p, c_void_p, P(c_void_p)],
     "kp_mesh_remap": [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p],
     "kp_trace": [c_void_p, c_int, c_ll, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -70,6 +70,24 @@ void block_tree_t::init_domain(  )
             throw std::runtime_error( "x_max must exceed x_min" );
         lim_[ a ] = ng / nb;
     }
+    // cyl_t::read (mesh/meshgen/cylindrical.h): geometric radial spacing
+    ratio_ = 1.0; dr0_ = -1.0;
+    if( desc.coord == 1 )
+    {
+        if( ! ( desc.x_min[ 0 ] > 0.0 ) )
+            throw std::runtime_error( "spherical meshes need r_min > 0" );
+        ratio_ = desc.r_ratio;
+        const int n_r = desc.n_cell_global[ 0 ];
+        if( ! ( std::fabs( ratio_ - 1 ) < 1e-6 ) )
+        {
+            if( ratio_ < 0 )
+                ratio_ = std::pow( desc.x_max[ 0 ] / desc.x_min[ 0 ], 1. / n_r );
+            dr0_  = desc.x_max[ 0 ] - desc.x_min[ 0 ];
+            dr0_ /= ( std::pow( ratio_, n_r ) - 1 ) / ( ratio_ - 1 );
+        }
+    }
+    else if( desc.coord != 0 )
+        throw std::runtime_error( "unknown coordinate system" );
 }
 
 block_tree_t::block_tree_t( const mesh_desc_t & desc ) : desc_( desc )
@@ -133,6 +151,11 @@ int block_tree_t::blocks_at( int level, int a ) const
 
 double block_tree_t::location( double x_logic, int a ) const
 {
+    if( a == 0 && ! radial_uniform(  ) )
+    {   // cyl_t::location: geometric radial faces
+        const double n_logic( x_logic * desc_.n_cell_global[ 0 ] );
+        return desc_.x_min[ 0 ] + dr0_ / ( ratio_ - 1 ) * ( std::pow( ratio_, n_logic ) - 1 );
+    }
     return desc_.x_min[ a ] + x_logic * ( desc_.x_max[ a ] - desc_.x_min[ a ] );
 }
 
@@ -326,6 +349,7 @@ void block_tree_t::build_tables(  )
             }
         }
     }
+    build_sph_tables(  );
     const int L = t.max_level;
     double n_lookup = 1.0;
     for( int a = 0; a < 3; ++ a )
@@ -362,16 +386,97 @@ void block_tree_t::build_tables(  )
     }
 }
 
+// Spherical tables: sph_t::set_coord_axes (radial faces loc_f(i) in double,
+// stored as float_t when the spacing is not uniform) and sph_t::volume
+// (mesh/meshgen/spherical.h), whose face coordinates come from geo_t::x_fc
+// in float_t (geometry.h) and whose arithmetic is double.
+namespace
+{
+template< class F >
+struct sph_geo_t
+{
+    const F * xf0; const F * dx0; const F * rf;
+    bool r_table;
+    F x_fc( int a, int i ) const
+    {
+        if( a == 0 && r_table ) return rf[ i + 1 ];      // one ghost face below
+        return xf0[ a ] + ( F ) i * dx0[ a ];
+    }
+};
+
+template< class F >
+double sph_volume( const sph_geo_t< F > & g, int c0, int c1, int c2 )
+{
+    const F r_l  = g.x_fc( 0, c0 ), r_r = g.x_fc( 0, c0 + 1 );
+    const F th_l = g.x_fc( 1, c1 ), th_r = g.x_fc( 1, c1 + 1 );
+    const F d_phi = g.x_fc( 2, c2 + 1 ) - g.x_fc( 2, c2 );
+    return ( std::pow( ( double ) r_r, 3. ) - std::pow( ( double ) r_l, 3. ) ) / 3.
+         * std::fabs( std::cos( ( double ) th_l ) - std::cos( ( double ) th_r ) ) * d_phi;
+}
+}   // namespace
+
+void block_tree_t::build_sph_tables(  )
+{
+    auto & t = tab_;
+    t.coord = desc_.coord;
+    t.rf_d.clear(  ); t.rf_f.clear(  ); t.vol_d.clear(  ); t.vol_f.clear(  );
+    if( desc_.coord != 1 )
+        return;
+    const int nb = t.n_blocks, n0 = t.nc[ 0 ], cpb = t.cells_per_block;
+    const bool table = ! radial_uniform(  );
+    const int nf = n0 + 3;                       // faces -1 .. n0 + 1 (one ghost each side)
+    t.rf_d.assign( ( size_t ) nb * nf, 0. );
+    t.rf_f.assign( ( size_t ) nb * nf, 0.f );
+    t.vol_d.assign( ( size_t ) nb * cpb, 0. );
+    t.vol_f.assign( ( size_t ) nb * cpb, 0.f );
+    for( int b = 0; b < nb; ++ b )
+    {
+        const double nl = blocks_at( t.level[ b ], 0 );
+        for( int i = -1; i <= n0 + 1; ++ i )
+        {
+            const double l = location( ( t.reg[ 3 * b ] + ( double ) i / n0 ) / nl, 0 );
+            t.rf_d[ ( size_t ) b * nf + i + 1 ] = l;
+            t.rf_f[ ( size_t ) b * nf + i + 1 ] = ( float ) l;
+        }
+        if( table )
+        {
+            t.dx0_d[ 3 * b ] = -1.0;
+            t.dx0_f[ 3 * b ] = -1.0f;
+        }
+        t.vol0_d[ b ] = -1.0;
+        t.vol0_f[ b ] = -1.0f;
+        const sph_geo_t< double > gd { & t.xf0_d[ 3 * b ], & t.dx0_d[ 3 * b ],
+                                       & t.rf_d[ ( size_t ) b * nf ], table };
+        const sph_geo_t< float >  gf { & t.xf0_f[ 3 * b ], & t.dx0_f[ 3 * b ],
+                                       & t.rf_f[ ( size_t ) b * nf ], table };
+        size_t k = ( size_t ) b * cpb;
+        for( int c2 = 0; c2 < t.nc[ 2 ]; ++ c2 )
+            for( int c1 = 0; c1 < t.nc[ 1 ]; ++ c1 )
+                for( int c0 = 0; c0 < n0; ++ c0, ++ k )
+                {
+                    t.vol_d[ k ] = sph_volume( gd, c0, c1, c2 );
+                    t.vol_f[ k ] = ( float ) sph_volume( gf, c0, c1, c2 );
+                }
+    }
+}
+
 bool block_tree_t::locate( const double x[ 3 ], int & ib, int cell[ 3 ] ) const
 {
+    // logical coordinate in [0, 1] (the inverse of location)
+    auto logic = [ & ]( int a ) -> double
+    {
+        if( a == 0 && ! radial_uniform(  ) )
+            return std::log1p( ( x[ 0 ] - desc_.x_min[ 0 ] ) * ( ratio_ - 1 ) / dr0_ )
+                 / std::log( ratio_ ) / desc_.n_cell_global[ 0 ];
+        return ( x[ a ] - desc_.x_min[ a ] ) / ( desc_.x_max[ a ] - desc_.x_min[ a ] );
+    };
     region_key_t k { 0, { 0, 0, 0 } };
     for( int a = 0; a < 3; ++ a )
     {
         if( ! ( x[ a ] >= desc_.x_min[ a ] && x[ a ] <= desc_.x_max[ a ] ) )
             return false;
-        const double u = ( x[ a ] - desc_.x_min[ a ] )
-                       / ( desc_.x_max[ a ] - desc_.x_min[ a ] );
-        k.i[ a ] = std::min( lim_[ a ] - 1, ( int ) std::floor( u * lim_[ a ] ) );
+        k.i[ a ] = std::max( 0, std::min( lim_[ a ] - 1,
+                                          ( int ) std::floor( logic( a ) * lim_[ a ] ) ) );
     }
     for( ;; )
     {
@@ -387,9 +492,7 @@ bool block_tree_t::locate( const double x[ 3 ], int & ib, int cell[ 3 ] ) const
         for( int a = 0; a < 3; ++ a )
         {
             const double n  = blocks_at( c.level, a );
-            const double u  = ( x[ a ] - desc_.x_min[ a ] )
-                            / ( desc_.x_max[ a ] - desc_.x_min[ a ] );
-            int i = ( int ) std::floor( u * n );
+            int i = ( int ) std::floor( logic( a ) * n );
             i = std::max( 2 * k.i[ a ], std::min( 2 * k.i[ a ] + 1, i ) );
             c.i[ a ] = i;
         }
@@ -398,8 +501,15 @@ bool block_tree_t::locate( const double x[ 3 ], int & ib, int cell[ 3 ] ) const
     const auto & t = tab_;
     for( int a = 0; a < 3; ++ a )
     {
-        const double f = ( x[ a ] - t.xf0_d[ 3 * ib + a ] ) / t.dx0_d[ 3 * ib + a ];
-        int i = ( int ) std::floor( f );
+        int i;
+        if( a == 0 && t.coord == 1 && t.dx0_d[ 3 * ib ] < 0 )
+        {   // radial face table: last face not above x
+            const double * f = & t.rf_d[ ( size_t ) ib * ( t.nc[ 0 ] + 3 ) + 1 ];
+            i = 0;
+            while( i + 1 < t.nc[ 0 ] && f[ i + 1 ] <= x[ 0 ] ) ++ i;
+        }
+        else
+            i = ( int ) std::floor( ( x[ a ] - t.xf0_d[ 3 * ib + a ] ) / t.dx0_d[ 3 * ib + a ] );
         cell[ a ] = std::max( 0, std::min( t.nc[ a ] - 1, i ) );
     }
     return true;

@@ -32,6 +32,11 @@ struct mesh_desc_t
     int    n_cell_block [ 3 ];
     bool   periodic     [ 3 ];
     std::vector< refine_box_t > refine;
+    // Coordinates: 0 Cartesian (meshgen::base_t); 1 spherical-polar
+    // (r, theta, phi) of meshgen::sph_t, whose radius follows cyl_t's
+    // geometric spacing ([mesh] r_ratio: 1 uniform, < 0 from the radii).
+    int    coord   = 0;
+    double r_ratio = 1.0;
 };
 
 // Region key: (level, logical block index) with the reference's lexical
@@ -73,6 +78,13 @@ struct block_tables_t
     std::vector< double >   xf0_d, dx0_d, vol0_d;   // [nb][3], [nb][3], [nb]
     std::vector< float  >   xf0_f, dx0_f, vol0_f;
     std::vector< uint8_t >  phybnd;        // [nb] bit (2a+s)
+    // Spherical meshes: radial faces [nb][nc0+3] (faces -1..nc0+1: one ghost
+    // each side, as geo_t keeps them; when the radial spacing
+    // is not uniform, dx0[0] is then -1) and cell volumes [n_cells], as
+    // sph_t::set_coord_axes and sph_t::volume give them (FP64 and FP32).
+    int coord = 0;
+    std::vector< double >   rf_d;  std::vector< float > rf_f;
+    std::vector< double >   vol_d; std::vector< float > vol_f;
     std::vector< int >      nb_id;         // [nb][24]
     std::vector< int8_t >   d_lvl;         // [nb][6]
     std::vector< uint8_t >  nb_shift;      // [nb][24] bit0: shift[0], bit1: shift[1]
@@ -119,9 +131,12 @@ private:
     double location( double x_logic, int a ) const;
     int    block_index( double loc, int level, int a ) const;
     void   build_tables(  );
+    void   build_sph_tables(  );
+    bool   radial_uniform(  ) const { return dr0_ <= 0.0; }
 
     mesh_desc_t                        desc_;
     int                                n_dim_ = 3;
+    double                             ratio_ = 1.0, dr0_ = -1.0;   // cyl_t::read
     int                                lim_[ 3 ];    // root blocks per axis
     std::map< region_key_t, node_t >   nodes_;
     block_tables_t                     tab_;

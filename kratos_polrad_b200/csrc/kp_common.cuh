@@ -112,6 +112,10 @@ struct mesh_view_t
     float  xlim_f[ 2 ][ 3 ];
     float  lbox_f[ 3 ];
     unsigned * status;
+    // spherical meshes only (null otherwise): radial faces [n_blocks][nc0+3]
+    // (faces -1..nc0+1) and cell volumes [n_blocks * cpb], per float_t
+    const float  * rf_f;  const double * rf_d;
+    const float  * vol_f; const double * vol_d;
 };
 
 }   // namespace kp
@@ -129,6 +133,8 @@ struct kp_mesh
     float2     * d_sigma  = nullptr;
     int        * d_lookup = nullptr;
     unsigned   * d_status = nullptr;
+    float      * d_rf_f  = nullptr;  double * d_rf_d  = nullptr;   // spherical tables
+    float      * d_vol_f = nullptr;  double * d_vol_d = nullptr;
 
     unsigned long long * d_work = nullptr;   // scratch: packet counters
 

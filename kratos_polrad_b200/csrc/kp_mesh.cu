@@ -36,6 +36,7 @@ kp::mesh_view_t kp_mesh::view(  ) const
         v.lbox_f[ a ] = t.l_box_f[ a ];
     }
     v.status = d_status;
+    v.rf_f = d_rf_f; v.rf_d = d_rf_d; v.vol_f = d_vol_f; v.vol_d = d_vol_d;
     return v;
 }
 
@@ -96,6 +97,21 @@ void kp_mesh::upload( bool with_sigma )
             KP_CUDA( cudaMalloc( & d_sigma,  n_cells * sizeof( float2 ) ) );
         KP_CUDA( cudaMalloc( & d_status, 4 * sizeof( unsigned ) ) );
         KP_CUDA( cudaMalloc( & d_work, 32 * sizeof( unsigned long long ) ) );
+        if( t.coord == 1 )
+        {
+            KP_CUDA( cudaMalloc( & d_rf_f, t.rf_f.size(  ) * sizeof( float ) ) );
+            KP_CUDA( cudaMalloc( & d_rf_d, t.rf_d.size(  ) * sizeof( double ) ) );
+            KP_CUDA( cudaMalloc( & d_vol_f, t.vol_f.size(  ) * sizeof( float ) ) );
+            KP_CUDA( cudaMalloc( & d_vol_d, t.vol_d.size(  ) * sizeof( double ) ) );
+            KP_CUDA( cudaMemcpy( d_rf_f, t.rf_f.data(  ), t.rf_f.size(  ) * sizeof( float ),
+                                 cudaMemcpyHostToDevice ) );
+            KP_CUDA( cudaMemcpy( d_rf_d, t.rf_d.data(  ), t.rf_d.size(  ) * sizeof( double ),
+                                 cudaMemcpyHostToDevice ) );
+            KP_CUDA( cudaMemcpy( d_vol_f, t.vol_f.data(  ), t.vol_f.size(  ) * sizeof( float ),
+                                 cudaMemcpyHostToDevice ) );
+            KP_CUDA( cudaMemcpy( d_vol_d, t.vol_d.data(  ), t.vol_d.size(  ) * sizeof( double ),
+                                 cudaMemcpyHostToDevice ) );
+        }
         KP_CUDA( cudaMemset( d_work, 0, 32 * sizeof( unsigned long long ) ) );
         KP_CUDA( cudaMemcpy( d_nb, t.nb_id.data(  ), nb * 24 * sizeof( int ),
                              cudaMemcpyHostToDevice ) );
@@ -128,41 +144,99 @@ void kp_mesh::release(  )
     cudaFree( d_lookup ); d_lookup = nullptr;
     cudaFree( d_status ); d_status = nullptr;
     cudaFree( d_work );   d_work   = nullptr;
+    cudaFree( d_rf_f );   d_rf_f   = nullptr;
+    cudaFree( d_rf_d );   d_rf_d   = nullptr;
+    cudaFree( d_vol_f );  d_vol_f  = nullptr;
+    cudaFree( d_vol_d );  d_vol_d  = nullptr;
     uploaded = false;
 }
 
 extern "C" {
+
+static kp::mesh_desc_t desc_from_c( const kp_mesh_desc_t * desc )
+{
+    require( desc->n_refine >= 0 && ( desc->n_refine == 0 || desc->refine ), "bad refine list" );
+    kp::mesh_desc_t d {  };
+    for( int a = 0; a < 3; ++ a )
+    {
+        d.x_min[ a ] = desc->x_min[ a ];
+        d.x_max[ a ] = desc->x_max[ a ];
+        d.n_cell_global[ a ] = desc->n_cell_global[ a ];
+        d.n_cell_block [ a ] = desc->n_cell_block [ a ];
+        d.periodic[ a ] = desc->periodic[ a ] != 0;
+    }
+    for( int r = 0; r < desc->n_refine; ++ r )
+    {
+        kp::refine_box_t b {  };
+        b.level = desc->refine[ r ].level;
+        for( int a = 0; a < 3; ++ a )
+        {
+            b.x_min[ a ] = desc->refine[ r ].x_min[ a ];
+            b.x_max[ a ] = desc->refine[ r ].x_max[ a ];
+        }
+        d.refine.push_back( b );
+    }
+    return d;
+}
 
 int kp_mesh_create( const kp_mesh_desc_t * desc, kp_mesh_t ** mesh )
 {
     return guarded( "kp_mesh_create", [ & ]
     {
         require( desc != nullptr && mesh != nullptr, "null argument" );
-        require( desc->n_refine >= 0 && ( desc->n_refine == 0 || desc->refine ),
-                 "bad refine list" );
-        kp::mesh_desc_t d {  };
-        for( int a = 0; a < 3; ++ a )
-        {
-            d.x_min[ a ] = desc->x_min[ a ];
-            d.x_max[ a ] = desc->x_max[ a ];
-            d.n_cell_global[ a ] = desc->n_cell_global[ a ];
-            d.n_cell_block [ a ] = desc->n_cell_block [ a ];
-            d.periodic[ a ] = desc->periodic[ a ] != 0;
-        }
-        for( int r = 0; r < desc->n_refine; ++ r )
-        {
-            kp::refine_box_t b {  };
-            b.level = desc->refine[ r ].level;
-            for( int a = 0; a < 3; ++ a )
-            {
-                b.x_min[ a ] = desc->refine[ r ].x_min[ a ];
-                b.x_max[ a ] = desc->refine[ r ].x_max[ a ];
-            }
-            d.refine.push_back( b );
-        }
+        auto m = std::make_unique< kp_mesh >(  );
+        m->tree = std::make_unique< kp::block_tree_t >( desc_from_c( desc ) );
+        * mesh = m.release(  );
+    } );
+}
+
+int kp_mesh_create_sph( const kp_mesh_desc_t * desc, double r_ratio, kp_mesh_t ** mesh )
+{
+    return guarded( "kp_mesh_create_sph", [ & ]
+    {
+        require( desc != nullptr && mesh != nullptr, "null argument" );
+        kp::mesh_desc_t d = desc_from_c( desc );
+        d.coord = 1;
+        d.r_ratio = r_ratio;
         auto m = std::make_unique< kp_mesh >(  );
         m->tree = std::make_unique< kp::block_tree_t >( d );
         * mesh = m.release(  );
+    } );
+}
+
+int kp_mesh_create_sph_ini( const char * path, kp_mesh_t ** mesh )
+{
+    return guarded( "kp_mesh_create_sph_ini", [ & ]
+    {
+        require( path != nullptr && mesh != nullptr, "null argument" );
+        kp::ini_t ini;
+        require( ini.read_file( path ), "cannot read INI file", KP_ERR_CONFIG );
+        kp::mesh_desc_t d = kp::mesh_desc_from_ini( ini );
+        d.coord = 1;
+        d.r_ratio = ini.get_or< double >( "mesh", "r_ratio", 1.0 );   // cyl_t::read
+        auto m = std::make_unique< kp_mesh >(  );
+        m->tree = std::make_unique< kp::block_tree_t >( d );
+        * mesh = m.release(  );
+    } );
+}
+
+int kp_mesh_geometry_sph( const kp_mesh_t * mesh, int precision, double * r_faces, double * vol )
+{
+    return guarded( "kp_mesh_geometry_sph", [ & ]
+    {
+        require( mesh && r_faces && vol, "null argument" );
+        require( precision == 4 || precision == 8, "precision must be 4 or 8" );
+        const auto & t = mesh->tree->tables(  );
+        require( t.coord == 1, "not a spherical mesh", KP_ERR_CONFIG );
+        const int n0 = t.nc[ 0 ];
+        for( int b = 0; b < t.n_blocks; ++ b )
+            for( int i = 0; i <= n0; ++ i )
+            {
+                const size_t k = ( size_t ) b * ( n0 + 3 ) + i + 1;
+                r_faces[ ( size_t ) b * ( n0 + 1 ) + i ] = precision == 4 ? t.rf_f[ k ] : t.rf_d[ k ];
+            }
+        for( size_t k = 0; k < t.vol_d.size(  ); ++ k )
+            vol[ k ] = precision == 4 ? t.vol_f[ k ] : t.vol_d[ k ];
     } );
 }
 

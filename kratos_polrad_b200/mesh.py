@@ -55,10 +55,17 @@ class Mesh:
     """Owns a ``kp_mesh_t``; building needs no GPU."""
 
     def __init__(self, cfg: MeshConfig | None = None, ini_path: str | None = None,
-                 _handle: ctypes.c_void_p | None = None):
+                 _handle: ctypes.c_void_p | None = None, spherical: bool = False,
+                 r_ratio: float = 1.0):
+        """Cartesian mesh from a MeshConfig or INI file; ``spherical``: axes
+        (r, theta, phi) of meshgen::sph_t with cyl_t's radial spacing
+        (``r_ratio`` for a MeshConfig; an INI file gives [mesh] r_ratio)."""
         h = ctypes.c_void_p()
+        self.spherical = bool(spherical)
         if _handle is not None:
             h = _handle
+        elif ini_path is not None and spherical:
+            call("kp_mesh_create_sph_ini", ini_path.encode(), ctypes.byref(h))
         elif ini_path is not None:
             call("kp_mesh_create_ini", ini_path.encode(), ctypes.byref(h))
         else:
@@ -75,7 +82,10 @@ class Mesh:
                     boxes[k].x_min[a], boxes[k].x_max[a] = r.x_min[a], r.x_max[a]
             d.n_refine = len(cfg.refine)
             d.refine = ctypes.cast(boxes, ctypes.POINTER(_lib.RefineBox))
-            call("kp_mesh_create", ctypes.byref(d), ctypes.byref(h))
+            if spherical:
+                call("kp_mesh_create_sph", ctypes.byref(d), float(r_ratio), ctypes.byref(h))
+            else:
+                call("kp_mesh_create", ctypes.byref(d), ctypes.byref(h))
         self.handle = h
         info = _lib.MeshInfo()
         call("kp_mesh_info", h, ctypes.byref(info))
@@ -140,6 +150,14 @@ class Mesh:
         n = int(np.prod(sigma2.shape))
         call("kp_mesh_set_sigma", self.handle, ptr(sigma2), n, on_dev, None)
 
+    def geometry_sph(self, precision: int = 8):
+        """Spherical meshes: radial faces [n_blocks, nc0 + 1] and cell volumes
+        [n_cells] as float_t of ``precision`` bytes holds them."""
+        rf = np.zeros((self.n_blocks, self.nc[0] + 1))
+        vol = np.zeros(self.n_cells)
+        call("kp_mesh_geometry_sph", self.handle, precision, ptr(rf), ptr(vol))
+        return rf, vol
+
     # ---- runtime refinement ----
     def flag_tau(self, tau_refine: float, tau_coarsen: float = 0.0, stream=None):
         """Per-block flags on the device (int32 tensor): +1 where a cell's
@@ -159,7 +177,7 @@ class Mesh:
             raise ValueError(f"need {self.n_blocks} flags, got {f.size}")
         h = ctypes.c_void_p()
         call("kp_mesh_adapt", self.handle, ptr(f), ctypes.byref(h))
-        return Mesh(_handle=h)
+        return Mesh(_handle=h, spherical=self.spherical)
 
     def remap_to(self, other: "Mesh", field, stream=None):
         """Per-cell field [n_cells, n_comp] (CUDA tensor, float32) of this mesh

@@ -57,3 +57,24 @@ def trace(mesh, pool: PacketPool, flux_mode: str = "fixed", fx_shift: int = 32,
          ptr(pool.cell), ptr(pool.ib), ptr(pool.proper), ptr(pool.step),
          ptr(pool.todo), mode, fx_shift, ptr(flux), s)
     return flux
+
+
+def trace_sph(mesh, pool: PacketPool, x_car: torch.Tensor, flux_mode: str = "fixed",
+              fx_shift: int = 32, flux: torch.Tensor | None = None,
+              stream: int | None = None) -> torch.Tensor:
+    """``photon::sph_t::proc`` (modules/particle/radiation/photon_sph.h) over a
+    spherical mesh: ``pool.x`` holds (r, theta, phi) and ``x_car`` [n, 3] its
+    Cartesian copy (both updated in place); otherwise as ``trace``."""
+    prec = pool.x.element_size()
+    xc = x_car.to(pool.x.dtype)
+    if not xc.is_contiguous() or xc.data_ptr() != x_car.data_ptr():
+        raise ValueError("x_car must be a contiguous tensor of the pool's float type")
+    if flux is None:
+        dt = torch.int64 if flux_mode == "fixed" else pool.x.dtype
+        flux = torch.zeros(mesh.n_cells, dtype=dt, device=pool.x.device)
+    mode = KP_FLUX_FIXED if flux_mode == "fixed" else KP_FLUX_FLOAT
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    call("kp_trace_sph", mesh.handle, prec, len(pool), ptr(pool.x), ptr(x_car), ptr(pool.dir),
+         ptr(pool.cell), ptr(pool.ib), ptr(pool.proper), ptr(pool.step),
+         ptr(pool.todo), mode, fx_shift, ptr(flux), s)
+    return flux

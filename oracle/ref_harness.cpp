@@ -29,6 +29,12 @@
 #include "modules/particle/types/proxy.h"
 #include "mesh/block/dual_data.h"
 #include "mesh/meshgen/meshgen.h"
+#include "mesh/meshgen/spherical.h"
+// photon_sph.h names coord_t unqualified; nothing in the reference declares
+// it in that namespace (the header is never instantiated there), so the
+// harness supplies the name it means.
+namespace particle::radiation::photon { using type::coord_t; }
+#include "modules/particle/radiation/photon_sph.h"
 #include "mesh/tree/tree.h"
 #include "mesh/mesh.h"
 #include "io/args/input.h"
@@ -69,18 +75,22 @@ namespace
 ////////////////////////////////////////////////////////////
 // Types
 
-struct mgn_t : mesh::meshgen::base_t
+// A mesh generator (the Cartesian base_t, or the spherical sph_t with its
+// cylindrical radial spacing) with the members the harness drives made
+// accessible.
+template< class G >
+struct mgn_x : G
 {
-    using base_t::read;
-    using base_t::load_refinement;
-    using base_t::set_uniformity;
-    using base_t::set_coord_axes;
-    using base_t::set_geo_fulldim;
-    const type::idx_t & nc_block(  ) const { return n_ceff_block; }
-    const type::idx_t & lim     (  ) const { return i_logic_lim;  }
-    int                 ndim    (  ) const { return n_dim;        }
+    using G::read;
+    using mesh::meshgen::base_t::load_refinement;
+    using G::set_uniformity;
+    using G::set_coord_axes;
+    using mesh::meshgen::base_t::set_geo_fulldim;
+    const type::idx_t & nc_block(  ) const { return this->n_ceff_block; }
+    const type::idx_t & lim     (  ) const { return this->i_logic_lim;  }
+    int                 ndim    (  ) const { return this->n_dim;        }
     const std::vector< mesh::meshgen::refine_region_t > & regions(  ) const
-    { return ref_regions; }
+    { return this->ref_regions; }
 };
 
 // Proxy carrying the radiation fields, as radiation::proxy_t does
@@ -102,7 +112,9 @@ struct bmap_t
 
 struct harness_t
 {
-    mgn_t                           mgn;
+    std::unique_ptr< mesh::meshgen::base_t > mgn;
+    type::idx_t                     nc;          // cells per block
+    bool                            spherical = false;
     mesh::tree_t                    tree;
     std::deque< mesh::block_t >     blocks;     // id order
     std::vector< prx_t >            prx;
@@ -174,6 +186,7 @@ void kp_ref_deposit( double * p, double v )
 ////////////////////////////////////////////////////////////
 // Mesh construction
 
+template< class G >
 static void build_mesh( const std::string & ini )
 {
     g_h = std::make_unique< harness_t >(  );
@@ -181,11 +194,13 @@ static void build_mesh( const std::string & ini )
     input args( ini, false );
     if( ! args.read(  ) )
         throw std::runtime_error( "cannot read " + ini );
+    auto mg = std::make_unique< mgn_x< G > >(  );
+    auto & mgn = * mg;
 
     // meshgen::base_t::init (meshgen.cpp:44-55)
-    h.mgn.read( args );
-    h.tree.n_dim    = h.mgn.ndim(  );
-    h.tree.reg_max  = h.mgn.lim (  );
+    mgn.read( args );
+    h.tree.n_dim    = mgn.ndim(  );
+    h.tree.reg_max  = mgn.lim (  );
     h.tree.periodic = { false, false, false };
     std::vector< std::string > kinds;
     args( "boundary", "kinds", kinds );
@@ -194,8 +209,8 @@ static void build_mesh( const std::string & ini )
             kinds[ side ].find( "per" ) != std::string::npos;
 
     // generate_tree (meshgen.cpp:144-163) on the harness's own tree
-    h.mgn.load_refinement( args );
-    for( const auto & ref : h.mgn.regions(  ) )
+    mgn.load_refinement( args );
+    for( const auto & ref : mgn.regions(  ) )
         if( ref.level > 0 )
             for( const auto & i : utils::loop( ref.i[ 0 ], ref.i[ 1 ], true ) )
             {
@@ -242,14 +257,15 @@ static void build_mesh( const std::string & ini )
     { return std::malloc( s ); };
     for( auto & b : h.blocks )
     {
-        h.mgn.set_uniformity( b );
-        b.geo.setup( h.mgn.nc_block(  ), 1, f_host );
-        h.mgn.set_coord_axes( b );
-        h.mgn.set_geo_fulldim( b );
+        mgn.set_uniformity( b );
+        b.geo.setup( mgn.nc_block(  ), 1, f_host );
+        mgn.set_coord_axes( b );
+        mgn.set_geo_fulldim( b );
     }
 
     // Fields: one contiguous flux pool so that deposits map to cells.
-    const auto & nc = h.mgn.nc_block(  );
+    const auto & nc = mgn.nc_block(  );
+    h.nc = nc;
     h.n_cell_blk = nc[ 0 ] * nc[ 1 ] * nc[ 2 ];
     const size_t nb = h.blocks.size(  );
     h.flux   .assign( nb * h.n_cell_blk, 0 );
@@ -278,7 +294,7 @@ static void build_mesh( const std::string & ini )
     }
 
     // block_map_t::update's box limits (block_map.h:84-103)
-    const auto & xl = h.mgn.x_lim_global;
+    const auto & xl = mgn.x_lim_global;
     for( int a = 0; a < 3; ++ a )
     {
         h.bmap.periodic[ a ] = h.tree.periodic[ a ];
@@ -287,6 +303,7 @@ static void build_mesh( const std::string & ini )
         h.bmap.l_box[ a ] = xl[ 1 ][ a ] - xl[ 0 ][ a ];
     }
     h.bmap.prx = h.prx.data(  );
+    h.mgn = std::move( mg );
 }
 
 ////////////////////////////////////////////////////////////
@@ -298,7 +315,7 @@ int kpref_float_size( void ) { return ( int ) sizeof( f_t ); }
 
 int kpref_mesh_load( const char * ini_path )
 {
-    try { build_mesh( ini_path ); }
+    try { build_mesh< mesh::meshgen::base_t >( ini_path ); }
     catch( const std::exception & e )
     {
         std::fprintf( stderr, "kpref_mesh_load: %s\n", e.what(  ) );
@@ -312,7 +329,7 @@ int kpref_n_blocks( void ) { return g_h ? ( int ) g_h->blocks.size(  ) : 0; }
 
 int kpref_block_cells( int * n3 )
 {
-    const auto & nc = g_h->mgn.nc_block(  );
+    const auto & nc = g_h->nc;
     for( int a = 0; a < 3; ++ a ) n3[ a ] = nc[ a ];
     return g_h->n_cell_blk;
 }
@@ -422,6 +439,93 @@ int kpref_trace( long n, const double * x, const double * dir,
         {
             x_out   [ 3 * p + a ] = par.x[ a ];
             cell_out[ 3 * p + a ] = par.i[ a ];
+        }
+        ib_out  [ p ] = par.ib_l;
+        step_out[ p ] = par.step;
+        todo_out[ p ] = par.dest.todo;
+    } );
+    if( flux_out )
+        for( size_t k = 0; k < h.flux.size(  ); ++ k )
+            flux_out[ k ] = h.flux[ k ];
+    if( flux_fx_out )
+        std::copy( h.flux_fx.begin(  ), h.flux_fx.end(  ), flux_fx_out );
+    return 0;
+}
+
+// Spherical-polar mesh (meshgen::sph_t on cyl_t's radial spacing, [mesh]
+// r_ratio; mesh/meshgen/spherical.h, cylindrical.h): axes (r, theta, phi).
+int kpref_mesh_load_sph( const char * ini_path )
+{
+    try { build_mesh< mesh::meshgen::sph_t >( ini_path ); }
+    catch( const std::exception & e )
+    {
+        std::fprintf( stderr, "kpref_mesh_load_sph: %s\n", e.what(  ) );
+        g_h.reset(  );
+        return -1;
+    }
+    g_h->spherical = true;
+    return ( int ) g_h->blocks.size(  );
+}
+
+// Per block: the radial faces x_fc( 0, 0..nc0 ) and every cell's volume
+// (geo_t::volume, x fastest), as float_t widened to double.
+int kpref_geo_sph( double * r_faces, double * vol )
+{
+    if( ! g_h ) return -1;
+    auto & h = * g_h;
+    const auto & nc = h.nc;
+    for( const auto & b : h.blocks )
+    {
+        const size_t id = b.id_l;
+        for( int i = 0; i <= nc[ 0 ]; ++ i )
+            r_faces[ id * ( nc[ 0 ] + 1 ) + i ] = b.geo.x_fc( 0, i );
+        size_t k = id * h.n_cell_blk;
+        for( int c2 = 0; c2 < nc[ 2 ]; ++ c2 )
+            for( int c1 = 0; c1 < nc[ 1 ]; ++ c1 )
+                for( int c0 = 0; c0 < nc[ 0 ]; ++ c0 )
+                    vol[ k ++ ] = b.geo.volume( type::idx_t( c0, c1, c2 ) );
+    }
+    return 0;
+}
+
+// photon::sph_t::proc (modules/particle/radiation/photon_sph.h) for every
+// packet: spherical x (r, theta, phi) and its Cartesian copy in, final state
+// and flux out.
+int kpref_trace_sph( long n, const double * x, const double * x_car, const double * dir,
+                     const int * cell, const int * ib, const double * proper,
+                     const int * steps, int fx_shift, int n_threads,
+                     double * x_out, double * x_car_out, int * cell_out, int * ib_out,
+                     int * step_out, int * todo_out,
+                     double * flux_out, long long * flux_fx_out )
+{
+    if( ! g_h || ! g_h->spherical ) return -1;
+    auto & h = * g_h;
+    h.fx_shift = fx_shift;
+    std::fill( h.flux.begin(  ), h.flux.end(  ), 0 );
+    std::fill( h.flux_fx.begin(  ), h.flux_fx.end(  ), 0 );
+    h.serial = ( n_threads <= 1 );
+    parallel_for( n, n_threads, [ & ]( long p )
+    {
+        particle::radiation::photon::sph_t<  > par;
+        par.dest.todo = particle::to_keep;
+        par.id        = ( int ) p;
+        for( int a = 0; a < 3; ++ a )
+        {
+            par.x    [ a ] = ( f_t ) x    [ 3 * p + a ];
+            par.x_car[ a ] = ( f_t ) x_car[ 3 * p + a ];
+            par.dir  [ a ] = ( f_t ) dir  [ 3 * p + a ];
+            par.i    [ a ] = cell[ 3 * p + a ];
+        }
+        par.ib_l   = ib[ p ];
+        par.proper = ( f_t ) proper[ p ];
+        par.step   = steps[ p ];
+        const int itg = 0;
+        par.proc( h.bmap, itg );
+        for( int a = 0; a < 3; ++ a )
+        {
+            x_out    [ 3 * p + a ] = par.x[ a ];
+            x_car_out[ 3 * p + a ] = par.x_car[ a ];
+            cell_out [ 3 * p + a ] = par.i[ a ];
         }
         ib_out  [ p ] = par.ib_l;
         step_out[ p ] = par.step;

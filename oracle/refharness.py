@@ -37,6 +37,8 @@ class RefMesh:
             cls._libs[precision] = ctypes.CDLL(path)
         return cls._libs[precision]
 
+    _loader = "kpref_mesh_load"
+
     def __init__(self, ini_text: str, precision: int = 1):
         self.lib = L = self._lib_for(precision)
         self.precision = precision
@@ -45,7 +47,7 @@ class RefMesh:
             f.write(ini_text)
             path = f.name
         try:
-            n = L.kpref_mesh_load(path.encode())
+            n = getattr(L, self._loader)(path.encode())
         finally:
             os.unlink(path)
         if n < 0:
@@ -103,6 +105,44 @@ class RefMesh:
                                   _p(out["flux"]), _p(out["flux_fx"]))
         if st != 0:
             raise RuntimeError("kpref_trace failed")
+        return out
+
+
+class RefMeshSph(RefMesh):
+    """Spherical-polar mesh built by the reference's meshgen::sph_t; axes
+    (r, theta, phi); [mesh] r_ratio sets the radial spacing."""
+
+    _loader = "kpref_mesh_load_sph"
+
+    def geometry_sph(self):
+        """(radial faces [nb, nc0 + 1], cell volumes [n_cells]) as float_t."""
+        rf = np.zeros((self.n_blocks, self.nc[0] + 1))
+        vol = np.zeros(self.n_cells)
+        if self.lib.kpref_geo_sph(_p(rf), _p(vol)) != 0:
+            raise RuntimeError("kpref_geo_sph failed")
+        return rf, vol
+
+    def trace(self, x, x_car, dir, cell, ib, proper, steps, fx_shift=32, n_threads=1):
+        """photon::sph_t::proc for every packet; final state + flux."""
+        n = len(ib)
+        c = lambda a, dt=np.float64, k=3: np.ascontiguousarray(a, dt).reshape(n, k) if k > 1 \
+            else np.ascontiguousarray(a, dt)
+        x, x_car, dir = c(x), c(x_car), c(dir)
+        cell, ib = c(cell, np.int32), c(ib, np.int32, 1)
+        proper, steps = c(proper, np.float64, 1), c(steps, np.int32, 1)
+        out = dict(x=np.zeros((n, 3)), x_car=np.zeros((n, 3)), cell=np.zeros((n, 3), np.int32),
+                   ib=np.zeros(n, np.int32), step=np.zeros(n, np.int32),
+                   todo=np.zeros(n, np.int32), flux=np.zeros(self.n_cells),
+                   flux_fx=np.zeros(self.n_cells, np.int64))
+        self.lib.kpref_trace_sph.argtypes = [ctypes.c_long] + [ctypes.c_void_p] * 7 + \
+            [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 8
+        st = self.lib.kpref_trace_sph(n, _p(x), _p(x_car), _p(dir), _p(cell), _p(ib), _p(proper),
+                                      _p(steps), fx_shift, n_threads, _p(out["x"]),
+                                      _p(out["x_car"]), _p(out["cell"]), _p(out["ib"]),
+                                      _p(out["step"]), _p(out["todo"]), _p(out["flux"]),
+                                      _p(out["flux_fx"]))
+        if st != 0:
+            raise RuntimeError("kpref_trace_sph failed")
         return out
 
 
