@@ -113,6 +113,66 @@ def make_bio(reference_tree):
     return [(p, os.path.getsize(p)) for p in (p1, p2)]
 
 
+# Spherical-polar fixture: r in [1, 3] geometric, theta [0.4, 2.7], phi periodic,
+# 16^3 cells in 8^3 blocks with one refined box.
+SPH_INI = """[mesh]
+x_min = 1.0 0.4 0.0
+x_max = 3.0 2.7 6.283185307179586
+n_cell_global = 16 16 16
+n_cell_block = 8 8 8
+r_ratio = -1.0
+
+[boundary]
+kinds = outflow outflow outflow outflow periodic periodic
+
+[refine_region_00000]
+level = 1
+x_min = 1.5 1.2 1.0
+x_max = 1.8 1.5 2.0
+"""
+
+
+def make_sph(precision, n=256, budget=120):
+    """Reference tables and photon::sph_t walk of seeded packets."""
+    ftype = np.float32 if precision == 1 else np.float64
+    ref = refharness.RefMeshSph(SPH_INI, precision)
+    rng = np.random.default_rng(300 + precision)
+    lo, hi = np.array([1.0, 0.4, 0.0]), np.array([3.0, 2.7, 2 * np.pi])
+    pad = np.array([0.02, 0.05, 0.0]) * (hi - lo)
+    x = lo + pad + rng.random((n, 3)) * (hi - lo - 2 * pad)
+    r, th, ph = x[:, 0], x[:, 1], x[:, 2]
+    xc = np.stack([r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)], 1)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    import tempfile
+    from kratos_polrad_b200 import Mesh
+    with tempfile.NamedTemporaryFile("w", suffix=".ini", delete=False) as f:
+        f.write(SPH_INI)
+    prod = Mesh(ini_path=f.name, spherical=True)
+    os.unlink(f.name)
+    rl, rr = ref.blocks()
+    pl, pr = prod.blocks()
+    key = {(int(l), *map(int, q)): i for i, (l, q) in enumerate(zip(pl, pr))}
+    inv = np.argsort(np.array([key[(int(l), *map(int, q))] for l, q in zip(rl, rr)]))
+    ib, cell = prod.locate(x)
+    x, xc, d = x.astype(ftype), xc.astype(ftype), d.astype(ftype)
+    proper = (rng.random(n) + 0.5).astype(ftype)
+    steps = np.full(n, budget, np.int32)
+    out = ref.trace(x, xc, d, cell, inv[ib], proper, steps, fx_shift=16)
+    xf0, dx0, vol0, pb = ref.geometry()
+    rf, vol = ref.geometry_sph()
+    ids, sh, dl = ref.neighbors()
+    path = os.path.join(HERE, f"sph_walk_p{precision}.npz")
+    np.savez_compressed(path, ini=np.array(SPH_INI), precision=np.int32(precision),
+                        ref_levels=rl, ref_regions=rr, xf0=xf0, dx0=dx0, vol0=vol0, phybnd=pb,
+                        r_faces=rf, volumes=vol, nb_ids=ids, nb_dlvl=dl,
+                        in_x=x, in_x_car=xc, in_dir=d, in_cell=cell.astype(np.int32),
+                        in_ib=inv[ib].astype(np.int32), in_proper=proper, in_steps=steps,
+                        out_x=out["x"], out_x_car=out["x_car"], out_cell=out["cell"],
+                        out_ib=out["ib"], out_step=out["step"], out_todo=out["todo"])
+    return path, os.path.getsize(path)
+
+
 if __name__ == "__main__":
     if not refharness.available(1):
         sys.exit("oracle/_ref not built: make -C oracle ref REF=<reference tree>")
@@ -121,3 +181,5 @@ if __name__ == "__main__":
         print(*make(name, prec))
     for p in make_bio(ref_tree):
         print(*p)
+    for prec in (1, 2):
+        print(*make_sph(prec))
