@@ -154,6 +154,19 @@ class mesh_t
 public:
     explicit mesh_t( const std::string & ini_path ) { api( kp_mesh_create_ini( ini_path.c_str(  ), & m_ ) ); }
     explicit mesh_t( const kp_mesh_desc_t & d ) { api( kp_mesh_create( & d, & m_ ) ); }
+    // Spherical-polar mesh (r, theta, phi) of meshgen::sph_t.
+    static mesh_t spherical( const kp_mesh_desc_t & d, double r_ratio )
+    {
+        kp_mesh_t * m = nullptr;
+        api( kp_mesh_create_sph( & d, r_ratio, & m ) );
+        return mesh_t( m );
+    }
+    static mesh_t spherical( const std::string & ini_path )
+    {
+        kp_mesh_t * m = nullptr;
+        api( kp_mesh_create_sph_ini( ini_path.c_str(  ), & m ) );
+        return mesh_t( m );
+    }
     ~mesh_t(  ) { if( m_ ) kp_mesh_destroy( m_ ); }
     mesh_t( const mesh_t & ) = delete;
     mesh_t & operator=( const mesh_t & ) = delete;
@@ -245,6 +258,20 @@ struct transport
     {
         api( kp_trace( m.get(  ), precision, n, x, dir, cell, ib, proper, step, todo, flux_mode,
                        fx_shift, flux, s ) );
+    }
+    static void trace_sph( mesh_t & m, int precision, long long n, void * x, void * x_car,
+                           const void * dir, int * cell, int * ib, const void * proper,
+                           int * step, int8_t * todo, int flux_mode, int fx_shift, void * flux,
+                           stream_t s = nullptr )
+    {
+        api( kp_trace_sph( m.get(  ), precision, n, x, x_car, dir, cell, ib, proper, step, todo,
+                           flux_mode, fx_shift, flux, s ) );
+    }
+    // One round of a decomposed solve on this rank (see kp_dd_round_t).
+    static void forward_dd( mesh_t & m, const kp_transport_cfg_t & c, const kp_dd_round_t & r,
+                            const kp_tallies_t & t, stream_t s = nullptr )
+    {
+        api( kp_transport_forward_dd( m.get(  ), & c, & r, & t, s ) );
     }
 };
 

@@ -40,6 +40,21 @@ static int host_part( const char * ini )
         std::printf( "OK throws \"%s\"\n", e.what(  ) );
     }
     std::printf( "OK abi %d\n", kp_abi_version(  ) );
+    // spherical mesh and runtime refinement through the C++ layer
+    kp_mesh_desc_t d {};
+    const double lo[ 3 ] = { 1.0, 0.4, 0.0 }, hi[ 3 ] = { 3.0, 2.7, 6.283185307179586 };
+    for( int a = 0; a < 3; ++ a )
+    {
+        d.x_min[ a ] = lo[ a ]; d.x_max[ a ] = hi[ a ];
+        d.n_cell_global[ a ] = 16; d.n_cell_block[ a ] = 8;
+    }
+    d.periodic[ 2 ] = 1;
+    kp::mesh_t sph = kp::mesh_t::spherical( d, -1.0 );
+    std::vector< int > flags( sph.info(  ).n_blocks, 0 );
+    flags[ 0 ] = 1;
+    kp::mesh_t fine = sph.adapt( flags );
+    if( fine.info(  ).n_blocks != sph.info(  ).n_blocks + 7 ) return 5;
+    std::printf( "OK spherical blocks=%d adapted=%d\n", sph.info(  ).n_blocks, fine.info(  ).n_blocks );
     return 0;
 }
 
