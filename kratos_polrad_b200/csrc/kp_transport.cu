@@ -35,6 +35,9 @@ namespace cg = cooperative_groups;
 // contribution is deposited and the walk resumes.  Peel-off rays draw no
 // random numbers, so each packet's history equals a sequential walk that
 // marches every peel-off ray at the moment of its interaction.
+#ifndef KP_PEEL_BATCH
+#define KP_PEEL_BATCH 24             // k_peel: lanes that wait for a fetch batch
+#endif
 #ifndef KP_FWD_RESIDENT
 #define KP_FWD_RESIDENT 768          // resident threads per SM the register budget targets
 #endif
@@ -44,7 +47,9 @@ namespace cg = cooperative_groups;
 // this rank's emissions; a ray handed off into a block of another rank is
 // written to that rank's out-queue instead of continuing.  Each packet's
 // arithmetic is that of the replicated solve.
-template< int TALLY, int NT, bool DD = false >
+// DEFER: a peel-off ray is written to the task queue for k_peel (when it
+// has room) instead of being marched here; the walk continues at once.
+template< int TALLY, int NT, bool DD = false, bool DEFER = false >
 __global__ void __launch_bounds__( NT, KP_FWD_RESIDENT / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
@@ -65,6 +70,22 @@ k_forward( const __grid_constant__ fwd_params_t P )
     int si = 0;                                   // scene of a batched launch
     int hop_ax = 0;                               // face axis of a pending hand-off
     bool solo = false;                            // DD: peel-off ray without a parked walk
+
+    // DEFER: appends the peel-off ray prepared in sp/sd (starting at p's
+    // position) to the queue; false when the queue is full.
+    auto defer_peel = [ & ](  ) -> bool
+    {
+        const unsigned long long k = atomicAdd( P.pq_count, 1ull );
+        if( k >= ( unsigned long long ) P.pq_cap )
+            return false;
+        const int t = threadIdx.x;
+        peel_task_t & o = P.pq[ k ];
+        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+        o.b = p.b;
+        o.w = sp.w[ t ]; o.I = sp.I[ t ]; o.Q = sp.Q[ t ]; o.U = sp.U[ t ]; o.V = sp.V[ t ];
+        o.pix = sp.pix[ t ]; o.cpix = sd.cpix[ t ];
+        return true;
+    };
 
     // coefficients of cell c of block b (DD: owned blocks stored compactly)
     auto sigma_at = [ & ]( int b, const int c[ 3 ] ) -> float2
@@ -383,10 +404,16 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sp.Q[ t ] = sp.U[ t ] = sp.V[ t ] = 0.0f;
                     sp.pix[ t ] = pix;
                     sd.cpix[ t ] = coarse_pixel( P, pix, sc.batch[ t ] );
-                    pend = 0; ptau = 0.0f; pk = 0;
-                    park_walk( sp, p );
-                    park_dir( sd, p, P.o, P.inv_o );
-                    peel = true;
+                    bool queued = false;
+                    if constexpr( DEFER )
+                        queued = defer_peel(  );
+                    if( ! queued )
+                    {
+                        pend = 0; ptau = 0.0f; pk = 0;
+                        park_walk( sp, p );
+                        park_dir( sd, p, P.o, P.inv_o );
+                        peel = true;
+                    }
                 }
             }
             faces_all( P.m, p.b, p.c, p.d, fx );
@@ -440,6 +467,9 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             if( ! end && p.n_steps >= P.max_steps )
                 end = PK_STEP_CAP;
+            if constexpr( DEFER )
+                if( do_peel && defer_peel(  ) )
+                    do_peel = false;             // queued: the walk goes on (or ends) now
             if( do_peel )
             {
                 park_walk( sp, p );
@@ -519,6 +549,129 @@ k_forward( const __grid_constant__ fwd_params_t P )
         atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );
 }
 
+// Marches the peel-off rays k_forward<..., DEFER> queued: each lane takes a
+// task, walks it toward the observer segment by segment exactly as the
+// forward kernel's inline peel-off ray does (same face cache, hand-off,
+// tau cut, deposit), and takes the next.  Fetches (with the deposit of the
+// finished ray) and block hand-offs wait for batches of lanes, as in
+// k_forward.  The direction is the launch's observer direction, so a lane
+// holds only the ray's position, faces, cell and optical depth.
+template< int TALLY >
+__global__ void __launch_bounds__( 256 )
+k_peel( const __grid_constant__ fwd_params_t P )
+{
+    __shared__ unsigned long long cnt_s[ KP_NCOUNTERS ];
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    if( threadIdx.x < KP_NCOUNTERS ) cnt_s[ threadIdx.x ] = 0;
+    __syncthreads(  );
+    const unsigned long long n_tasks =
+        min( * P.pq_count, ( unsigned long long ) P.pq_cap );
+    double x[ 3 ], fx[ 3 ];
+    int    c[ 3 ] = { 0, 0, 0 }, b = 0, hop_ax = 0, pk = 0;
+    float  ptau = 0.0f;
+    long long task = -1;
+    unsigned n_seg_done = 0;
+    int phase = PH_EMIT;
+    for( ;; )
+    {
+        const unsigned m_fetch = __ballot_sync( FULL, phase == PH_EMIT );
+        const unsigned m_seg   = __ballot_sync( FULL, phase == PH_SEGMENT );
+        const unsigned m_hop   = __ballot_sync( FULL, phase == PH_HOP );
+        if( ( m_fetch | m_seg | m_hop ) == 0u )
+            break;
+        const int n_fetch = __popc( m_fetch ), n_seg = __popc( m_seg ), n_hop = __popc( m_hop );
+        int run;
+        if( n_fetch > 0 && ( n_fetch >= P.peel_batch || n_seg == 0 ) )
+            run = PH_EMIT;
+        else if( n_hop > 0 && ( n_hop >= P.hop_batch || n_seg == 0 ) )
+            run = PH_HOP;
+        else
+            run = PH_SEGMENT;
+
+        if( run == PH_EMIT )
+        {
+            if( phase != PH_EMIT ) continue;
+            if( task >= 0 && ptau <= P.tau_cut )
+            {   // deposit of the ray that just ended (after_crossing's)
+                const peel_task_t & o = P.pq[ task ];
+                const float att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                deposit_pixel< TALLY >( P, o.pix, o.cpix, __fmul_rn( att, o.I ), __fmul_rn( att, o.Q ),
+                                        __fmul_rn( att, o.U ), __fmul_rn( att, o.V ) );
+                atomicAdd( cnt_s + KP_CNT_DEPOSITS, 1ull );
+            }
+            task = -1;
+            const int leader = __ffs( m_fetch ) - 1;
+            const unsigned rank = __popc( m_fetch & ( ( 1u << lane ) - 1u ) );
+            unsigned long long base = 0;
+            if( ( int ) lane == leader )
+                base = atomicAdd( P.pq_next, ( unsigned long long ) n_fetch );
+            base = __shfl_sync( m_fetch, base, leader );
+            const unsigned long long idx = base + rank;
+            if( idx >= n_tasks )
+            {
+                phase = PH_DONE;
+                continue;
+            }
+            const peel_task_t & o = P.pq[ idx ];
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a ) { x[ a ] = o.x[ a ]; c[ a ] = o.c[ a ]; }
+            b = o.b;
+            task = ( long long ) idx;
+            ptau = 0.0f; pk = 0;
+            faces_all( P.m, b, c, P.o, fx );
+            phase = PH_SEGMENT;
+            continue;
+        }
+
+        if( run == PH_HOP )
+        {
+            if( phase != PH_HOP ) continue;
+            const int b_old = b;
+            bool lost;
+            const bool left = ! cross_face( P.m, b, c, x, hop_ax, comp( P.o, hop_ax ) > 0.0f, lost );
+            if( left )
+            {
+                phase = PH_EMIT;
+                continue;
+            }
+            faces_all( P.m, b, c, P.o, fx );
+            if( b != b_old ) atomicAdd( cnt_s + KP_CNT_HOPS, 1ull );
+            phase = pk >= ( 1 << 20 ) ? PH_EMIT : PH_SEGMENT;
+            continue;
+        }
+
+        if( phase != PH_SEGMENT ) continue;
+        const float2 sg = P.m.sigma[ cell_index( P.m, b, c ) ];
+        const float ext = __fadd_rn( sg.x, sg.y );
+        int ax;
+        const double t = exit_cached( x, fx, P.o, P.inv_o, ax );
+        ++ n_seg_done;
+        ++ pk;
+        ptau = __fadd_rn( ptau, __fmul_rn( ext, ( float ) t ) );
+        if( ptau > P.tau_cut )
+        {
+            phase = PH_EMIT;
+            continue;
+        }
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+            if( a != ax ) x[ a ] = __fma_rn( t, ( double ) comp( P.o, a ), x[ a ] );
+        if( ! step_in_block( P.m, b, c, x, fx, ax, P.o ) )
+        {
+            hop_ax = ax;
+            phase = PH_HOP;
+            continue;
+        }
+        if( pk >= ( 1 << 20 ) )
+            phase = PH_EMIT;
+    }
+    atomicAdd( cnt_s + KP_CNT_PEEL_STEPS, ( unsigned long long ) n_seg_done );
+    __syncthreads(  );
+    if( P.counters && threadIdx.x < KP_NCOUNTERS && cnt_s[ threadIdx.x ] )
+        atomicAdd( P.counters + threadIdx.x, cnt_s[ threadIdx.x ] );
+}
+
 }   // namespace
 
 ////////////////////////////////////////////////////////////
@@ -595,6 +748,7 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     // scenes, whatever the event batch): the neighbour lookup and the new
     // block's geometry are dependent loads, paid once per batch.
     P.hop_batch = 8;
+    P.peel_batch = KP_PEEL_BATCH;
     P.mu_tally = t.mu;
     P.image = t.image;
     P.img_batch = t.image_batch;
@@ -675,6 +829,41 @@ void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int
 
 }   // namespace kp
 
+namespace kp
+{
+// Solve with peel-off rays deferred: k_forward<..., DEFER> walks the packets
+// and queues their peel-off rays (marching them inline only if the queue is
+// full), then k_peel marches the queue.  The queue belongs to the mesh and
+// grows to 12 rays per packet, at most 2^27 rays (10.7 GB).
+template< int TALLY >
+void launch_deferred( kp_mesh_t * mesh, fwd_params_t & P, cudaStream_t s )
+{
+    const long long want = std::min< long long >( std::max< long long >( 12 * P.n_packets, 1 << 16 ),
+                                                  1ll << 27 );
+    if( mesh->pq_cap < want )
+    {
+        cudaFree( mesh->d_pq );
+        mesh->d_pq = nullptr;
+        mesh->pq_cap = 0;
+        KP_CUDA( cudaMalloc( & mesh->d_pq, ( size_t ) want * sizeof( peel_task_t ) ) );
+        mesh->pq_cap = want;
+    }
+    P.pq = static_cast< peel_task_t * >( mesh->d_pq );
+    P.pq_cap = mesh->pq_cap;
+    P.pq_count = P.work + 1;
+    P.pq_next = P.work + 2;
+    KP_CUDA( cudaMemsetAsync( P.work, 0, 3 * sizeof( unsigned long long ), s ) );
+    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true >;
+    long long grid = persistent_grid( kf, 256 );
+    grid = std::min< long long >( grid, ( P.n_packets + 255 ) / 256 );
+    k_forward< TALLY, 256, false, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+    KP_CUDA( cudaGetLastError(  ) );
+    const long long gp = persistent_grid( ( const void * ) k_peel< TALLY >, 256 );
+    k_peel< TALLY ><<< ( unsigned ) gp, 256, 0, s >>>( P );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+}   // namespace kp
+
 extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                                      const kp_tallies_t * tallies, void * stream )
 {
@@ -685,6 +874,16 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = mesh->workspace(  );
+        if( cfg->image_n > 0 && P.n_packets > 0 )
+        {   // peel-off rays through their own kernel; without them the walk
+            // kernel's interactions run best in batches of 12 lanes (measured)
+            if( cfg->lane_batch == 0 ) P.ev_batch = 12;
+            if( cfg->tally_mode == KP_TALLY_FIXED )
+                kp::launch_deferred< KP_TALLY_FIXED >( mesh, P, ( cudaStream_t ) stream );
+            else
+                kp::launch_deferred< KP_TALLY_FLOAT >( mesh, P, ( cudaStream_t ) stream );
+            return;
+        }
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
     } );
 }

@@ -64,6 +64,7 @@ struct fwd_params_t
     long long   max_steps;
     int         ev_batch;          // lanes that must wait for an event batch
     int         hop_batch;         // lanes that must wait for a hand-off batch
+    int         peel_batch;        // k_peel: lanes that must wait for a fetch batch
     double      lk_inv[ 3 ];       // lookup cells per unit length
     void      * mu_tally;
     void      * image;
@@ -96,7 +97,23 @@ struct fwd_params_t
     int       * dd_out_peel_rank;
     long long   dd_cap_walk, dd_cap_peel;
     unsigned long long * dd_out_count;  // [2]: walks, peel-off rays
+    // peel-off rays deferred to k_peel (plain forward solves)
+    struct peel_task_t * pq;            // [pq_cap] tasks
+    unsigned long long * pq_count;      // tasks written (may exceed pq_cap: those ran inline)
+    unsigned long long * pq_next;       // k_peel's task counter
+    long long   pq_cap;
     src_dev_t   src[ MAX_SOURCES ];
+};
+
+// A peel-off ray waiting for k_peel: where it starts (the interaction or
+// emission point) and its pending contribution.
+struct __align__( 16 ) peel_task_t
+{
+    double x[ 3 ];
+    int    b, c[ 3 ];
+    float  w, I, Q, U, V;
+    int    pix, cpix;
+    int    pad[ 3 ];
 };
 
 // A packet's walk crossing into a block of another rank (it has entered the
