@@ -119,9 +119,9 @@ def measured_peak():
 
 
 def ncu_traffic(n_packets):
-    """DRAM bytes (read + write) of one transport launch from the committed
-    ncu summary (profiles/k_forward_clump_traffic.txt), when it was captured on
-    this packet count (the traffic does not scale with packets), else None."""
+    """DRAM bytes (read + write) of the two launches of one solve, per kernel,
+    from the committed ncu summary (profiles/k_forward_clump_traffic.txt),
+    when it was captured on this packet count, else None."""
     p = os.path.join(ROOT, "profiles", "k_forward_clump_traffic.txt")
     try:
         kv = {}
@@ -131,7 +131,8 @@ def ncu_traffic(n_packets):
                 kv[k.strip()] = float(v)
         if int(kv["packets"]) != int(n_packets):
             return None
-        return kv["dram_read_bytes"] + kv["dram_write_bytes"]
+        return {k: kv[k + ".dram_read_bytes"] + kv[k + ".dram_write_bytes"]
+                for k in ("k_forward", "k_peel")}
     except (OSError, KeyError, ValueError):
         return None
 
@@ -590,6 +591,10 @@ def main():
           for _ in range(args.steps)]
     kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
+    # recorded by the library between the walk and the peel-off kernel
+    mid = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for e in mid:
+        e.record()                      # creates the CUDA event
     counts = []
     if world > 1:
         dist.barrier()
@@ -600,6 +605,7 @@ def main():
             flush.fill_(float(k))
             ev[k][0].record()
             kev[k][0].record()
+            call("kp_transport_split_event", mid[k].cuda_event)
             forward(mesh, cfg, tal)
             kev[k][1].record()
             allreduce()
@@ -609,7 +615,10 @@ def main():
     if world > 1:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    call("kp_transport_split_event", None)
     kern_ms = [a.elapsed_time(b) for a, b in kev]
+    walk_ms = statistics.mean(a.elapsed_time(m) for (a, _), m in zip(kev, mid))
+    peel_ms = statistics.mean(m.elapsed_time(b) for (_, b), m in zip(kev, mid))
     t_local = sum(step_ms) / 1e3
     t = torch.tensor([t_local], dtype=torch.float64, device=dev)
     if world > 1:
@@ -631,11 +640,17 @@ def main():
     kern_s = statistics.mean(kern_ms) / 1e3
     peak, peak_kind = measured_peak()
     ach = algorithmic_bytes(c_rank) / kern_s / 1e9
+    traffic = ncu_traffic(n_pk)
     roofline = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": ach / peak, "peak_source": peak_kind, "kernel": "k_forward",
-                "traffic": ncu_traffic(n_pk),
+                "frac": ach / peak, "peak_source": peak_kind,
+                "kernel": "k_forward + k_peel (the two launches of one solve)",
+                "traffic": sum(traffic.values()) if traffic else None,
                 "algorithmic_bytes": algorithmic_bytes(c_rank),
-                "kernel_ms": statistics.mean(kern_ms)}
+                "kernel_ms": statistics.mean(kern_ms),
+                "kernels": {"k_forward": {"ms": walk_ms, "share": walk_ms / (walk_ms + peel_ms),
+                                          "traffic": traffic and traffic["k_forward"]},
+                            "k_peel": {"ms": peel_ms, "share": peel_ms / (walk_ms + peel_ms),
+                                       "traffic": traffic and traffic["k_peel"]}}}
 
     # ---- adjoint: gradient of an image loss, cost relative to one forward ----
     from kratos_polrad_b200.adjoint import adjoint as run_adjoint
@@ -713,7 +728,8 @@ def main():
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
                "adjoint": adjoint_info,
-               "gpu_launches": args.steps, "clocks": clk.summary()}
+               "gpu_launches": args.steps * (2 if cfg.image_n > 0 else 1),
+               "clocks": clk.summary()}
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()

@@ -330,6 +330,14 @@ typedef struct kp_tallies
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
+/* Profiling hook.  With an image, kp_transport_forward runs two kernels:
+ * the walk (which queues the peel-off rays) and the peel-off march.  Later
+ * kp_transport_forward calls of this host thread record `event` (a
+ * cudaEvent_t) on their stream between the two launches, so that a caller
+ * can time them apart; without an image it is recorded after the only
+ * kernel.  NULL turns it off.  No counterpart in the reference. */
+int kp_transport_split_event( void * event );
+
 /* ------------------------------------------------------------------ */
 /* Batched solves: many independent scenes in one persistent launch.    */
 /* The reference solves one mesh per process, one cycle at a time       */

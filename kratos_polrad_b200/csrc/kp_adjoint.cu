@@ -385,8 +385,8 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         }
         after_crossing( peel_cut, false, false );
     }
-    count( sp, KP_CNT_STEPS, cnt.steps );
-    count( sp, KP_CNT_PEEL_STEPS, cnt.peel );
+    count_all( sp, KP_CNT_STEPS, cnt.steps );
+    count_all( sp, KP_CNT_PEEL_STEPS, cnt.peel );
     __syncthreads(  );
     if( P.counters && threadIdx.x < KP_NCOUNTERS && sp.cnt[ threadIdx.x ] )
         atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );

@@ -38,6 +38,15 @@ namespace cg = cooperative_groups;
 #ifndef KP_PEEL_BATCH
 #define KP_PEEL_BATCH 24             // k_peel: lanes that wait for a fetch batch
 #endif
+#ifndef KP_PEEL_INNER
+#define KP_PEEL_INNER 8              // k_peel: segments per scheduling round
+#endif
+#ifndef KP_PEEL_MINB
+#define KP_PEEL_MINB 4               // k_peel: resident blocks of 256 the registers allow
+#endif
+#ifndef KP_WALK_INNER
+#define KP_WALK_INNER 2              // k_forward<DEFER>: segments per scheduling round
+#endif
 #ifndef KP_FWD_RESIDENT
 #define KP_FWD_RESIDENT 768          // resident threads per SM the register budget targets
 #endif
@@ -72,10 +81,17 @@ k_forward( const __grid_constant__ fwd_params_t P )
     bool solo = false;                            // DD: peel-off ray without a parked walk
 
     // DEFER: appends the peel-off ray prepared in sp/sd (starting at p's
-    // position) to the queue; false when the queue is full.
+    // position) to the queue; false when the queue is full.  The lanes that
+    // append together take their slots with one atomic.
     auto defer_peel = [ & ](  ) -> bool
     {
-        const unsigned long long k = atomicAdd( P.pq_count, 1ull );
+        const unsigned m = __activemask(  );
+        const int leader = __ffs( m ) - 1;
+        unsigned long long base = 0;
+        if( ( int ) lane == leader )
+            base = atomicAdd( P.pq_count, ( unsigned long long ) __popc( m ) );
+        base = __shfl_sync( m, base, leader );
+        const unsigned long long k = base + __popc( m & ( ( 1u << lane ) - 1u ) );
         if( k >= ( unsigned long long ) P.pq_cap )
             return false;
         const int t = threadIdx.x;
@@ -494,56 +510,63 @@ k_forward( const __grid_constant__ fwd_params_t P )
             continue;
         }
 
-        // ---- PH_SEGMENT: one segment of the active ray ----
+        // ---- PH_SEGMENT: segments of the active ray, up to KP_WALK_INNER
+        // (DEFER) before the next scheduling round ----
         if( phase != PH_SEGMENT ) continue;
-        // the active ray's direction is in p.d / p.inv (a peel-off ray holds
-        // them while the walk's are parked)
-        const float2 sg = sigma_at( p.b, p.c );
-        const float ext = __fadd_rn( sg.x, sg.y );
-        int ax;
-        const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
-        const float et = __fmul_rn( ext, ( float ) t );
-        bool interact = false, peel_cut = false;
-        if( peel )
+        #pragma unroll 1
+        for( int it = 0; it < ( DEFER ? KP_WALK_INNER : 1 ); ++ it )
         {
-            ++ cnt.peel;
-            ++ pk;
-            ptau = __fadd_rn( ptau, et );
-            peel_cut = ptau > P.tau_cut;
-        }
-        else
-        {
-            ++ cnt.steps;
-            ++ p.n_steps;
-            interact = et >= p.tau;
-        }
-        if( interact )
-        {
-            double ti = ( double ) __fdiv_rn( p.tau, ext );
-            ti = ti > t ? t : ti;
-            p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
-            p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
-            p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
-            phase = PH_EVENT;
-            continue;
-        }
-        if( ! peel_cut )
-        {   // advance to the exit face and into the next cell (shared code)
-            if( ! peel ) p.tau = __fsub_rn( p.tau, et );
-            #pragma unroll
-            for( int a = 0; a < 3; ++ a )
-                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
-            if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
-            {   // leaves the block: wait for a batched hand-off
-                hop_ax = ax;
-                phase = PH_HOP;
-                continue;
+            // the active ray's direction is in p.d / p.inv (a peel-off ray
+            // holds them while the walk's are parked)
+            const float2 sg = sigma_at( p.b, p.c );
+            const float ext = __fadd_rn( sg.x, sg.y );
+            int ax;
+            const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
+            const float et = __fmul_rn( ext, ( float ) t );
+            bool interact = false, peel_cut = false;
+            if( peel )
+            {
+                ++ cnt.peel;
+                ++ pk;
+                ptau = __fadd_rn( ptau, et );
+                peel_cut = ptau > P.tau_cut;
             }
+            else
+            {
+                ++ cnt.steps;
+                ++ p.n_steps;
+                interact = et >= p.tau;
+            }
+            if( interact )
+            {
+                double ti = ( double ) __fdiv_rn( p.tau, ext );
+                ti = ti > t ? t : ti;
+                p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
+                p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
+                p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
+                phase = PH_EVENT;
+                break;
+            }
+            if( ! peel_cut )
+            {   // advance to the exit face and into the next cell (shared code)
+                if( ! peel ) p.tau = __fsub_rn( p.tau, et );
+                #pragma unroll
+                for( int a = 0; a < 3; ++ a )
+                    if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
+                if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
+                {   // leaves the block: wait for a batched hand-off
+                    hop_ax = ax;
+                    phase = PH_HOP;
+                    break;
+                }
+            }
+            after_crossing( peel_cut, false, false );
+            if( phase != PH_SEGMENT )
+                break;
         }
-        after_crossing( peel_cut, false, false );
     }
-    count( sp, KP_CNT_STEPS, cnt.steps );
-    count( sp, KP_CNT_PEEL_STEPS, cnt.peel );
+    count_all( sp, KP_CNT_STEPS, cnt.steps );
+    count_all( sp, KP_CNT_PEEL_STEPS, cnt.peel );
     __syncthreads(  );
     if( P.counters && threadIdx.x < KP_NCOUNTERS && sp.cnt[ threadIdx.x ] )
         atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );
@@ -554,10 +577,14 @@ k_forward( const __grid_constant__ fwd_params_t P )
 // forward kernel's inline peel-off ray does (same face cache, hand-off,
 // tau cut, deposit), and takes the next.  Fetches (with the deposit of the
 // finished ray) and block hand-offs wait for batches of lanes, as in
-// k_forward.  The direction is the launch's observer direction, so a lane
-// holds only the ray's position, faces, cell and optical depth.
+// k_forward; segments run up to KP_PEEL_INNER at a time between two
+// scheduling rounds.  The direction is the launch's observer direction, so
+// the face side and the cell-index step of each axis are the same for every
+// lane, and a lane holds only the ray's position, faces, cell, optical depth
+// and its block's origin and spacing (the next face is computed from them,
+// with exit_dist's expression, without a load).
 template< int TALLY >
-__global__ void __launch_bounds__( 256 )
+__global__ void __launch_bounds__( 256, KP_PEEL_MINB )
 k_peel( const __grid_constant__ fwd_params_t P )
 {
     __shared__ unsigned long long cnt_s[ KP_NCOUNTERS ];
@@ -567,12 +594,29 @@ k_peel( const __grid_constant__ fwd_params_t P )
     __syncthreads(  );
     const unsigned long long n_tasks =
         min( * P.pq_count, ( unsigned long long ) P.pq_cap );
-    double x[ 3 ], fx[ 3 ];
-    int    c[ 3 ] = { 0, 0, 0 }, b = 0, hop_ax = 0, pk = 0;
+    const int nc0 = P.m.nc[ 0 ], nc1 = P.m.nc[ 1 ];
+    double x[ 3 ], fx[ 3 ], g0[ 3 ], gd[ 3 ];
+    int    c[ 3 ] = { 0, 0, 0 }, b = 0, hop_ax = 0, pk = 0, ci = 0;
+    const float2 * sb = P.m.sigma;                // this block's coefficients
     float  ptau = 0.0f;
     long long task = -1;
     unsigned n_seg_done = 0;
     int phase = PH_EMIT;
+    // geometry of block b, its face cache and the cell's index in the block
+    auto enter = [ & ](  )
+    {
+        const double * g = P.m.geo_d + 16 * ( size_t ) b;
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+        {
+            g0[ a ] = g[ a ];
+            gd[ a ] = g[ 3 + a ];
+            fx[ a ] = __fma_rn( ( double ) ( c[ a ] + ( comp( P.o, a ) > 0.0f ? 1 : 0 ) ), gd[ a ],
+                                g0[ a ] );
+        }
+        sb = P.m.sigma + ( size_t ) b * P.m.cpb;
+        ci = c[ 0 ] + nc0 * ( c[ 1 ] + nc1 * c[ 2 ] );
+    };
     for( ;; )
     {
         const unsigned m_fetch = __ballot_sync( FULL, phase == PH_EMIT );
@@ -592,16 +636,19 @@ k_peel( const __grid_constant__ fwd_params_t P )
         if( run == PH_EMIT )
         {
             if( phase != PH_EMIT ) continue;
-            if( task >= 0 && ptau <= P.tau_cut )
+            const int leader = __ffs( m_fetch ) - 1;
+            const bool dep = task >= 0 && ptau <= P.tau_cut;
+            if( dep )
             {   // deposit of the ray that just ended (after_crossing's)
                 const peel_task_t & o = P.pq[ task ];
                 const float att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
                 deposit_pixel< TALLY >( P, o.pix, o.cpix, __fmul_rn( att, o.I ), __fmul_rn( att, o.Q ),
                                         __fmul_rn( att, o.U ), __fmul_rn( att, o.V ) );
-                atomicAdd( cnt_s + KP_CNT_DEPOSITS, 1ull );
             }
+            const unsigned m_dep = __ballot_sync( m_fetch, dep );
+            if( ( int ) lane == leader && m_dep )
+                atomicAdd( cnt_s + KP_CNT_DEPOSITS, ( unsigned long long ) __popc( m_dep ) );
             task = -1;
-            const int leader = __ffs( m_fetch ) - 1;
             const unsigned rank = __popc( m_fetch & ( ( 1u << lane ) - 1u ) );
             unsigned long long base = 0;
             if( ( int ) lane == leader )
@@ -619,7 +666,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
             b = o.b;
             task = ( long long ) idx;
             ptau = 0.0f; pk = 0;
-            faces_all( P.m, b, c, P.o, fx );
+            enter(  );
             phase = PH_SEGMENT;
             continue;
         }
@@ -630,43 +677,68 @@ k_peel( const __grid_constant__ fwd_params_t P )
             const int b_old = b;
             bool lost;
             const bool left = ! cross_face( P.m, b, c, x, hop_ax, comp( P.o, hop_ax ) > 0.0f, lost );
+            const unsigned m_moved = __ballot_sync( m_hop, ! left && b != b_old );
+            if( lane == ( unsigned ) ( __ffs( m_hop ) - 1 ) && m_moved )
+                atomicAdd( cnt_s + KP_CNT_HOPS, ( unsigned long long ) __popc( m_moved ) );
             if( left )
             {
                 phase = PH_EMIT;
                 continue;
             }
-            faces_all( P.m, b, c, P.o, fx );
-            if( b != b_old ) atomicAdd( cnt_s + KP_CNT_HOPS, 1ull );
+            enter(  );
             phase = pk >= ( 1 << 20 ) ? PH_EMIT : PH_SEGMENT;
             continue;
         }
 
         if( phase != PH_SEGMENT ) continue;
-        const float2 sg = P.m.sigma[ cell_index( P.m, b, c ) ];
-        const float ext = __fadd_rn( sg.x, sg.y );
-        int ax;
-        const double t = exit_cached( x, fx, P.o, P.inv_o, ax );
-        ++ n_seg_done;
-        ++ pk;
-        ptau = __fadd_rn( ptau, __fmul_rn( ext, ( float ) t ) );
-        if( ptau > P.tau_cut )
+        #pragma unroll 1
+        for( int it = 0; it < KP_PEEL_INNER; ++ it )
         {
-            phase = PH_EMIT;
-            continue;
+            const float2 sg = sb[ ci ];
+            const float ext = __fadd_rn( sg.x, sg.y );
+            int ax;
+            const double t = exit_cached( x, fx, P.o, P.inv_o, ax );
+            ++ n_seg_done;
+            ++ pk;
+            ptau = __fadd_rn( ptau, __fmul_rn( ext, ( float ) t ) );
+            if( ptau > P.tau_cut )
+            {
+                phase = PH_EMIT;
+                break;
+            }
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a )
+                if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
+            // step_in_block with the block geometry in registers
+            const bool pos = comp( P.o, ax ) > 0.0f;
+            const int cax = ax == 0 ? c[ 0 ] : ( ax == 1 ? c[ 1 ] : c[ 2 ] );
+            const int cn = cax + ( pos ? 1 : -1 );
+            if( cn < 0 || cn >= ( ax == 0 ? nc0 : ( ax == 1 ? nc1 : P.m.nc[ 2 ] ) ) )
+            {
+                hop_ax = ax;
+                phase = PH_HOP;
+                break;
+            }
+            const double nf = __fma_rn( ( double ) ( cn + ( pos ? 1 : 0 ) ),
+                                        ax == 0 ? gd[ 0 ] : ( ax == 1 ? gd[ 1 ] : gd[ 2 ] ),
+                                        ax == 0 ? g0[ 0 ] : ( ax == 1 ? g0[ 1 ] : g0[ 2 ] ) );
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a )
+                if( a == ax ) { c[ a ] = cn; x[ a ] = fx[ a ]; fx[ a ] = nf; }
+            const int st = ax == 0 ? 1 : ( ax == 1 ? nc0 : nc0 * nc1 );
+            ci += pos ? st : -st;
+            if( pk >= ( 1 << 20 ) )
+            {
+                phase = PH_EMIT;
+                break;
+            }
         }
-        #pragma unroll
-        for( int a = 0; a < 3; ++ a )
-            if( a != ax ) x[ a ] = __fma_rn( t, ( double ) comp( P.o, a ), x[ a ] );
-        if( ! step_in_block( P.m, b, c, x, fx, ax, P.o ) )
-        {
-            hop_ax = ax;
-            phase = PH_HOP;
-            continue;
-        }
-        if( pk >= ( 1 << 20 ) )
-            phase = PH_EMIT;
     }
-    atomicAdd( cnt_s + KP_CNT_PEEL_STEPS, ( unsigned long long ) n_seg_done );
+    {   // all lanes of the warp are here
+        const unsigned v = __reduce_add_sync( FULL, n_seg_done );
+        if( lane == 0 )
+            atomicAdd( cnt_s + KP_CNT_PEEL_STEPS, ( unsigned long long ) v );
+    }
     __syncthreads(  );
     if( P.counters && threadIdx.x < KP_NCOUNTERS && cnt_s[ threadIdx.x ] )
         atomicAdd( P.counters + threadIdx.x, cnt_s[ threadIdx.x ] );
@@ -831,6 +903,9 @@ void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int
 
 namespace kp
 {
+// Event recorded between the two kernels of a solve (kp_transport_split_event).
+thread_local cudaEvent_t split_event = nullptr;
+
 // Solve with peel-off rays deferred: k_forward<..., DEFER> walks the packets
 // and queues their peel-off rays (marching them inline only if the queue is
 // full), then k_peel marches the queue.  The queue belongs to the mesh and
@@ -858,6 +933,7 @@ void launch_deferred( kp_mesh_t * mesh, fwd_params_t & P, cudaStream_t s )
     grid = std::min< long long >( grid, ( P.n_packets + 255 ) / 256 );
     k_forward< TALLY, 256, false, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
+    if( split_event ) KP_CUDA( cudaEventRecord( split_event, s ) );
     const long long gp = persistent_grid( ( const void * ) k_peel< TALLY >, 256 );
     k_peel< TALLY ><<< ( unsigned ) gp, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
@@ -885,7 +961,14 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
             return;
         }
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
+        if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
     } );
+}
+
+extern "C" int kp_transport_split_event( void * event )
+{
+    kp::split_event = static_cast< cudaEvent_t >( event );
+    return KP_OK;
 }
 
 ////////////////////////////////////////////////////////////

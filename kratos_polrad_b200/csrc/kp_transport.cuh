@@ -676,10 +676,23 @@ __device__ __forceinline__ void unpark_walk( const SP & sp, packet_t & p )
     for( int a = 0; a < 3; ++ a ) { p.x[ a ] = sp.x[ a ][ t ]; p.c[ a ] = sp.c[ a ][ t ]; }
     p.b = sp.b[ t ];
 }
+// One event for counter k: the lanes that count the same k together add
+// with one shared atomic (lanes of a batch would otherwise serialise on it).
 template< class SP >
-__device__ __forceinline__ void count( SP & sp, int k, unsigned v = 1u )
+__device__ __forceinline__ void count( SP & sp, int k )
 {
-    atomicAdd( sp.cnt + k, ( unsigned long long ) v );
+    const unsigned m = __match_any_sync( __activemask(  ), k );
+    if( ( threadIdx.x & 31u ) == ( unsigned ) ( __ffs( m ) - 1 ) )
+        atomicAdd( sp.cnt + k, ( unsigned long long ) __popc( m ) );
+}
+// v events per lane for counter k, all lanes of the warp together (after
+// the scheduling loop).
+template< class SP >
+__device__ __forceinline__ void count_all( SP & sp, int k, unsigned v )
+{
+    const unsigned s = __reduce_add_sync( 0xffffffffu, v );
+    if( ( threadIdx.x & 31u ) == 0 && s )
+        atomicAdd( sp.cnt + k, ( unsigned long long ) s );
 }
 
 // Host helpers shared by the transport entry points (kp_transport.cu).
