@@ -330,6 +330,16 @@ typedef struct kp_tallies
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
+/* Upper bound on the mesh's peel-off queue (device memory, 80 B per ray;
+ * default 2^27 rays = 10.7 GB).  With an image, kp_transport_forward queues
+ * the peel-off rays of its packets and marches them in a second kernel; the
+ * queue holds 12 rays per packet, so solves of more than limit/12 packets
+ * run in chunks of that many packets, and a chunk that queues more rays
+ * than the queue holds marches the rest where they start (same tallies).
+ * A queue larger than the new limit is freed now.  Limits below 1024 rays
+ * are refused (KP_ERR_CONFIG).  No counterpart in the reference. */
+int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays );
+
 /* Profiling hook.  With an image, kp_transport_forward runs two kernels:
  * the walk (which queues the peel-off rays) and the peel-off march.  Later
  * kp_transport_forward calls of this host thread record `event` (a

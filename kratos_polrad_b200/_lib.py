@@ -84,6 +84,7 @@ _SIGS = {
     "kp_event_elapsed": [P(c_float), c_void_p, c_void_p],
     "kp_launch_host": [c_void_p, c_void_p, c_void_p],
     "kp_transport_split_event": [c_void_p],
+    "kp_mesh_peel_queue_limit": [c_void_p, c_ll],
     "kp_mesh_create": [P(MeshDesc), P(c_void_p)],
     "kp_mesh_create_ini": [ctypes.c_char_p, P(c_void_p)],
     "kp_mesh_destroy": [c_void_p],

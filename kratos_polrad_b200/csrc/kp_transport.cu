@@ -909,22 +909,14 @@ thread_local cudaEvent_t split_event = nullptr;
 // Solve with peel-off rays deferred: k_forward<..., DEFER> walks the packets
 // and queues their peel-off rays (marching them inline only if the queue is
 // full), then k_peel marches the queue.  The queue belongs to the mesh and
-// grows to 12 rays per packet, at most 2^27 rays (10.7 GB).
+// holds 12 rays per packet, at most the mesh's limit (default 2^27 rays,
+// 10.7 GB); larger solves run in chunks of packets (cap / 12 packets each,
+// walk then march), so the queue is sized for the chunk, not the solve.
+constexpr int PQ_PER_PACKET = 12;
+
 template< int TALLY >
-void launch_deferred( kp_mesh_t * mesh, fwd_params_t & P, cudaStream_t s )
+void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s )
 {
-    const long long want = std::min< long long >( std::max< long long >( 12 * P.n_packets, 1 << 16 ),
-                                                  1ll << 27 );
-    if( mesh->pq_cap < want )
-    {
-        cudaFree( mesh->d_pq );
-        mesh->d_pq = nullptr;
-        mesh->pq_cap = 0;
-        KP_CUDA( cudaMalloc( & mesh->d_pq, ( size_t ) want * sizeof( peel_task_t ) ) );
-        mesh->pq_cap = want;
-    }
-    P.pq = static_cast< peel_task_t * >( mesh->d_pq );
-    P.pq_cap = mesh->pq_cap;
     P.pq_count = P.work + 1;
     P.pq_next = P.work + 2;
     KP_CUDA( cudaMemsetAsync( P.work, 0, 3 * sizeof( unsigned long long ), s ) );
@@ -937,6 +929,34 @@ void launch_deferred( kp_mesh_t * mesh, fwd_params_t & P, cudaStream_t s )
     const long long gp = persistent_grid( ( const void * ) k_peel< TALLY >, 256 );
     k_peel< TALLY ><<< ( unsigned ) gp, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
+}
+
+template< int TALLY >
+void launch_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
+{
+    const long long want = std::min( std::max< long long >( PQ_PER_PACKET * P.n_packets, 1 << 16 ),
+                                     mesh->pq_limit );
+    if( mesh->pq_cap < want )
+    {
+        cudaFree( mesh->d_pq );
+        mesh->d_pq = nullptr;
+        mesh->pq_cap = 0;
+        KP_CUDA( cudaMalloc( & mesh->d_pq, ( size_t ) want * sizeof( peel_task_t ) ) );
+        mesh->pq_cap = want;
+    }
+    const long long chunk = std::max< long long >( mesh->pq_cap / PQ_PER_PACKET, 1 );
+    static thread_local fwd_params_t C;
+    for( long long done = 0; done < P.n_packets; done += chunk )
+    {
+        C = P;
+        C.pq = static_cast< peel_task_t * >( mesh->d_pq );
+        C.pq_cap = mesh->pq_cap;
+        C.pid0 = P.pid0 + done;
+        C.n_packets = std::min( chunk, P.n_packets - done );
+        C.n_record = std::max< long long >( P.n_record - done, 0 );
+        C.records = C.n_record > 0 ? P.records + done : nullptr;
+        launch_deferred_chunk< TALLY >( C, s );
+    }
 }
 }   // namespace kp
 
@@ -962,6 +982,23 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
         }
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
         if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
+    } );
+}
+
+extern "C" int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays )
+{
+    return kp::guarded( "kp_mesh_peel_queue_limit", [ & ]
+    {
+        kp::require( mesh, "null mesh" );
+        kp::require( max_rays >= 1024, "the peel-off queue limit must be at least 1024 rays",
+                     KP_ERR_CONFIG );
+        if( mesh->pq_cap > max_rays )
+        {   // the next solve allocates a queue within the new limit
+            KP_CUDA( cudaFree( mesh->d_pq ) );
+            mesh->d_pq = nullptr;
+            mesh->pq_cap = 0;
+        }
+        mesh->pq_limit = max_rays;
     } );
 }
 
