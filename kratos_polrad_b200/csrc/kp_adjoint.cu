@@ -31,25 +31,6 @@ constexpr int ADJ_KMAX = 32;
 enum ray_kind { RAY_WALK = 0, RAY_MEASURE = 1, RAY_DEPOSIT = 2 };
 
 template< int TALLY >
-__device__ __forceinline__ void add_grad( void * base, size_t i, double v, double sc )
-{
-    if( TALLY == KP_TALLY_FIXED )
-        atomicAdd( ( unsigned long long * ) base + i,
-                   ( unsigned long long ) __double2ll_rn( __dmul_rn( v, sc ) ) );
-    else
-        atomicAdd( ( float * ) base + i, ( float ) v );
-}
-
-// <dL/dimage[pix], (I, Q, U, V)>
-__device__ __forceinline__ float score( const fwd_params_t & P, int pix, float I, float Q,
-                                        float U, float V )
-{
-    const float4 g = P.adj_img[ pix ];
-    return __fadd_rn( __fadd_rn( __fadd_rn( __fmul_rn( g.x, I ), __fmul_rn( g.y, Q ) ),
-                                 __fmul_rn( g.z, U ) ), __fmul_rn( g.w, V ) );
-}
-
-template< int TALLY >
 __global__ void __launch_bounds__( FWD_THREADS, 3 )
 k_adjoint( const __grid_constant__ fwd_params_t P )
 {
@@ -70,6 +51,11 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
     bool  remeasure = false;
     double R = 0.0;
     float gk[ ADJ_KMAX ];
+    // packets of a list (the deferred adjoint's overflow), whose first
+    // replay the deferred walk has counted already
+    const unsigned long long n_items = P.adj_list ? * P.adj_list_n
+                                                  : ( unsigned long long ) P.n_packets;
+    auto counting = [ & ](  ) { return pass == 1 || ! P.adj_quiet; };
 
     // Starts pass 1 of the lane's packet (same id, RNG from its start).
     auto begin_pass1 = [ & ](  )
@@ -157,10 +143,13 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         }
         if( left || p.n_steps >= P.max_steps )
         {
-            if( left )
-                count( sp, lost ? KP_CNT_LOST : KP_CNT_ESCAPED );
-            else
-                count( sp, KP_CNT_CAPPED );
+            if( counting(  ) )
+            {
+                if( left )
+                    count( sp, lost ? KP_CNT_LOST : KP_CNT_ESCAPED );
+                else
+                    count( sp, KP_CNT_CAPPED );
+            }
             end_packet(  );
         }
     };
@@ -196,7 +185,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             if( ! left )
             {
                 faces_all( P.m, p.b, p.c, p.d, fx );
-                if( p.b != b_old ) count( sp, KP_CNT_HOPS );
+                if( p.b != b_old && counting(  ) ) count( sp, KP_CNT_HOPS );
             }
             phase = PH_SEGMENT;
             after_crossing( false, left, lost );
@@ -213,18 +202,19 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                 base = atomicAdd( P.work, ( unsigned long long ) n_emit );
             base = __shfl_sync( m_emit, base, leader );
             const unsigned long long idx = base + rank;
-            if( idx >= ( unsigned long long ) P.n_packets )
+            if( idx >= n_items )
             {
                 phase = PH_DONE;
                 continue;
             }
-            if( ! emit_packet( P, P.pid0 + ( long long ) idx, p,
-                               P.src[ ( P.pid0 + ( long long ) idx ) % P.n_src ], P.stream ) )
+            const long long pid = P.pid0 + ( P.adj_list ? ( long long ) P.adj_list[ idx ]
+                                                        : ( long long ) idx );
+            if( ! emit_packet( P, pid, p, P.src[ pid % P.n_src ], P.stream ) )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
                 continue;
             }
-            count( sp, KP_CNT_EMITTED );
+            if( ! P.adj_quiet ) count( sp, KP_CNT_EMITTED );
             p.tau = sample_tau( p.rng );
             store_cold( sc, p );
             pass = 0; nv = 0; R = 0.0; G0 = 0.f;
@@ -254,7 +244,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             if( phase != PH_EVENT ) continue;
             load_cold( sc, p, P.seed );
             ++ p.n_scat;
-            count( sp, KP_CNT_SCATTER );
+            if( counting(  ) ) count( sp, KP_CNT_SCATTER );
             const size_t ci = cell_index( P.m, p.b, p.c );
             {
                 const float2 sg = P.m.sigma[ ci ];
@@ -349,7 +339,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         }
         else
         {
-            ++ cnt.steps;
+            if( counting(  ) ) ++ cnt.steps;
             ++ p.n_steps;
             interact = et >= p.tau;
         }
@@ -392,6 +382,308 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );
 }
 
+// Deferred adjoint, the walks.  PASS 0 walks every packet of the launch and
+// queues the peel-off ray of each vertex (the emission of an isotropic point
+// source and every interaction, when its point projects into the image) as
+// a task, linked in vertex order per packet; a packet whose ray finds the
+// queue full is flagged and listed for k_adjoint.  k_peel (mode 1) then
+// measures each ray's score G, k_adj_fold sums them per packet.  PASS 1
+// replays the walks with R, the sum of the scores of the interactions still
+// ahead (adj_R0 at the start, minus each vertex's G after it), and deposits
+// -R * length along the walk and R / sigma_sca at interactions; k_peel
+// (mode 2) deposits along the rays.  Per packet this is k_adjoint's
+// arithmetic in k_adjoint's order, so the int64 gradients are the same.
+template< int TALLY, int PASS >
+__global__ void __launch_bounds__( FWD_THREADS, 3 )
+k_adj_walk( const __grid_constant__ fwd_params_t P )
+{
+    struct cnt_park_t { unsigned long long cnt[ KP_NCOUNTERS ]; };
+    __shared__ cnt_park_t sp;
+    __shared__ cold_park_t< FWD_THREADS > sc;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    if( threadIdx.x < KP_NCOUNTERS ) sp.cnt[ threadIdx.x ] = 0;
+    __syncthreads(  );
+    counts32_t cnt;
+    packet_t p;
+    double fx[ 3 ];
+    int phase = PH_EMIT, hop_ax = 0;
+    int lp = 0;        // the packet's index in the launch
+    int link = -1;     // PASS 0: its last task (-1 none, -2 the queue overflowed);
+                       // PASS 1: its next task
+    double R = 0.0;    // PASS 1
+
+    // PASS 0: queues the ray of vertex kv (toward the observer, weight w,
+    // Stokes I, Q, U, V), the lanes together with one atomic.
+    auto queue_ray = [ & ]( int pix, float w, float I, float Q, float U, float V, int kv )
+    {
+        const unsigned m = __activemask(  );
+        const int leader = __ffs( m ) - 1;
+        unsigned long long base = 0;
+        if( ( int ) lane == leader )
+            base = atomicAdd( P.pq_count, ( unsigned long long ) __popc( m ) );
+        base = __shfl_sync( m, base, leader );
+        const unsigned long long k = base + __popc( m & ( ( 1u << lane ) - 1u ) );
+        if( k >= ( unsigned long long ) P.pq_cap )
+        {   // the whole packet goes to k_adjoint
+            link = -2;
+            P.adj_flag[ lp ] = 1;
+            P.adj_list[ atomicAdd( P.adj_list_n, 1ull ) ] = lp;
+            return;
+        }
+        peel_task_t & o = P.pq[ k ];
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+        o.b = p.b;
+        o.w = w; o.I = I; o.Q = Q; o.U = U; o.V = V;
+        o.pix = pix; o.cpix = -1; o.lp = lp; o.kv = kv;
+        if( link >= 0 ) P.pq[ link ].cpix = ( int ) k;
+        else P.adj_head[ lp ] = ( int ) k;
+        link = ( int ) k;
+    };
+
+    for( ;; )
+    {
+        const unsigned m_emit = __ballot_sync( FULL, phase == PH_EMIT );
+        const unsigned m_seg  = __ballot_sync( FULL, phase == PH_SEGMENT );
+        const unsigned m_ev   = __ballot_sync( FULL, phase == PH_EVENT );
+        const unsigned m_hop  = __ballot_sync( FULL, phase == PH_HOP );
+        if( ( m_emit | m_seg | m_ev | m_hop ) == 0u )
+            break;
+        const int n_seg = __popc( m_seg ), n_ev = __popc( m_ev ), n_emit = __popc( m_emit );
+        const int n_hop = __popc( m_hop );
+        int run;
+        if( n_ev > 0 && ( n_ev >= P.ev_batch || n_seg == 0 ) )
+            run = PH_EVENT;
+        else if( n_emit > 0 && ( n_emit >= P.ev_batch || n_seg == 0 ) )
+            run = PH_EMIT;
+        else if( n_hop > 0 && ( n_hop >= P.hop_batch || n_seg == 0 ) )
+            run = PH_HOP;
+        else
+            run = PH_SEGMENT;
+
+        if( run == PH_HOP )
+        {
+            if( phase != PH_HOP ) continue;
+            const int b_old = p.b;
+            bool lost;
+            const bool left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax,
+                                            comp( p.d, hop_ax ) > 0.0f, lost );
+            if( left )
+            {
+                count( sp, lost ? KP_CNT_LOST : KP_CNT_ESCAPED );
+                phase = PH_EMIT;
+                continue;
+            }
+            faces_all( P.m, p.b, p.c, p.d, fx );
+            if( p.b != b_old ) count( sp, KP_CNT_HOPS );
+            if( p.n_steps >= P.max_steps )
+            {
+                count( sp, KP_CNT_CAPPED );
+                phase = PH_EMIT;
+            }
+            else
+                phase = PH_SEGMENT;
+            continue;
+        }
+
+        if( run == PH_EMIT )
+        {
+            if( phase != PH_EMIT ) continue;
+            const int leader = __ffs( m_emit ) - 1;
+            const unsigned rank = __popc( m_emit & ( ( 1u << lane ) - 1u ) );
+            unsigned long long base = 0;
+            if( ( int ) lane == leader )
+                base = atomicAdd( P.work, ( unsigned long long ) n_emit );
+            base = __shfl_sync( m_emit, base, leader );
+            const unsigned long long idx = base + rank;
+            if( idx >= ( unsigned long long ) P.n_packets )
+            {
+                phase = PH_DONE;
+                continue;
+            }
+            lp = ( int ) idx;
+            if constexpr( PASS == 1 )
+                if( P.adj_flag[ lp ] )
+                    continue;                     // replayed by k_adjoint
+            const long long pid = P.pid0 + ( long long ) idx;
+            const src_dev_t & s = P.src[ pid % P.n_src ];
+            if( ! emit_packet( P, pid, p, s, P.stream ) )
+            {
+                atomicOr( P.m.status, ST_BAD_SOURCE );
+                continue;
+            }
+            if constexpr( PASS == 0 )
+            {
+                count( sp, KP_CNT_EMITTED );
+                link = -1;
+            }
+            else
+            {
+                link = P.adj_head[ lp ];
+                R = P.adj_R0[ lp ];
+            }
+            p.tau = sample_tau( p.rng );
+            store_cold( sc, p );
+            if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
+            {   // direct light of an isotropic, unpolarized point source
+                const int pix = image_pixel( P, p.x );
+                if( pix >= 0 )
+                {
+                    if constexpr( PASS == 0 )
+                        queue_ray( pix, 1.0f, 0x1.45f306p-4f, 0.0f, 0.0f, 0.0f, 0 );
+                    else if( link >= 0 )
+                        link = P.pq[ link ].cpix;     // its ray is deposited by k_peel
+                }
+            }
+            faces_all( P.m, p.b, p.c, p.d, fx );
+            phase = PH_SEGMENT;
+            continue;
+        }
+
+        if( run == PH_EVENT )
+        {
+            if( phase != PH_EVENT ) continue;
+            load_cold( sc, p, P.seed );
+            ++ p.n_scat;
+            count( sp, KP_CNT_SCATTER );
+            const size_t ci = cell_index( P.m, p.b, p.c );
+            {
+                const float2 sg = P.m.sigma[ ci ];
+                p.w = __fmul_rn( p.w, __fdiv_rn( sg.x, __fadd_rn( sg.x, sg.y ) ) );
+                if constexpr( PASS == 1 )
+                    if( R != 0.0 )
+                        add_grad< TALLY >( P.g_int, ci, __ddiv_rn( R, ( double ) sg.x ), P.g_scale );
+            }
+            if( P.img_n > 0 )
+            {
+                const int pix = image_pixel( P, p.x );
+                if( pix >= 0 )
+                {
+                    if constexpr( PASS == 0 )
+                    {
+                        if( link != -2 )
+                        {
+                            float Q, U, V;
+                            const float I = phys::peel_stokes( P.ph, p.d, p.e1, p.S, P.o, P.ev,
+                                                               P.eh, Q, U, V );
+                            queue_ray( pix, p.w, I, Q, U, V, p.n_scat );
+                        }
+                    }
+                    else if( link >= 0 )
+                    {   // this vertex's score leaves R once its ray is deposited
+                        const float G = P.adj_G[ link ];
+                        link = P.pq[ link ].cpix;
+                        if( G != 0.0f )
+                            R = __dsub_rn( R, ( double ) G );
+                    }
+                }
+            }
+            int end = 0;
+            if( p.n_scat >= P.max_scatter )
+                end = PK_SCATTER_CAP;
+            else if( p.w < P.w_min )
+            {   // Russian roulette
+                const phys::u4 r = p.rng.next(  );
+                if( phys::u01( r.x ) < P.rr_survive )
+                    p.w = __fdiv_rn( p.w, P.rr_survive );
+                else
+                    end = PK_ABSORBED;
+            }
+            if( ! end )
+            {
+                phys::scatter( P.ph, p.rng, p.d, p.e1, p.S );
+                set_inv( p );
+                p.tau = sample_tau( p.rng );
+            }
+            if( ! end && p.n_steps >= P.max_steps )
+                end = PK_STEP_CAP;
+            if( end )
+                phase = PH_EMIT;
+            else
+            {
+                store_cold( sc, p );
+                faces_all( P.m, p.b, p.c, p.d, fx );
+                phase = PH_SEGMENT;
+            }
+            continue;
+        }
+
+        // ---- PH_SEGMENT: walk segments, up to KP_WALK_INNER per round ----
+        if( phase != PH_SEGMENT ) continue;
+        #pragma unroll 1
+        for( int it = 0; it < KP_WALK_INNER; ++ it )
+        {
+            const size_t ci = cell_index( P.m, p.b, p.c );
+            const float2 sg = P.m.sigma[ ci ];
+            const float ext = __fadd_rn( sg.x, sg.y );
+            int ax;
+            const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
+            const float et = __fmul_rn( ext, ( float ) t );
+            ++ cnt.steps;
+            ++ p.n_steps;
+            if( et >= p.tau )
+            {
+                double ti = ( double ) __fdiv_rn( p.tau, ext );
+                ti = ti > t ? t : ti;
+                if constexpr( PASS == 1 )
+                    if( R != 0.0 )
+                        add_grad< TALLY >( P.g_len, ci, __dmul_rn( -R, ti ), P.g_scale );
+                p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
+                p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
+                p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
+                phase = PH_EVENT;
+                break;
+            }
+            p.tau = __fsub_rn( p.tau, et );
+            if constexpr( PASS == 1 )
+                if( R != 0.0 )
+                    add_grad< TALLY >( P.g_len, ci, __dmul_rn( -R, t ), P.g_scale );
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a )
+                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
+            if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
+            {   // leaves the block: wait for a batched hand-off
+                hop_ax = ax;
+                phase = PH_HOP;
+                break;
+            }
+            if( p.n_steps >= P.max_steps )
+            {
+                count( sp, KP_CNT_CAPPED );
+                phase = PH_EMIT;
+                break;
+            }
+        }
+    }
+    count_all( sp, KP_CNT_STEPS, cnt.steps );
+    __syncthreads(  );
+    if( P.counters && threadIdx.x < KP_NCOUNTERS && sp.cnt[ threadIdx.x ] )
+        atomicAdd( P.counters + threadIdx.x, sp.cnt[ threadIdx.x ] );
+}
+
+// Deferred adjoint: R of each packet, the sum of its interactions' scores in
+// vertex order (k_adjoint's first replay).  Task indices grow along a
+// packet's list, which bounds the walk through it.
+__global__ void k_adj_fold( const __grid_constant__ fwd_params_t P )
+{
+    for( long long lp = blockIdx.x * ( long long ) blockDim.x + threadIdx.x; lp < P.n_packets;
+         lp += ( long long ) gridDim.x * blockDim.x )
+    {
+        if( P.adj_flag[ lp ] ) continue;
+        double R = 0.0;
+        for( int t = P.adj_head[ lp ]; t >= 0; )
+        {
+            const peel_task_t & o = P.pq[ t ];
+            if( o.kv > 0 )
+                R = __dadd_rn( R, ( double ) P.adj_G[ t ] );
+            const int nx = o.cpix;
+            t = nx > t ? nx : -1;
+        }
+        P.adj_R0[ lp ] = R;
+    }
+}
+
 }   // namespace
 }   // namespace kp
 
@@ -425,17 +717,74 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
         P.work = mesh->workspace(  );
         if( P.n_packets == 0 ) return;
         auto s = ( cudaStream_t ) stream;
+        const bool fx = c.tally_mode == KP_TALLY_FIXED;
         const int threads = kp::FWD_THREADS;
-        const void * k = c.tally_mode == KP_TALLY_FIXED
-                       ? ( const void * ) kp::k_adjoint< KP_TALLY_FIXED >
-                       : ( const void * ) kp::k_adjoint< KP_TALLY_FLOAT >;
-        long long grid = kp::persistent_grid( k, threads );
-        grid = std::min< long long >( grid, ( P.n_packets + threads - 1 ) / threads );
-        KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
-        if( c.tally_mode == KP_TALLY_FIXED )
-            kp::k_adjoint< KP_TALLY_FIXED ><<< ( unsigned ) grid, threads, 0, s >>>( P );
-        else
-            kp::k_adjoint< KP_TALLY_FLOAT ><<< ( unsigned ) grid, threads, 0, s >>>( P );
-        KP_CUDA( cudaGetLastError(  ) );
+        // The vertices' peel-off rays go through the mesh's queue (12 rays per
+        // packet, chunks of packets beyond that) and are marched by k_peel.
+        kp::ensure_peel_queue( mesh, P.n_packets );
+        const long long cap = mesh->pq_cap;
+        const long long chunk = std::max< long long >( cap / kp::PQ_PER_PACKET, 1 );
+        const long long n_pk = std::min( chunk, P.n_packets );
+        if( mesh->adj_tasks < cap || mesh->adj_packets < n_pk )
+        {
+            cudaFree( mesh->d_adj );
+            mesh->d_adj = nullptr;
+            mesh->adj_tasks = mesh->adj_packets = 0;
+            KP_CUDA( cudaMalloc( & mesh->d_adj, ( size_t ) n_pk * ( sizeof( double ) + 3 * sizeof( int ) )
+                                                + ( size_t ) cap * sizeof( float ) ) );
+            mesh->adj_tasks = cap;
+            mesh->adj_packets = n_pk;
+        }
+        char * a = static_cast< char * >( mesh->d_adj );
+        P.adj_R0   = reinterpret_cast< double * >( a );
+        P.adj_G    = reinterpret_cast< float * >( a + n_pk * sizeof( double ) );
+        P.adj_head = reinterpret_cast< int * >( a + n_pk * sizeof( double ) + cap * sizeof( float ) );
+        P.adj_flag = P.adj_head + n_pk;
+        P.adj_list = P.adj_flag + n_pk;
+        P.pq = static_cast< kp::peel_task_t * >( mesh->d_pq );
+        P.pq_cap = cap;
+        P.pq_count = P.work + 1;
+        P.pq_next = P.work + 2;
+        P.adj_list_n = P.work + 3;
+        const void * kw0 = fx ? ( const void * ) kp::k_adj_walk< KP_TALLY_FIXED, 0 >
+                              : ( const void * ) kp::k_adj_walk< KP_TALLY_FLOAT, 0 >;
+        const void * ka = fx ? ( const void * ) kp::k_adjoint< KP_TALLY_FIXED >
+                             : ( const void * ) kp::k_adjoint< KP_TALLY_FLOAT >;
+        const long long grid_w = kp::persistent_grid( kw0, threads );
+        const long long grid_a = kp::persistent_grid( ka, threads );
+        static thread_local kp::fwd_params_t C;
+        for( long long done = 0; done < P.n_packets; done += chunk )
+        {
+            C = P;
+            C.pid0 = P.pid0 + done;
+            C.n_packets = std::min( chunk, P.n_packets - done );
+            const unsigned gw = ( unsigned ) std::min< long long >( grid_w,
+                                                                   ( C.n_packets + threads - 1 ) / threads );
+            KP_CUDA( cudaMemsetAsync( P.work, 0, 4 * sizeof( unsigned long long ), s ) );
+            KP_CUDA( cudaMemsetAsync( C.adj_head, 0xff, C.n_packets * sizeof( int ), s ) );
+            KP_CUDA( cudaMemsetAsync( C.adj_flag, 0, C.n_packets * sizeof( int ), s ) );
+            // first replay: walks, vertex rays queued
+            if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 0 ><<< gw, threads, 0, s >>>( C );
+            else     kp::k_adj_walk< KP_TALLY_FLOAT, 0 ><<< gw, threads, 0, s >>>( C );
+            KP_CUDA( cudaGetLastError(  ) );
+            kp::launch_peel_adjoint( C, c.tally_mode, 1, s );          // scores G
+            const unsigned gf = ( unsigned ) std::min< long long >( 4096, ( C.n_packets + 255 ) / 256 );
+            kp::k_adj_fold<<< gf, 256, 0, s >>>( C );                   // R per packet
+            KP_CUDA( cudaGetLastError(  ) );
+            // second replay: deposits along the walks, then along the rays
+            KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
+            if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 1 ><<< gw, threads, 0, s >>>( C );
+            else     kp::k_adj_walk< KP_TALLY_FLOAT, 1 ><<< gw, threads, 0, s >>>( C );
+            KP_CUDA( cudaGetLastError(  ) );
+            kp::launch_peel_adjoint( C, c.tally_mode, 2, s );
+            // packets whose rays found the queue full: both replays inline
+            KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
+            C.adj_quiet = 1;
+            const unsigned ga = ( unsigned ) std::min< long long >( grid_a,
+                                                                   ( C.n_packets + threads - 1 ) / threads );
+            if( fx ) kp::k_adjoint< KP_TALLY_FIXED ><<< ga, threads, 0, s >>>( C );
+            else     kp::k_adjoint< KP_TALLY_FLOAT ><<< ga, threads, 0, s >>>( C );
+            KP_CUDA( cudaGetLastError(  ) );
+        }
     } );
 }

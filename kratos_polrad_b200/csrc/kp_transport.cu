@@ -44,9 +44,6 @@ namespace cg = cooperative_groups;
 #ifndef KP_PEEL_MINB
 #define KP_PEEL_MINB 4               // k_peel: resident blocks of 256 the registers allow
 #endif
-#ifndef KP_WALK_INNER
-#define KP_WALK_INNER 2              // k_forward<DEFER>: segments per scheduling round
-#endif
 #ifndef KP_FWD_RESIDENT
 #define KP_FWD_RESIDENT 768          // resident threads per SM the register budget targets
 #endif
@@ -583,8 +580,14 @@ k_forward( const __grid_constant__ fwd_params_t P )
 // lane, and a lane holds only the ray's position, faces, cell, optical depth
 // and its block's origin and spacing (the next face is computed from them,
 // with exit_dist's expression, without a load).
-template< int TALLY >
-__global__ void __launch_bounds__( 256, KP_PEEL_MINB )
+// MODE 0 deposits each ray into the image (forward solve).  The deferred
+// adjoint marches the same tasks twice: MODE 1 measures each ray's score G
+// (what the image deposit would be worth to the loss) into adj_G, MODE 2
+// deposits -G * length into the path-length gradient along each segment
+// inside the depth cut; both skip the tasks of packets left to k_adjoint,
+// and MODE 2 the rays with G = 0.
+template< int TALLY, int MODE >
+__global__ void __launch_bounds__( 256, MODE == 2 ? 3 : KP_PEEL_MINB )
 k_peel( const __grid_constant__ fwd_params_t P )
 {
     __shared__ unsigned long long cnt_s[ KP_NCOUNTERS ];
@@ -599,6 +602,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
     int    c[ 3 ] = { 0, 0, 0 }, b = 0, hop_ax = 0, pk = 0, ci = 0;
     const float2 * sb = P.m.sigma;                // this block's coefficients
     float  ptau = 0.0f;
+    float  pG = 0.0f;                             // MODE 2: the ray's score
     long long task = -1;
     unsigned n_seg_done = 0;
     int phase = PH_EMIT;
@@ -637,17 +641,34 @@ k_peel( const __grid_constant__ fwd_params_t P )
         {
             if( phase != PH_EMIT ) continue;
             const int leader = __ffs( m_fetch ) - 1;
-            const bool dep = task >= 0 && ptau <= P.tau_cut;
-            if( dep )
-            {   // deposit of the ray that just ended (after_crossing's)
-                const peel_task_t & o = P.pq[ task ];
-                const float att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
-                deposit_pixel< TALLY >( P, o.pix, o.cpix, __fmul_rn( att, o.I ), __fmul_rn( att, o.Q ),
-                                        __fmul_rn( att, o.U ), __fmul_rn( att, o.V ) );
+            if constexpr( MODE == 0 )
+            {
+                const bool dep = task >= 0 && ptau <= P.tau_cut;
+                if( dep )
+                {   // deposit of the ray that just ended (after_crossing's)
+                    const peel_task_t & o = P.pq[ task ];
+                    const float att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    deposit_pixel< TALLY >( P, o.pix, o.cpix, __fmul_rn( att, o.I ),
+                                            __fmul_rn( att, o.Q ), __fmul_rn( att, o.U ),
+                                            __fmul_rn( att, o.V ) );
+                }
+                const unsigned m_dep = __ballot_sync( m_fetch, dep );
+                if( ( int ) lane == leader && m_dep )
+                    atomicAdd( cnt_s + KP_CNT_DEPOSITS, ( unsigned long long ) __popc( m_dep ) );
             }
-            const unsigned m_dep = __ballot_sync( m_fetch, dep );
-            if( ( int ) lane == leader && m_dep )
-                atomicAdd( cnt_s + KP_CNT_DEPOSITS, ( unsigned long long ) __popc( m_dep ) );
+            if constexpr( MODE == 1 )
+                if( task >= 0 )
+                {   // score of the ray that just ended (k_adjoint's measure ray)
+                    const peel_task_t & o = P.pq[ task ];
+                    float G = 0.0f;
+                    if( ptau <= P.tau_cut )
+                    {
+                        const float att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                        G = score( P, o.pix, __fmul_rn( att, o.I ), __fmul_rn( att, o.Q ),
+                                   __fmul_rn( att, o.U ), __fmul_rn( att, o.V ) );
+                    }
+                    P.adj_G[ task ] = G;
+                }
             task = -1;
             const unsigned rank = __popc( m_fetch & ( ( 1u << lane ) - 1u ) );
             unsigned long long base = 0;
@@ -661,6 +682,17 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             const peel_task_t & o = P.pq[ idx ];
+            if constexpr( MODE != 0 )
+            {   // rays of packets left to k_adjoint, and rays worth nothing
+                if( P.adj_flag[ o.lp ] )
+                    continue;
+                if constexpr( MODE == 2 )
+                {
+                    pG = P.adj_G[ idx ];
+                    if( pG == 0.0f )
+                        continue;
+                }
+            }
             #pragma unroll
             for( int a = 0; a < 3; ++ a ) { x[ a ] = o.x[ a ]; c[ a ] = o.c[ a ]; }
             b = o.b;
@@ -706,6 +738,9 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 phase = PH_EMIT;
                 break;
             }
+            if constexpr( MODE == 2 )
+                add_grad< TALLY >( P.g_len, ( size_t ) ( sb - P.m.sigma ) + ci,
+                                   __dmul_rn( -( double ) pG, t ), P.g_scale );
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
                 if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
@@ -912,7 +947,22 @@ thread_local cudaEvent_t split_event = nullptr;
 // holds 12 rays per packet, at most the mesh's limit (default 2^27 rays,
 // 10.7 GB); larger solves run in chunks of packets (cap / 12 packets each,
 // walk then march), so the queue is sized for the chunk, not the solve.
-constexpr int PQ_PER_PACKET = 12;
+
+// Grows the mesh's peel-off queue to 12 rays per packet of a solve of
+// n_packets (at least 2^16 rays, at most the mesh's limit).
+void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets )
+{
+    const long long want = std::min( std::max< long long >( PQ_PER_PACKET * n_packets, 1 << 16 ),
+                                     mesh->pq_limit );
+    if( mesh->pq_cap < want )
+    {
+        cudaFree( mesh->d_pq );
+        mesh->d_pq = nullptr;
+        mesh->pq_cap = 0;
+        KP_CUDA( cudaMalloc( & mesh->d_pq, ( size_t ) want * sizeof( peel_task_t ) ) );
+        mesh->pq_cap = want;
+    }
+}
 
 template< int TALLY >
 void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s )
@@ -926,24 +976,39 @@ void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s )
     k_forward< TALLY, 256, false, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
     if( split_event ) KP_CUDA( cudaEventRecord( split_event, s ) );
-    const long long gp = persistent_grid( ( const void * ) k_peel< TALLY >, 256 );
-    k_peel< TALLY ><<< ( unsigned ) gp, 256, 0, s >>>( P );
+    const long long gp = persistent_grid( ( const void * ) k_peel< TALLY, 0 >, 256 );
+    k_peel< TALLY, 0 ><<< ( unsigned ) gp, 256, 0, s >>>( P );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+
+// The deferred adjoint's marches of the queued vertex rays: mode 1 measures
+// their scores, mode 2 deposits along them (k_peel).
+void launch_peel_adjoint( const fwd_params_t & P, int tally_mode, int mode, cudaStream_t s )
+{
+    KP_CUDA( cudaMemsetAsync( P.pq_next, 0, sizeof( unsigned long long ), s ) );
+    const bool fx = tally_mode == KP_TALLY_FIXED;
+    const void * k = mode == 1 ? ( fx ? ( const void * ) k_peel< KP_TALLY_FIXED, 1 >
+                                      : ( const void * ) k_peel< KP_TALLY_FLOAT, 1 > )
+                               : ( fx ? ( const void * ) k_peel< KP_TALLY_FIXED, 2 >
+                                      : ( const void * ) k_peel< KP_TALLY_FLOAT, 2 > );
+    const unsigned gp = ( unsigned ) persistent_grid( k, 256 );
+    if( mode == 1 )
+    {
+        if( fx ) k_peel< KP_TALLY_FIXED, 1 ><<< gp, 256, 0, s >>>( P );
+        else     k_peel< KP_TALLY_FLOAT, 1 ><<< gp, 256, 0, s >>>( P );
+    }
+    else
+    {
+        if( fx ) k_peel< KP_TALLY_FIXED, 2 ><<< gp, 256, 0, s >>>( P );
+        else     k_peel< KP_TALLY_FLOAT, 2 ><<< gp, 256, 0, s >>>( P );
+    }
     KP_CUDA( cudaGetLastError(  ) );
 }
 
 template< int TALLY >
 void launch_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
 {
-    const long long want = std::min( std::max< long long >( PQ_PER_PACKET * P.n_packets, 1 << 16 ),
-                                     mesh->pq_limit );
-    if( mesh->pq_cap < want )
-    {
-        cudaFree( mesh->d_pq );
-        mesh->d_pq = nullptr;
-        mesh->pq_cap = 0;
-        KP_CUDA( cudaMalloc( & mesh->d_pq, ( size_t ) want * sizeof( peel_task_t ) ) );
-        mesh->pq_cap = want;
-    }
+    ensure_peel_queue( mesh, P.n_packets );
     const long long chunk = std::max< long long >( mesh->pq_cap / PQ_PER_PACKET, 1 );
     static thread_local fwd_params_t C;
     for( long long done = 0; done < P.n_packets; done += chunk )
@@ -997,6 +1062,9 @@ extern "C" int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays )
             KP_CUDA( cudaFree( mesh->d_pq ) );
             mesh->d_pq = nullptr;
             mesh->pq_cap = 0;
+            KP_CUDA( cudaFree( mesh->d_adj ) );
+            mesh->d_adj = nullptr;
+            mesh->adj_tasks = mesh->adj_packets = 0;
         }
         mesh->pq_limit = max_rays;
     } );

@@ -39,6 +39,12 @@ struct scene_dev_t
     uint32_t  pad;
 };
 
+// Walk segments per scheduling round in the kernels whose peel-off rays are
+// marched by k_peel (k_forward<DEFER>, k_adj_walk).
+#ifndef KP_WALK_INNER
+#define KP_WALK_INNER 2
+#endif
+
 // Everything a transport launch reads, passed by value.
 struct fwd_params_t
 {
@@ -102,18 +108,30 @@ struct fwd_params_t
     unsigned long long * pq_count;      // tasks written (may exceed pq_cap: those ran inline)
     unsigned long long * pq_next;       // k_peel's task counter
     long long   pq_cap;
+    // deferred adjoint (kp_transport_adjoint): the tasks are the vertices'
+    // peel-off rays, linked in vertex order per packet of the launch
+    float     * adj_G;                  // [pq_cap] G of each task's ray
+    int       * adj_head;               // [n_packets] first task of the packet, -1: none
+    double    * adj_R0;                 // [n_packets] sum of G over its interactions
+    int       * adj_flag;               // [n_packets] 1: the queue overflowed for it
+    int       * adj_list;               // [n_packets] packets handed to k_adjoint
+    unsigned long long * adj_list_n;    //   ... and their count
+    int         adj_quiet;              // k_adjoint: its first replay counts nothing
     src_dev_t   src[ MAX_SOURCES ];
 };
 
 // A peel-off ray waiting for k_peel: where it starts (the interaction or
-// emission point) and its pending contribution.
+// emission point) and its pending contribution.  In the deferred adjoint
+// `cpix` holds the packet's next task (-1: last), `lp` the packet's index in
+// the launch and `kv` the vertex (0: emission).
 struct __align__( 16 ) peel_task_t
 {
     double x[ 3 ];
     int    b, c[ 3 ];
     float  w, I, Q, U, V;
     int    pix, cpix;
-    int    pad[ 3 ];
+    int    lp, kv;
+    int    pad;
 };
 
 // A packet's walk crossing into a block of another rank (it has entered the
@@ -520,6 +538,26 @@ __device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel
     add_tally< TALLY >( P.img_batch, bp + 3, V, P.fx_scale );
 }
 
+// Adjoint gradient deposit (int64 fixed point or float atomics).
+template< int TALLY >
+__device__ __forceinline__ void add_grad( void * base, size_t i, double v, double sc )
+{
+    if( TALLY == KP_TALLY_FIXED )
+        atomicAdd( ( unsigned long long * ) base + i,
+                   ( unsigned long long ) __double2ll_rn( __dmul_rn( v, sc ) ) );
+    else
+        atomicAdd( ( float * ) base + i, ( float ) v );
+}
+
+// Adjoint score of a peel-off contribution: <dL/dimage[pix], (I, Q, U, V)>.
+__device__ __forceinline__ float score( const fwd_params_t & P, int pix, float I, float Q,
+                                        float U, float V )
+{
+    const float4 g = P.adj_img[ pix ];
+    return __fadd_rn( __fadd_rn( __fadd_rn( __fmul_rn( g.x, I ), __fmul_rn( g.y, Q ) ),
+                                 __fmul_rn( g.z, U ) ), __fmul_rn( g.w, V ) );
+}
+
 // Escape tally: mu = d.z bins, Stokes in the meridian frame (Q > 0 in the
 // plane of d and +z).
 template< int TALLY >
@@ -702,6 +740,9 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
                          fwd_params_t & P );
 void make_source( kp_mesh_t * mesh, const kp_source_t & s, src_dev_t & d );
 int  persistent_grid( const void * kernel, int threads );
+void launch_peel_adjoint( const fwd_params_t & P, int tally_mode, int mode, cudaStream_t s );
+constexpr int PQ_PER_PACKET = 12;    // peel-off queue rays per packet of a solve
+void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets );
 void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int threads,
                      int grid_pct );
 
