@@ -410,8 +410,13 @@ int kp_batch_autotune( kp_batch_t * batch, const kp_transport_cfg_t * cfg, doubl
  * (cfg->tally_mode KP_TALLY_FIXED) or float, per cell:
  *     grad_len  the path-length term, grad_int  the interaction term, so
  *     dL/dsigma_sca = grad_len + grad_int,  dL/dsigma_abs = grad_len.
- * Each packet is replayed twice from its RNG counter; no path is stored.
- * counters (optional) receives the KP_CNT_* counts of both replays. */
+ * Each packet is replayed twice from its RNG counter.  Between the two
+ * replays the peel-off rays of its vertices (start point, weight and Stokes
+ * vector toward the observer) wait in the mesh's peel-off queue, where two
+ * marches measure their scores and deposit along them; packets whose rays
+ * do not fit the queue (kp_mesh_peel_queue_limit) are replayed with their
+ * rays inline, with the same results.  counters (optional) receives the
+ * KP_CNT_* counts of both replays. */
 int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const float * adj_image, int grad_fx_shift,
                           void * grad_len, void * grad_int,

@@ -11,12 +11,17 @@
 // where n_k(c) counts interactions in cell c among vertices 1..k, L_k(c) is
 // the walk's path length in c up to vertex k and L_obs,k(c) the peel-off
 // ray's.  With G_k = <dL/dimage[pixel_k], C_k>, the gradient is
-// sum_k G_k d ln f_k.  Every packet is replayed twice from its RNG counter
-// (no path is stored): pass 0 computes each G_k (kept in a 32-entry per-lane
-// array; later vertices are re-measured in pass 1) and R = sum_{k>=1} G_k;
-// pass 1 deposits -R * length along walk segments (R the suffix sum of the
-// vertices still ahead), +R / sigma_sca at interactions, and -G_k * length
-// along each peel-off ray, subtracting G_k from R after vertex k.
+// sum_k G_k d ln f_k.  Every packet is replayed twice from its RNG counter:
+// pass 0 computes each G_k and R = sum_{k>=1} G_k; pass 1 deposits
+// -R * length along walk segments (R the suffix sum of the vertices still
+// ahead), +R / sigma_sca at interactions, and -G_k * length along each
+// peel-off ray, subtracting G_k from R after vertex k.
+// kp_transport_adjoint runs this in five launches per chunk of packets
+// (k_adj_walk pass 0, k_peel measuring, k_adj_fold, k_adj_walk pass 1,
+// k_peel depositing), the vertices' rays queued between them; k_adjoint
+// does both passes in one launch with the rays inline (G_k kept in a
+// 32-entry per-lane array, later vertices re-measured in pass 1) and takes
+// the packets whose rays did not fit the queue.
 // Outputs: g_len (length term, shared by both coefficients) and g_int
 // (interaction term, scattering only):
 //     dL/dsigma_sca = g_len + g_int,  dL/dsigma_abs = g_len.
