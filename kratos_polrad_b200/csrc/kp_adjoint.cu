@@ -32,6 +32,11 @@ namespace kp
 namespace
 {
 
+// Private copies of the path-length tally for the depositing march.
+#ifndef KP_ADJ_PRIV
+#define KP_ADJ_PRIV 8
+#endif
+
 constexpr int ADJ_KMAX = 32;
 enum ray_kind { RAY_WALK = 0, RAY_MEASURE = 1, RAY_DEPOSIT = 2 };
 
@@ -689,6 +694,32 @@ __global__ void k_adj_fold( const __grid_constant__ fwd_params_t P )
     }
 }
 
+// Deferred adjoint: adds the private path-length tallies of the depositing
+// march into grad_len (integer sums: the same result in any order).
+template< int TALLY >
+__global__ void k_adj_reduce( const __grid_constant__ fwd_params_t P )
+{
+    const long long n = ( long long ) P.m.n_blocks * P.m.cpb;
+    for( long long i = blockIdx.x * ( long long ) blockDim.x + threadIdx.x; i < n;
+         i += ( long long ) gridDim.x * blockDim.x )
+    {
+        if constexpr( TALLY == KP_TALLY_FIXED )
+        {
+            const unsigned long long * q = static_cast< const unsigned long long * >( P.adj_priv );
+            unsigned long long v = 0;
+            for( int k = 0; k < P.adj_npriv; ++ k ) v += q[ k * n + i ];
+            if( v ) static_cast< unsigned long long * >( P.g_len )[ i ] += v;
+        }
+        else
+        {
+            const float * q = static_cast< const float * >( P.adj_priv );
+            float v = 0.0f;
+            for( int k = 0; k < P.adj_npriv; ++ k ) v = __fadd_rn( v, q[ k * n + i ] );
+            if( v != 0.0f ) static_cast< float * >( P.g_len )[ i ] += v;
+        }
+    }
+}
+
 }   // namespace
 }   // namespace kp
 
@@ -730,15 +761,19 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
         const long long cap = mesh->pq_cap;
         const long long chunk = std::max< long long >( cap / kp::PQ_PER_PACKET, 1 );
         const long long n_pk = std::min( chunk, P.n_packets );
-        if( mesh->adj_tasks < cap || mesh->adj_packets < n_pk )
+        const long long n_cells = ( long long ) P.m.n_blocks * P.m.cpb;
+        const int n_priv = KP_ADJ_PRIV;
+        const size_t priv_bytes = n_priv > 1 ? ( size_t ) n_priv * n_cells * 8 : 0;
+        // per-packet and per-task arrays, then the private tallies (256-byte aligned)
+        const size_t adj_bytes = ( ( size_t ) n_pk * ( sizeof( double ) + 3 * sizeof( int ) )
+                                   + ( size_t ) cap * sizeof( float ) + 255 ) & ~( size_t ) 255;
+        if( mesh->adj_bytes < adj_bytes + priv_bytes )
         {
             cudaFree( mesh->d_adj );
             mesh->d_adj = nullptr;
-            mesh->adj_tasks = mesh->adj_packets = 0;
-            KP_CUDA( cudaMalloc( & mesh->d_adj, ( size_t ) n_pk * ( sizeof( double ) + 3 * sizeof( int ) )
-                                                + ( size_t ) cap * sizeof( float ) ) );
-            mesh->adj_tasks = cap;
-            mesh->adj_packets = n_pk;
+            mesh->adj_bytes = 0;
+            KP_CUDA( cudaMalloc( & mesh->d_adj, adj_bytes + priv_bytes ) );
+            mesh->adj_bytes = adj_bytes + priv_bytes;
         }
         char * a = static_cast< char * >( mesh->d_adj );
         P.adj_R0   = reinterpret_cast< double * >( a );
@@ -746,6 +781,11 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
         P.adj_head = reinterpret_cast< int * >( a + n_pk * sizeof( double ) + cap * sizeof( float ) );
         P.adj_flag = P.adj_head + n_pk;
         P.adj_list = P.adj_flag + n_pk;
+        if( n_priv > 1 )
+        {
+            P.adj_priv = a + adj_bytes;
+            P.adj_npriv = n_priv;
+        }
         P.pq = static_cast< kp::peel_task_t * >( mesh->d_pq );
         P.pq_cap = cap;
         P.pq_count = P.work + 1;
@@ -781,7 +821,17 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
             if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 1 ><<< gw, threads, 0, s >>>( C );
             else     kp::k_adj_walk< KP_TALLY_FLOAT, 1 ><<< gw, threads, 0, s >>>( C );
             KP_CUDA( cudaGetLastError(  ) );
+            if( n_priv > 1 )
+                KP_CUDA( cudaMemsetAsync( C.adj_priv, 0, ( size_t ) n_priv * n_cells
+                                          * ( fx ? 8 : 4 ), s ) );
             kp::launch_peel_adjoint( C, c.tally_mode, 2, s );
+            if( n_priv > 1 )
+            {
+                const unsigned gr = ( unsigned ) std::min< long long >( 4096, ( n_cells + 255 ) / 256 );
+                if( fx ) kp::k_adj_reduce< KP_TALLY_FIXED ><<< gr, 256, 0, s >>>( C );
+                else     kp::k_adj_reduce< KP_TALLY_FLOAT ><<< gr, 256, 0, s >>>( C );
+                KP_CUDA( cudaGetLastError(  ) );
+            }
             // packets whose rays found the queue full: both replays inline
             KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
             C.adj_quiet = 1;

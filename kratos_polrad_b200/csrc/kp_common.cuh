@@ -135,7 +135,7 @@ struct kp_mesh
     unsigned   * d_status = nullptr;
     void       * d_pq    = nullptr;  long long pq_cap = 0;        // deferred peel-off rays
     long long    pq_limit = 1ll << 27;                             // ... at most this many
-    void       * d_adj   = nullptr;  long long adj_tasks = 0, adj_packets = 0;  // deferred adjoint
+    void       * d_adj   = nullptr;  size_t adj_bytes = 0;      // deferred adjoint
     float      * d_rf_f  = nullptr;  double * d_rf_d  = nullptr;   // spherical tables
     float      * d_vol_f = nullptr;  double * d_vol_d = nullptr;
 

@@ -145,7 +145,7 @@ void kp_mesh::release(  )
     cudaFree( d_status ); d_status = nullptr;
     cudaFree( d_work );   d_work   = nullptr;
     cudaFree( d_pq );     d_pq     = nullptr; pq_cap = 0;
-    cudaFree( d_adj );    d_adj    = nullptr; adj_tasks = adj_packets = 0;
+    cudaFree( d_adj );    d_adj    = nullptr; adj_bytes = 0;
     cudaFree( d_rf_f );   d_rf_f   = nullptr;
     cudaFree( d_rf_d );   d_rf_d   = nullptr;
     cudaFree( d_vol_f );  d_vol_f  = nullptr;

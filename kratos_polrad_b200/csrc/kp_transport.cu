@@ -603,6 +603,14 @@ k_peel( const __grid_constant__ fwd_params_t P )
     const float2 * sb = P.m.sigma;                // this block's coefficients
     float  ptau = 0.0f;
     float  pG = 0.0f;                             // MODE 2: the ray's score
+    // MODE 2: every ray leaves toward the observer along the same corridor of
+    // cells, so the blocks deposit into private copies (summed afterwards)
+    // rather than all into one tally
+    void * g_dep = P.g_len;
+    if constexpr( MODE == 2 )
+        if( P.adj_priv )
+            g_dep = ( char * ) P.adj_priv + ( size_t ) ( blockIdx.x % P.adj_npriv )
+                    * ( ( size_t ) P.m.n_blocks * P.m.cpb ) * ( TALLY == KP_TALLY_FIXED ? 8 : 4 );
     long long task = -1;
     unsigned n_seg_done = 0;
     int phase = PH_EMIT;
@@ -739,7 +747,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 break;
             }
             if constexpr( MODE == 2 )
-                add_grad< TALLY >( P.g_len, ( size_t ) ( sb - P.m.sigma ) + ci,
+                add_grad< TALLY >( g_dep, ( size_t ) ( sb - P.m.sigma ) + ci,
                                    __dmul_rn( -( double ) pG, t ), P.g_scale );
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
@@ -1064,7 +1072,7 @@ extern "C" int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays )
             mesh->pq_cap = 0;
             KP_CUDA( cudaFree( mesh->d_adj ) );
             mesh->d_adj = nullptr;
-            mesh->adj_tasks = mesh->adj_packets = 0;
+            mesh->adj_bytes = 0;
         }
         mesh->pq_limit = max_rays;
     } );

@@ -117,6 +117,8 @@ struct fwd_params_t
     int       * adj_list;               // [n_packets] packets handed to k_adjoint
     unsigned long long * adj_list_n;    //   ... and their count
     int         adj_quiet;              // k_adjoint: its first replay counts nothing
+    void      * adj_priv;               // k_peel mode 2: adj_npriv private path-length
+    int         adj_npriv;              //   tallies (block b uses copy b % adj_npriv)
     src_dev_t   src[ MAX_SOURCES ];
 };
 
