@@ -508,10 +508,11 @@ k_forward( const __grid_constant__ fwd_params_t P )
         }
 
         // ---- PH_SEGMENT: segments of the active ray, up to KP_WALK_INNER
-        // (DEFER) before the next scheduling round ----
+        // before the next scheduling round where no peel-off ray runs here
+        // (DEFER, or no image) ----
         if( phase != PH_SEGMENT ) continue;
         #pragma unroll 1
-        for( int it = 0; it < ( DEFER ? KP_WALK_INNER : 1 ); ++ it )
+        for( int it = 0; it < ( DEFER || ( ! DD && P.img_n == 0 ) ? KP_WALK_INNER : 1 ); ++ it )
         {
             // the active ray's direction is in p.d / p.inv (a peel-off ray
             // holds them while the walk's are parked)
