@@ -216,6 +216,9 @@ public:
     {
         api( kp_mesh_set_sigma( m_, src, n_values, on_device ? 1 : 0, s ) );
     }
+    // Upper bound on the peel-off queue in rays (80 B each); larger solves
+    // run in chunks of limit / 12 packets.
+    void peel_queue_limit( long long max_rays ) { api( kp_mesh_peel_queue_limit( m_, max_rays ) ); }
     // Device error bits of the last kernels (0: none); throws if any is set
     // when `raise` is true, as the reference's debug flag aborts a run.
     unsigned status( stream_t s = nullptr, bool raise = true )
@@ -240,6 +243,9 @@ struct transport
     {
         api( kp_transport_forward( m.get(  ), & c, & t, s ) );
     }
+    // Profiling: later forward solves of this thread record `event` (a
+    // cudaEvent_t) between the walk and the peel-off march (nullptr: off).
+    static void split_event( void * event ) { api( kp_transport_split_event( event ) ); }
     static void forward_noalloc( mesh_t & m, const kp_transport_cfg_t & c,
                                  const kp_tallies_t & t, stream_t s = nullptr )
     {

@@ -40,6 +40,18 @@ static int host_part( const char * ini )
         std::printf( "OK throws \"%s\"\n", e.what(  ) );
     }
     std::printf( "OK abi %d\n", kp_abi_version(  ) );
+    // peel-off queue limit: checked before any device work
+    mesh.peel_queue_limit( 1 << 20 );
+    try
+    {
+        mesh.peel_queue_limit( 100 );
+        return 6;
+    }
+    catch( const std::runtime_error & e )
+    {
+        std::printf( "OK queue limit throws \"%s\"\n", e.what(  ) );
+    }
+    kp::transport::split_event( nullptr );
     // spherical mesh and runtime refinement through the C++ layer
     kp_mesh_desc_t d {};
     const double lo[ 3 ] = { 1.0, 0.4, 0.0 }, hi[ 3 ] = { 3.0, 2.7, 6.283185307179586 };

@@ -34,7 +34,7 @@ def test_host_parts(program):
     exe, ini = program
     r = subprocess.run([exe, "host", ini], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("OK ") == 5, r.stdout
+    assert r.stdout.count("OK ") == 6, r.stdout
 
 
 @pytest.mark.gpu
