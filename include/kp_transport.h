@@ -422,6 +422,30 @@ int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           void * grad_len, void * grad_int,
                           unsigned long long * counters, void * stream );
 
+/* A forward solve followed by gradients of it (an autograd step).  No
+ * reference counterpart.  kp_transport_forward_tape is kp_transport_forward
+ * (same tallies, bit for bit) that also keeps, in the mesh, each packet's
+ * vertex peel-off rays in vertex order with their attenuation; *tape_id
+ * receives an id (> 0), or 0 when the solve has more packets than one chunk
+ * of the peel-off queue (kp_mesh_peel_queue_limit / 12) and was not taped.
+ * kp_transport_adjoint_tape then computes kp_transport_adjoint's gradients
+ * (bit for bit in fixed point) without its first replay and measuring
+ * march; it may be called several times per tape (different adj_image).
+ * The tape lasts until the next forward or adjoint solve on the mesh,
+ * kp_mesh_set_sigma, kp_mesh_sigma_ptr or kp_mesh_peel_queue_limit; the
+ * adjoint refuses (KP_ERR_CONFIG) a tape that is gone or a cfg that does
+ * not describe the taped solve.  The coefficients must be those of the
+ * taped solve.  counters receives the counts of the work done (the second
+ * replay and the deposits). */
+int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                               const kp_tallies_t * tallies, void * stream, long long * tape_id );
+int kp_transport_adjoint_tape( kp_mesh_t * mesh, long long tape_id,
+                               const kp_transport_cfg_t * cfg, const float * adj_image,
+                               int grad_fx_shift, void * grad_len, void * grad_int,
+                               unsigned long long * counters, void * stream );
+/* Id of the mesh's current tape (0: none). */
+int kp_mesh_tape_id( const kp_mesh_t * mesh, long long * tape_id );
+
 /* Same solve as kp_transport_forward, for callers that must not allocate
  * device memory during the call: code that owns every device byte itself
  * (a fixed arena or pool it sized at start-up), or a step that has to run

@@ -446,8 +446,8 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
         for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
         o.b = p.b;
         o.w = w; o.I = I; o.Q = Q; o.U = U; o.V = V;
-        o.pix = pix; o.cpix = -1; o.lp = lp; o.kv = kv;
-        if( link >= 0 ) P.pq[ link ].cpix = ( int ) k;
+        o.pix = pix; o.cpix = 0; o.lp = lp; o.kv = kv; o.next = -1;
+        if( link >= 0 ) P.pq[ link ].next = ( int ) k;
         else P.adj_head[ lp ] = ( int ) k;
         link = ( int ) k;
     };
@@ -543,7 +543,7 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
                     if constexpr( PASS == 0 )
                         queue_ray( pix, 1.0f, 0x1.45f306p-4f, 0.0f, 0.0f, 0.0f, 0 );
                     else if( link >= 0 )
-                        link = P.pq[ link ].cpix;     // its ray is deposited by k_peel
+                        link = P.pq[ link ].next;     // its ray is deposited by k_peel
                 }
             }
             faces_all( P.m, p.b, p.c, p.d, fx );
@@ -583,7 +583,7 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
                     else if( link >= 0 )
                     {   // this vertex's score leaves R once its ray is deposited
                         const float G = P.adj_G[ link ];
-                        link = P.pq[ link ].cpix;
+                        link = P.pq[ link ].next;
                         if( G != 0.0f )
                             R = __dsub_rn( R, ( double ) G );
                     }
@@ -687,10 +687,30 @@ __global__ void k_adj_fold( const __grid_constant__ fwd_params_t P )
             const peel_task_t & o = P.pq[ t ];
             if( o.kv > 0 )
                 R = __dadd_rn( R, ( double ) P.adj_G[ t ] );
-            const int nx = o.cpix;
+            const int nx = o.next;
             t = nx > t ? nx : -1;
         }
         P.adj_R0[ lp ] = R;
+    }
+}
+
+// Adjoint of a taped solve: the score of every queued ray from the
+// attenuation the solve's march kept (k_peel mode 3), with the expression of
+// the measuring march (k_peel mode 1).  Rays of flagged packets are skipped.
+__global__ void k_adj_score( const __grid_constant__ fwd_params_t P )
+{
+    const long long n = min( * P.pq_count, ( unsigned long long ) P.pq_cap );
+    for( long long t = blockIdx.x * ( long long ) blockDim.x + threadIdx.x; t < n;
+         t += ( long long ) gridDim.x * blockDim.x )
+    {
+        const peel_task_t & o = P.pq[ t ];
+        if( P.adj_flag[ o.lp ] ) continue;
+        const float att = P.adj_att[ t ];
+        float G = 0.0f;
+        if( att >= 0.0f )
+            G = score( P, o.pix, __fmul_rn( att, o.I ), __fmul_rn( att, o.Q ),
+                       __fmul_rn( att, o.U ), __fmul_rn( att, o.V ) );
+        P.adj_G[ t ] = G;
     }
 }
 
@@ -723,6 +743,138 @@ __global__ void k_adj_reduce( const __grid_constant__ fwd_params_t P )
 }   // namespace
 }   // namespace kp
 
+namespace kp
+{
+void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk )
+{
+    const long long cap = mesh->pq_cap;
+    const long long n_cells = ( long long ) P.m.n_blocks * P.m.cpb;
+    const int n_priv = KP_ADJ_PRIV;
+    const size_t priv_bytes = n_priv > 1 ? ( size_t ) n_priv * n_cells * 8 : 0;
+    // 256 B of counters, the per-packet and per-task arrays, then the private
+    // tallies (256-byte aligned)
+    const size_t adj_bytes = ( 256 + ( size_t ) n_pk * ( sizeof( double ) + 3 * sizeof( int ) )
+                               + ( size_t ) cap * 2 * sizeof( float ) + 255 ) & ~( size_t ) 255;
+    if( mesh->adj_bytes < adj_bytes + priv_bytes )
+    {
+        cudaFree( mesh->d_adj );
+        mesh->d_adj = nullptr;
+        mesh->adj_bytes = 0;
+        mesh->tape_id = 0;
+        KP_CUDA( cudaMalloc( & mesh->d_adj, adj_bytes + priv_bytes ) );
+        mesh->adj_bytes = adj_bytes + priv_bytes;
+    }
+    char * a = static_cast< char * >( mesh->d_adj );
+    P.work     = reinterpret_cast< unsigned long long * >( a );
+    P.pq_count = P.work + 1;
+    P.pq_next  = P.work + 2;
+    P.adj_list_n = P.work + 3;
+    a += 256;
+    P.adj_R0   = reinterpret_cast< double * >( a );
+    P.adj_G    = reinterpret_cast< float * >( a + n_pk * sizeof( double ) );
+    P.adj_att  = P.adj_G + cap;
+    P.adj_head = reinterpret_cast< int * >( P.adj_att + cap );
+    P.adj_flag = P.adj_head + n_pk;
+    P.adj_list = P.adj_flag + n_pk;
+    P.adj_priv = n_priv > 1 ? static_cast< char * >( mesh->d_adj ) + adj_bytes : nullptr;
+    P.adj_npriv = n_priv > 1 ? n_priv : 0;
+    P.pq = static_cast< peel_task_t * >( mesh->d_pq );
+    P.pq_cap = cap;
+}
+}   // namespace kp
+
+namespace
+{
+// Launch parameters of an adjoint: the forward's, with the image tallies
+// replaced by the gradient outputs.
+void adjoint_params( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg, const float * adj_image,
+                     int grad_fx_shift, void * grad_len, void * grad_int,
+                     unsigned long long * counters, kp::fwd_params_t & P )
+{
+    kp::require( mesh && cfg && adj_image && grad_len && grad_int, "null argument" );
+    kp::require( cfg->image_n > 0, "the adjoint needs a peel-off image (image_n > 0)" );
+    kp::require( grad_fx_shift >= 0 && grad_fx_shift <= 48, "grad_fx_shift out of range" );
+    mesh->upload(  );
+    kp_tallies_t none {  };
+    none.counters = counters;
+    // the forward's image buffers are not written by the adjoint; any
+    // non-null placeholders pass the configuration checks
+    none.image = grad_len;
+    none.image_batch = grad_len;
+    none.mu = grad_len;
+    kp_transport_cfg_t c = * cfg;
+    c.n_record = 0;
+    kp::make_fwd_params( mesh, c, none, P );
+    P.image = P.img_batch = P.mu_tally = nullptr;
+    P.adj_img = reinterpret_cast< const float4 * >( adj_image );
+    P.g_len = grad_len;
+    P.g_int = grad_int;
+    P.g_scale = std::ldexp( 1.0, grad_fx_shift );
+}
+
+// The adjoint once every queued ray of the chunk C has its score in adj_G:
+// R per packet, the second replay, the deposits along the rays, and the
+// packets left to k_adjoint (whose first replay counts nothing).
+void adjoint_second_half( kp::fwd_params_t & C, int tally_mode, cudaStream_t s )
+{
+    const bool fx = tally_mode == KP_TALLY_FIXED;
+    const int threads = kp::FWD_THREADS;
+    const long long n_cells = ( long long ) C.m.n_blocks * C.m.cpb;
+    const void * kw = fx ? ( const void * ) kp::k_adj_walk< KP_TALLY_FIXED, 1 >
+                         : ( const void * ) kp::k_adj_walk< KP_TALLY_FLOAT, 1 >;
+    const void * ka = fx ? ( const void * ) kp::k_adjoint< KP_TALLY_FIXED >
+                         : ( const void * ) kp::k_adjoint< KP_TALLY_FLOAT >;
+    const long long blocks = ( C.n_packets + threads - 1 ) / threads;
+    const unsigned gw = ( unsigned ) std::min< long long >( kp::persistent_grid( kw, threads ), blocks );
+    const unsigned ga = ( unsigned ) std::min< long long >( kp::persistent_grid( ka, threads ), blocks );
+    const unsigned gf = ( unsigned ) std::min< long long >( 4096, ( C.n_packets + 255 ) / 256 );
+    kp::k_adj_fold<<< gf, 256, 0, s >>>( C );                           // R per packet
+    KP_CUDA( cudaGetLastError(  ) );
+    KP_CUDA( cudaMemsetAsync( C.work, 0, sizeof( unsigned long long ), s ) );
+    if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 1 ><<< gw, threads, 0, s >>>( C );
+    else     kp::k_adj_walk< KP_TALLY_FLOAT, 1 ><<< gw, threads, 0, s >>>( C );
+    KP_CUDA( cudaGetLastError(  ) );
+    if( C.adj_priv )
+        KP_CUDA( cudaMemsetAsync( C.adj_priv, 0, ( size_t ) C.adj_npriv * n_cells * ( fx ? 8 : 4 ), s ) );
+    kp::launch_peel_adjoint( C, tally_mode, 2, s );
+    if( C.adj_priv )
+    {
+        const unsigned gr = ( unsigned ) std::min< long long >( 4096, ( n_cells + 255 ) / 256 );
+        if( fx ) kp::k_adj_reduce< KP_TALLY_FIXED ><<< gr, 256, 0, s >>>( C );
+        else     kp::k_adj_reduce< KP_TALLY_FLOAT ><<< gr, 256, 0, s >>>( C );
+        KP_CUDA( cudaGetLastError(  ) );
+    }
+    // packets whose rays found the queue full: both replays inline
+    KP_CUDA( cudaMemsetAsync( C.work, 0, sizeof( unsigned long long ), s ) );
+    C.adj_quiet = 1;
+    if( fx ) kp::k_adjoint< KP_TALLY_FIXED ><<< ga, threads, 0, s >>>( C );
+    else     kp::k_adjoint< KP_TALLY_FLOAT ><<< ga, threads, 0, s >>>( C );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+
+// The fields of two solve configurations that decide the packets' paths and
+// their peel-off rays.
+bool same_solve( const kp_transport_cfg_t & a, const kp_source_t * sa, const kp_transport_cfg_t & b )
+{
+    bool eq = a.n_packets == b.n_packets && a.packet_offset == b.packet_offset
+           && a.seed == b.seed && a.stream_id == b.stream_id && a.phase == b.phase
+           && a.hg_g == b.hg_g && a.pol_max == b.pol_max && a.n_sources == b.n_sources
+           && a.image_n == b.image_n && a.inclination_deg == b.inclination_deg
+           && a.azimuth_deg == b.azimuth_deg && a.image_half_width == b.image_half_width
+           && a.tau_peel_max == b.tau_peel_max && a.w_min == b.w_min
+           && a.rr_survive == b.rr_survive && a.max_scatter == b.max_scatter
+           && a.max_steps == b.max_steps && b.sources != nullptr;
+    for( int k = 0; eq && k < 3; ++ k ) eq = a.image_center[ k ] == b.image_center[ k ];
+    for( int k = 0; eq && k < b.n_sources; ++ k )
+    {
+        const kp_source_t & x = sa[ k ], & y = b.sources[ k ];
+        eq = x.kind == y.kind && x.emit == y.emit && x.pos[ 0 ] == y.pos[ 0 ]
+          && x.pos[ 1 ] == y.pos[ 1 ] && x.pos[ 2 ] == y.pos[ 2 ];
+    }
+    return eq;
+}
+}   // namespace
+
 extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                                      const float * adj_image, int grad_fx_shift,
                                      void * grad_len, void * grad_int,
@@ -730,73 +882,21 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
 {
     return kp::guarded( "kp_transport_adjoint", [ & ]
     {
-        kp::require( mesh && cfg && adj_image && grad_len && grad_int, "null argument" );
-        kp::require( cfg->image_n > 0, "the adjoint needs a peel-off image (image_n > 0)" );
-        kp::require( grad_fx_shift >= 0 && grad_fx_shift <= 48, "grad_fx_shift out of range" );
-        mesh->upload(  );
         static thread_local kp::fwd_params_t P;
-        kp_tallies_t none {  };
-        none.counters = counters;
-        // the forward's image buffers are not written by the adjoint; any
-        // non-null placeholders pass the configuration checks
-        none.image = grad_len;
-        none.image_batch = grad_len;
-        none.mu = grad_len;
-        kp_transport_cfg_t c = * cfg;
-        c.n_record = 0;
-        kp::make_fwd_params( mesh, c, none, P );
-        P.image = P.img_batch = P.mu_tally = nullptr;
-        P.adj_img = reinterpret_cast< const float4 * >( adj_image );
-        P.g_len = grad_len;
-        P.g_int = grad_int;
-        P.g_scale = std::ldexp( 1.0, grad_fx_shift );
-        P.work = mesh->workspace(  );
+        adjoint_params( mesh, cfg, adj_image, grad_fx_shift, grad_len, grad_int, counters, P );
         if( P.n_packets == 0 ) return;
         auto s = ( cudaStream_t ) stream;
-        const bool fx = c.tally_mode == KP_TALLY_FIXED;
+        const bool fx = cfg->tally_mode == KP_TALLY_FIXED;
         const int threads = kp::FWD_THREADS;
+        mesh->tape_id = 0;                  // the queue is overwritten
         // The vertices' peel-off rays go through the mesh's queue (12 rays per
         // packet, chunks of packets beyond that) and are marched by k_peel.
         kp::ensure_peel_queue( mesh, P.n_packets );
-        const long long cap = mesh->pq_cap;
-        const long long chunk = std::max< long long >( cap / kp::PQ_PER_PACKET, 1 );
-        const long long n_pk = std::min( chunk, P.n_packets );
-        const long long n_cells = ( long long ) P.m.n_blocks * P.m.cpb;
-        const int n_priv = KP_ADJ_PRIV;
-        const size_t priv_bytes = n_priv > 1 ? ( size_t ) n_priv * n_cells * 8 : 0;
-        // per-packet and per-task arrays, then the private tallies (256-byte aligned)
-        const size_t adj_bytes = ( ( size_t ) n_pk * ( sizeof( double ) + 3 * sizeof( int ) )
-                                   + ( size_t ) cap * sizeof( float ) + 255 ) & ~( size_t ) 255;
-        if( mesh->adj_bytes < adj_bytes + priv_bytes )
-        {
-            cudaFree( mesh->d_adj );
-            mesh->d_adj = nullptr;
-            mesh->adj_bytes = 0;
-            KP_CUDA( cudaMalloc( & mesh->d_adj, adj_bytes + priv_bytes ) );
-            mesh->adj_bytes = adj_bytes + priv_bytes;
-        }
-        char * a = static_cast< char * >( mesh->d_adj );
-        P.adj_R0   = reinterpret_cast< double * >( a );
-        P.adj_G    = reinterpret_cast< float * >( a + n_pk * sizeof( double ) );
-        P.adj_head = reinterpret_cast< int * >( a + n_pk * sizeof( double ) + cap * sizeof( float ) );
-        P.adj_flag = P.adj_head + n_pk;
-        P.adj_list = P.adj_flag + n_pk;
-        if( n_priv > 1 )
-        {
-            P.adj_priv = a + adj_bytes;
-            P.adj_npriv = n_priv;
-        }
-        P.pq = static_cast< kp::peel_task_t * >( mesh->d_pq );
-        P.pq_cap = cap;
-        P.pq_count = P.work + 1;
-        P.pq_next = P.work + 2;
-        P.adj_list_n = P.work + 3;
+        const long long chunk = std::max< long long >( mesh->pq_cap / kp::PQ_PER_PACKET, 1 );
+        kp::adjoint_buffers( mesh, P, std::min( chunk, P.n_packets ) );
         const void * kw0 = fx ? ( const void * ) kp::k_adj_walk< KP_TALLY_FIXED, 0 >
                               : ( const void * ) kp::k_adj_walk< KP_TALLY_FLOAT, 0 >;
-        const void * ka = fx ? ( const void * ) kp::k_adjoint< KP_TALLY_FIXED >
-                             : ( const void * ) kp::k_adjoint< KP_TALLY_FLOAT >;
         const long long grid_w = kp::persistent_grid( kw0, threads );
-        const long long grid_a = kp::persistent_grid( ka, threads );
         static thread_local kp::fwd_params_t C;
         for( long long done = 0; done < P.n_packets; done += chunk )
         {
@@ -805,41 +905,88 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
             C.n_packets = std::min( chunk, P.n_packets - done );
             const unsigned gw = ( unsigned ) std::min< long long >( grid_w,
                                                                    ( C.n_packets + threads - 1 ) / threads );
-            KP_CUDA( cudaMemsetAsync( P.work, 0, 4 * sizeof( unsigned long long ), s ) );
+            KP_CUDA( cudaMemsetAsync( C.work, 0, 4 * sizeof( unsigned long long ), s ) );
             KP_CUDA( cudaMemsetAsync( C.adj_head, 0xff, C.n_packets * sizeof( int ), s ) );
             KP_CUDA( cudaMemsetAsync( C.adj_flag, 0, C.n_packets * sizeof( int ), s ) );
             // first replay: walks, vertex rays queued
             if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 0 ><<< gw, threads, 0, s >>>( C );
             else     kp::k_adj_walk< KP_TALLY_FLOAT, 0 ><<< gw, threads, 0, s >>>( C );
             KP_CUDA( cudaGetLastError(  ) );
-            kp::launch_peel_adjoint( C, c.tally_mode, 1, s );          // scores G
-            const unsigned gf = ( unsigned ) std::min< long long >( 4096, ( C.n_packets + 255 ) / 256 );
-            kp::k_adj_fold<<< gf, 256, 0, s >>>( C );                   // R per packet
-            KP_CUDA( cudaGetLastError(  ) );
-            // second replay: deposits along the walks, then along the rays
-            KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
-            if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 1 ><<< gw, threads, 0, s >>>( C );
-            else     kp::k_adj_walk< KP_TALLY_FLOAT, 1 ><<< gw, threads, 0, s >>>( C );
-            KP_CUDA( cudaGetLastError(  ) );
-            if( n_priv > 1 )
-                KP_CUDA( cudaMemsetAsync( C.adj_priv, 0, ( size_t ) n_priv * n_cells
-                                          * ( fx ? 8 : 4 ), s ) );
-            kp::launch_peel_adjoint( C, c.tally_mode, 2, s );
-            if( n_priv > 1 )
-            {
-                const unsigned gr = ( unsigned ) std::min< long long >( 4096, ( n_cells + 255 ) / 256 );
-                if( fx ) kp::k_adj_reduce< KP_TALLY_FIXED ><<< gr, 256, 0, s >>>( C );
-                else     kp::k_adj_reduce< KP_TALLY_FLOAT ><<< gr, 256, 0, s >>>( C );
-                KP_CUDA( cudaGetLastError(  ) );
-            }
-            // packets whose rays found the queue full: both replays inline
-            KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
-            C.adj_quiet = 1;
-            const unsigned ga = ( unsigned ) std::min< long long >( grid_a,
-                                                                   ( C.n_packets + threads - 1 ) / threads );
-            if( fx ) kp::k_adjoint< KP_TALLY_FIXED ><<< ga, threads, 0, s >>>( C );
-            else     kp::k_adjoint< KP_TALLY_FLOAT ><<< ga, threads, 0, s >>>( C );
-            KP_CUDA( cudaGetLastError(  ) );
+            kp::launch_peel_adjoint( C, cfg->tally_mode, 1, s );       // scores G
+            adjoint_second_half( C, cfg->tally_mode, s );
         }
+    } );
+}
+
+extern "C" int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                          const kp_tallies_t * tallies, void * stream,
+                                          long long * tape_id )
+{
+    return kp::guarded( "kp_transport_forward_tape", [ & ]
+    {
+        kp::require( mesh && cfg && tallies && tape_id, "null argument" );
+        * tape_id = 0;
+        kp::require( cfg->image_n > 0, "a taped solve needs a peel-off image (image_n > 0)" );
+        mesh->upload(  );
+        mesh->tape_id = 0;
+        static thread_local kp::fwd_params_t P;
+        kp::make_fwd_params( mesh, * cfg, * tallies, P );
+        if( P.n_packets == 0 ) return;
+        kp::ensure_peel_queue( mesh, P.n_packets );
+        if( P.n_packets > std::max< long long >( mesh->pq_cap / kp::PQ_PER_PACKET, 1 ) )
+        {   // more packets than one chunk of the queue: an untaped solve
+            kp::require( kp_transport_forward( mesh, cfg, tallies, stream ) == KP_OK,
+                         kp_last_error(  ), KP_ERR_CUDA );
+            return;
+        }
+        if( cfg->lane_batch == 0 ) P.ev_batch = 12;
+        kp::adjoint_buffers( mesh, P, P.n_packets );
+        auto s = ( cudaStream_t ) stream;
+        KP_CUDA( cudaMemsetAsync( P.work, 0, 4 * sizeof( unsigned long long ), s ) );
+        KP_CUDA( cudaMemsetAsync( P.adj_head, 0xff, P.n_packets * sizeof( int ), s ) );
+        KP_CUDA( cudaMemsetAsync( P.adj_flag, 0, P.n_packets * sizeof( int ), s ) );
+        if( cfg->tally_mode == KP_TALLY_FIXED )
+            kp::launch_deferred_chunk< KP_TALLY_FIXED, true >( P, s );
+        else
+            kp::launch_deferred_chunk< KP_TALLY_FLOAT, true >( P, s );
+        mesh->tape_cfg = * cfg;
+        mesh->tape_cfg.sources = nullptr;
+        for( int k = 0; k < cfg->n_sources; ++ k ) mesh->tape_src[ k ] = cfg->sources[ k ];
+        mesh->tape_n = P.n_packets;
+        mesh->tape_id = ++ mesh->tape_serial;
+        * tape_id = mesh->tape_id;
+    } );
+}
+
+extern "C" int kp_transport_adjoint_tape( kp_mesh_t * mesh, long long tape_id,
+                                          const kp_transport_cfg_t * cfg, const float * adj_image,
+                                          int grad_fx_shift, void * grad_len, void * grad_int,
+                                          unsigned long long * counters, void * stream )
+{
+    return kp::guarded( "kp_transport_adjoint_tape", [ & ]
+    {
+        kp::require( mesh && cfg, "null argument" );
+        kp::require( tape_id > 0 && tape_id == mesh->tape_id,
+                     "no taped solve with this id on the mesh (a later solve or new "
+                     "coefficients replaced it)", KP_ERR_CONFIG );
+        kp::require( same_solve( mesh->tape_cfg, mesh->tape_src, * cfg ),
+                     "cfg differs from the taped solve's", KP_ERR_CONFIG );
+        static thread_local kp::fwd_params_t P;
+        adjoint_params( mesh, cfg, adj_image, grad_fx_shift, grad_len, grad_int, counters, P );
+        kp::adjoint_buffers( mesh, P, mesh->tape_n );      // the taped solve's layout
+        auto s = ( cudaStream_t ) stream;
+        const unsigned gs = 4 * 148;
+        kp::k_adj_score<<< gs, 256, 0, s >>>( P );                        // G from the tape
+        KP_CUDA( cudaGetLastError(  ) );
+        adjoint_second_half( P, cfg->tally_mode, s );
+    } );
+}
+
+extern "C" int kp_mesh_tape_id( const kp_mesh_t * mesh, long long * tape_id )
+{
+    return kp::guarded( "kp_mesh_tape_id", [ & ]
+    {
+        kp::require( mesh && tape_id, "null argument" );
+        * tape_id = mesh->tape_id;
     } );
 }

@@ -136,6 +136,11 @@ struct kp_mesh
     void       * d_pq    = nullptr;  long long pq_cap = 0;        // deferred peel-off rays
     long long    pq_limit = 1ll << 27;                             // ... at most this many
     void       * d_adj   = nullptr;  size_t adj_bytes = 0;      // deferred adjoint
+    // the taped forward solve whose rays the queue and d_adj hold (0: none)
+    long long    tape_id = 0, tape_serial = 0;
+    long long    tape_n  = 0;                                      // its packets
+    kp_transport_cfg_t tape_cfg {  };
+    kp_source_t  tape_src[ KP_MAX_SOURCES ] {  };
     float      * d_rf_f  = nullptr;  double * d_rf_d  = nullptr;   // spherical tables
     float      * d_vol_f = nullptr;  double * d_vol_d = nullptr;
 

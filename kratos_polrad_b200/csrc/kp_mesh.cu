@@ -145,7 +145,7 @@ void kp_mesh::release(  )
     cudaFree( d_status ); d_status = nullptr;
     cudaFree( d_work );   d_work   = nullptr;
     cudaFree( d_pq );     d_pq     = nullptr; pq_cap = 0;
-    cudaFree( d_adj );    d_adj    = nullptr; adj_bytes = 0;
+    cudaFree( d_adj );    d_adj    = nullptr; adj_bytes = 0; tape_id = 0;
     cudaFree( d_rf_f );   d_rf_f   = nullptr;
     cudaFree( d_rf_d );   d_rf_d   = nullptr;
     cudaFree( d_vol_f );  d_vol_f  = nullptr;
@@ -378,6 +378,7 @@ int kp_mesh_set_sigma( kp_mesh_t * mesh, const float * src, long long n_values,
         const long long n_cells = ( long long ) t.n_blocks * t.cells_per_block;
         require( n_values == 2 * n_cells, "sigma needs 2*n_cells values" );
         mesh->upload(  );
+        mesh->tape_id = 0;                  // new coefficients: a taped solve is stale
         KP_CUDA( cudaMemcpyAsync( mesh->d_sigma, src, n_values * sizeof( float ),
                                   on_device ? cudaMemcpyDeviceToDevice
                                             : cudaMemcpyHostToDevice,
@@ -393,6 +394,7 @@ int kp_mesh_sigma_ptr( kp_mesh_t * mesh, float ** sigma )
     {
         require( mesh && sigma, "null argument" );
         mesh->upload(  );
+        mesh->tape_id = 0;                  // the caller may write new coefficients
         * sigma = reinterpret_cast< float * >( mesh->d_sigma );
     } );
 }

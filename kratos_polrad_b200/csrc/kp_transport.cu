@@ -55,7 +55,10 @@ namespace cg = cooperative_groups;
 // arithmetic is that of the replicated solve.
 // DEFER: a peel-off ray is written to the task queue for k_peel (when it
 // has room) instead of being marched here; the walk continues at once.
-template< int TALLY, int NT, bool DD = false, bool DEFER = false >
+// TAPE (with DEFER): the rays are also linked per packet, in vertex order,
+// for the adjoint of this solve (kp_transport_adjoint_tape); a packet with a
+// ray that found the queue full is flagged and listed instead.
+template< int TALLY, int NT, bool DD = false, bool DEFER = false, bool TAPE = false >
 __global__ void __launch_bounds__( NT, KP_FWD_RESIDENT / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
@@ -76,11 +79,12 @@ k_forward( const __grid_constant__ fwd_params_t P )
     int si = 0;                                   // scene of a batched launch
     int hop_ax = 0;                               // face axis of a pending hand-off
     bool solo = false;                            // DD: peel-off ray without a parked walk
+    int tlink = -1;                               // TAPE: the packet's last task (-2: flagged)
 
-    // DEFER: appends the peel-off ray prepared in sp/sd (starting at p's
-    // position) to the queue; false when the queue is full.  The lanes that
-    // append together take their slots with one atomic.
-    auto defer_peel = [ & ](  ) -> bool
+    // DEFER: appends the peel-off ray of vertex kv prepared in sp/sd
+    // (starting at p's position) to the queue; false when the queue is full.
+    // The lanes that append together take their slots with one atomic.
+    auto defer_peel = [ & ]( int kv ) -> bool
     {
         const unsigned m = __activemask(  );
         const int leader = __ffs( m ) - 1;
@@ -89,14 +93,31 @@ k_forward( const __grid_constant__ fwd_params_t P )
             base = atomicAdd( P.pq_count, ( unsigned long long ) __popc( m ) );
         base = __shfl_sync( m, base, leader );
         const unsigned long long k = base + __popc( m & ( ( 1u << lane ) - 1u ) );
+        const int lp = TAPE ? ( int ) ( p.pid(  ) - P.pid0 ) : 0;
         if( k >= ( unsigned long long ) P.pq_cap )
+        {
+            if constexpr( TAPE )
+                if( tlink != -2 )
+                {   // the adjoint replays this packet with its rays inline
+                    tlink = -2;
+                    P.adj_flag[ lp ] = 1;
+                    P.adj_list[ atomicAdd( P.adj_list_n, 1ull ) ] = lp;
+                }
             return false;
+        }
         const int t = threadIdx.x;
         peel_task_t & o = P.pq[ k ];
         for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
         o.b = p.b;
         o.w = sp.w[ t ]; o.I = sp.I[ t ]; o.Q = sp.Q[ t ]; o.U = sp.U[ t ]; o.V = sp.V[ t ];
         o.pix = sp.pix[ t ]; o.cpix = sd.cpix[ t ];
+        if constexpr( TAPE )
+        {
+            o.lp = lp; o.kv = kv; o.next = -1;
+            if( tlink >= 0 ) P.pq[ tlink ].next = ( int ) k;
+            else P.adj_head[ lp ] = ( int ) k;
+            tlink = ( int ) k;
+        }
         return true;
     };
 
@@ -378,6 +399,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             count( sp, KP_CNT_EMITTED );
+            if constexpr( TAPE ) tlink = -1;     // a new packet: its list starts empty
             sc.batch[ threadIdx.x ] = ( int ) ( p.pid(  ) % P.n_batch );
             p.tau = sample_tau( p.rng );
             phase = PH_SEGMENT;
@@ -419,7 +441,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sd.cpix[ t ] = coarse_pixel( P, pix, sc.batch[ t ] );
                     bool queued = false;
                     if constexpr( DEFER )
-                        queued = defer_peel(  );
+                        queued = defer_peel( 0 );
                     if( ! queued )
                     {
                         pend = 0; ptau = 0.0f; pk = 0;
@@ -481,7 +503,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             if( ! end && p.n_steps >= P.max_steps )
                 end = PK_STEP_CAP;
             if constexpr( DEFER )
-                if( do_peel && defer_peel(  ) )
+                if( do_peel && defer_peel( p.n_scat ) )
                     do_peel = false;             // queued: the walk goes on (or ends) now
             if( do_peel )
             {
@@ -581,7 +603,9 @@ k_forward( const __grid_constant__ fwd_params_t P )
 // lane, and a lane holds only the ray's position, faces, cell, optical depth
 // and its block's origin and spacing (the next face is computed from them,
 // with exit_dist's expression, without a load).
-// MODE 0 deposits each ray into the image (forward solve).  The deferred
+// MODE 0 deposits each ray into the image (forward solve); MODE 3 does the
+// same and keeps each ray's attenuation w exp(-tau) (-1 beyond the cut) in
+// adj_att for the adjoint of a taped solve.  The deferred
 // adjoint marches the same tasks twice: MODE 1 measures each ray's score G
 // (what the image deposit would be worth to the loss) into adj_G, MODE 2
 // deposits -G * length into the path-length gradient along each segment
@@ -650,17 +674,21 @@ k_peel( const __grid_constant__ fwd_params_t P )
         {
             if( phase != PH_EMIT ) continue;
             const int leader = __ffs( m_fetch ) - 1;
-            if constexpr( MODE == 0 )
+            if constexpr( MODE == 0 || MODE == 3 )
             {
                 const bool dep = task >= 0 && ptau <= P.tau_cut;
+                float att = -1.0f;                    // MODE 3: -1 marks a ray beyond the cut
                 if( dep )
                 {   // deposit of the ray that just ended (after_crossing's)
                     const peel_task_t & o = P.pq[ task ];
-                    const float att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
+                    att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
                     deposit_pixel< TALLY >( P, o.pix, o.cpix, __fmul_rn( att, o.I ),
                                             __fmul_rn( att, o.Q ), __fmul_rn( att, o.U ),
                                             __fmul_rn( att, o.V ) );
                 }
+                if constexpr( MODE == 3 )
+                    if( task >= 0 )
+                        P.adj_att[ task ] = att;
                 const unsigned m_dep = __ballot_sync( m_fetch, dep );
                 if( ( int ) lane == leader && m_dep )
                     atomicAdd( cnt_s + KP_CNT_DEPOSITS, ( unsigned long long ) __popc( m_dep ) );
@@ -691,7 +719,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             const peel_task_t & o = P.pq[ idx ];
-            if constexpr( MODE != 0 )
+            if constexpr( MODE == 1 || MODE == 2 )
             {   // rays of packets left to k_adjoint, and rays worth nothing
                 if( P.adj_flag[ o.lp ] )
                     continue;
@@ -973,22 +1001,25 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets )
     }
 }
 
-template< int TALLY >
+template< int TALLY, bool TAPE >
 void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s )
 {
     P.pq_count = P.work + 1;
     P.pq_next = P.work + 2;
     KP_CUDA( cudaMemsetAsync( P.work, 0, 3 * sizeof( unsigned long long ), s ) );
-    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true >;
+    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true, TAPE >;
     long long grid = persistent_grid( kf, 256 );
     grid = std::min< long long >( grid, ( P.n_packets + 255 ) / 256 );
-    k_forward< TALLY, 256, false, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+    k_forward< TALLY, 256, false, true, TAPE ><<< ( unsigned ) grid, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
     if( split_event ) KP_CUDA( cudaEventRecord( split_event, s ) );
-    const long long gp = persistent_grid( ( const void * ) k_peel< TALLY, 0 >, 256 );
-    k_peel< TALLY, 0 ><<< ( unsigned ) gp, 256, 0, s >>>( P );
+    constexpr int MODE = TAPE ? 3 : 0;
+    const long long gp = persistent_grid( ( const void * ) k_peel< TALLY, MODE >, 256 );
+    k_peel< TALLY, MODE ><<< ( unsigned ) gp, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
 }
+template void launch_deferred_chunk< KP_TALLY_FIXED, true >( fwd_params_t &, cudaStream_t );
+template void launch_deferred_chunk< KP_TALLY_FLOAT, true >( fwd_params_t &, cudaStream_t );
 
 // The deferred adjoint's marches of the queued vertex rays: mode 1 measures
 // their scores, mode 2 deposits along them (k_peel).
@@ -1017,6 +1048,7 @@ void launch_peel_adjoint( const fwd_params_t & P, int tally_mode, int mode, cuda
 template< int TALLY >
 void launch_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
 {
+    mesh->tape_id = 0;                      // the queue is overwritten
     ensure_peel_queue( mesh, P.n_packets );
     const long long chunk = std::max< long long >( mesh->pq_cap / PQ_PER_PACKET, 1 );
     static thread_local fwd_params_t C;
@@ -1029,7 +1061,7 @@ void launch_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
         C.n_packets = std::min( chunk, P.n_packets - done );
         C.n_record = std::max< long long >( P.n_record - done, 0 );
         C.records = C.n_record > 0 ? P.records + done : nullptr;
-        launch_deferred_chunk< TALLY >( C, s );
+        launch_deferred_chunk< TALLY, false >( C, s );
     }
 }
 }   // namespace kp
@@ -1074,6 +1106,7 @@ extern "C" int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays )
             KP_CUDA( cudaFree( mesh->d_adj ) );
             mesh->d_adj = nullptr;
             mesh->adj_bytes = 0;
+            mesh->tape_id = 0;
         }
         mesh->pq_limit = max_rays;
     } );

@@ -111,6 +111,7 @@ struct fwd_params_t
     // deferred adjoint (kp_transport_adjoint): the tasks are the vertices'
     // peel-off rays, linked in vertex order per packet of the launch
     float     * adj_G;                  // [pq_cap] G of each task's ray
+    float     * adj_att;                // [pq_cap] taped solve: w exp(-tau) of each ray (-1: cut)
     int       * adj_head;               // [n_packets] first task of the packet, -1: none
     double    * adj_R0;                 // [n_packets] sum of G over its interactions
     int       * adj_flag;               // [n_packets] 1: the queue overflowed for it
@@ -123,9 +124,10 @@ struct fwd_params_t
 };
 
 // A peel-off ray waiting for k_peel: where it starts (the interaction or
-// emission point) and its pending contribution.  In the deferred adjoint
-// `cpix` holds the packet's next task (-1: last), `lp` the packet's index in
-// the launch and `kv` the vertex (0: emission).
+// emission point) and its pending contribution.  When the rays are linked
+// per packet (the deferred adjoint, a taped forward solve), `next` holds the
+// packet's next task (-1: last), `lp` the packet's index in the launch and
+// `kv` the vertex (0: emission).
 struct __align__( 16 ) peel_task_t
 {
     double x[ 3 ];
@@ -133,7 +135,7 @@ struct __align__( 16 ) peel_task_t
     float  w, I, Q, U, V;
     int    pix, cpix;
     int    lp, kv;
-    int    pad;
+    int    next;
 };
 
 // A packet's walk crossing into a block of another rank (it has entered the
@@ -745,6 +747,11 @@ int  persistent_grid( const void * kernel, int threads );
 void launch_peel_adjoint( const fwd_params_t & P, int tally_mode, int mode, cudaStream_t s );
 constexpr int PQ_PER_PACKET = 12;    // peel-off queue rays per packet of a solve
 void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets );
+// Points P's queue and deferred-adjoint fields at the mesh's buffers (grown
+// for chunks of n_pk packets), with their own counters: P.work is set to
+// them, so launches that use the mesh's workspace do not touch a tape.
+void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk );
+template< int TALLY, bool TAPE > void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s );
 void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int threads,
                      int grid_pct );
 

@@ -194,6 +194,12 @@ class Mesh:
         call("kp_mesh_remap", self.handle, other.handle, n_comp, ptr(src), ptr(dst), s)
         return dst if src.dim() > 1 else dst[:, 0]
 
+    def tape_id(self) -> int:
+        """Id of the taped forward solve the mesh holds (0: none)."""
+        tid = ctypes.c_longlong(0)
+        call("kp_mesh_tape_id", self.handle, ctypes.byref(tid))
+        return tid.value
+
     def status(self, stream=None) -> int:
         flags = ctypes.c_uint()
         call("kp_mesh_status", self.handle, stream, ctypes.byref(flags))

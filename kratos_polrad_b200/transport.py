@@ -164,13 +164,25 @@ class Tallies:
 
 
 def forward(mesh, cfg: TransportConfig, tallies: Tallies | None = None,
-            stream: int | None = None) -> Tallies:
-    """Runs ``cfg.n_packets`` packets through ``mesh``; returns the tallies."""
+            stream: int | None = None, tape: bool = False) -> Tallies:
+    """Runs ``cfg.n_packets`` packets through ``mesh``; returns the tallies.
+
+    With ``tape`` the mesh also keeps the solve's peel-off rays for a later
+    ``adjoint(..., tape_id=tallies.tape_id)``; ``tallies.tape_id`` is 0 when
+    the solve was too large to tape (more packets than one queue chunk).
+    """
     if tallies is None:
         tallies = Tallies(cfg)
     c, t = cfg.to_c(), tallies.to_c()
     s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
-    call("kp_transport_forward", mesh.handle, ctypes.byref(c), ctypes.byref(t), s)
+    tallies.tape_id = 0
+    if tape:
+        tid = ctypes.c_longlong(0)
+        call("kp_transport_forward_tape", mesh.handle, ctypes.byref(c), ctypes.byref(t), s,
+             ctypes.byref(tid))
+        tallies.tape_id = tid.value
+    else:
+        call("kp_transport_forward", mesh.handle, ctypes.byref(c), ctypes.byref(t), s)
     return tallies
 
 

@@ -1,0 +1,73 @@
+"""Taped forward solves and their gradients (kp_transport_forward_tape,
+kp_transport_adjoint_tape) against the untaped entry points, bit for bit.
+
+A taped solve is an ordinary forward solve that leaves each packet's
+peel-off rays and their attenuation in the mesh, so that the gradient of
+that solve skips the adjoint's first replay.  Its tallies must equal the
+plain solve's and its gradients the full adjoint's (int64 tallies: no
+tolerance), for several adjoint images per tape; the tape must be refused
+once anything replaced it.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from kratos_polrad_b200._lib import KP_ERR_CONFIG, KPError
+from kratos_polrad_b200.adjoint import adjoint
+from kratos_polrad_b200.transport import Tallies, forward
+from transport_cases import case
+
+pytestmark = pytest.mark.gpu
+
+
+def _adj(t, seed):
+    a = np.random.default_rng(seed).normal(size=(t.image_n, t.image_n, 4)).astype(np.float32)
+    return torch.tensor(a, device="cuda")
+
+
+@pytest.mark.parametrize("name", ["amr_point", "hg_multi"])
+def test_tape_matches_plain_solve_and_full_adjoint(name):
+    mesh, sig, t = case(name)
+    mesh.set_sigma(sig)
+    plain = forward(mesh, t)
+    taped = forward(mesh, t, Tallies(t), tape=True)
+    torch.cuda.synchronize()
+    assert taped.tape_id > 0 and mesh.tape_id() == taped.tape_id
+    for k in ("mu", "image", "image_batch", "counters", "records"):
+        assert torch.equal(getattr(taped, k), getattr(plain, k)), k
+    t0 = dataclasses.replace(t, n_record=0)
+    a1, a2 = _adj(t, 1), _adj(t, 2)
+    tape1 = adjoint(mesh, t0, a1, 24, tape_id=taped.tape_id)
+    tape2 = adjoint(mesh, t0, a2, 24, tape_id=taped.tape_id)      # same tape again
+    torch.cuda.synchronize()
+    assert mesh.status() == 0
+    full1 = adjoint(mesh, t0, a1, 24)                               # replaces the tape
+    full2 = adjoint(mesh, t0, a2, 24)
+    torch.cuda.synchronize()
+    assert mesh.tape_id() == 0
+    for x, y in zip(tape1 + tape2, full1 + full2):
+        assert torch.equal(x, y)
+
+
+def test_tape_is_dropped_by_new_coefficients_and_later_solves():
+    mesh, sig, t = case("amr_point")
+    t = dataclasses.replace(t, n_record=0)
+    mesh.set_sigma(sig)
+    tid = forward(mesh, t, tape=True).tape_id
+    assert tid > 0
+    mesh.set_sigma(sig)                                             # same values, new upload
+    assert mesh.tape_id() == 0
+    with pytest.raises(KPError) as e:
+        adjoint(mesh, t, _adj(t, 3), 24, tape_id=tid)
+    assert e.value.code == KP_ERR_CONFIG
+    tid2 = forward(mesh, t, tape=True).tape_id
+    assert tid2 > tid
+    forward(mesh, t)                                                # an untaped solve
+    assert mesh.tape_id() == 0
+    # a cfg that is not the taped solve's
+    tid3 = forward(mesh, t, tape=True).tape_id
+    with pytest.raises(KPError) as e:
+        adjoint(mesh, dataclasses.replace(t, seed=t.seed + 1), _adj(t, 3), 24, tape_id=tid3)
+    assert e.value.code == KP_ERR_CONFIG
