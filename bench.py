@@ -670,10 +670,34 @@ def main():
         torch.cuda.synchronize()
         adj_ms.append(a0.elapsed_time(a1))
     ac = adj_cnt.cpu().numpy()
+    # the gradient of a taped forward solve (an autograd step): forward with
+    # the tape kept, then the adjoint from the tape; gradients checked equal
+    g_full = run_adjoint(mesh, cfg, adj_img, 24)
+    tape_fwd_ms, tape_adj_ms, tape_same = [], [], True
+    tal_t = Tallies(cfg)
+    for k in range(max(1, min(args.steps, 3))):
+        tal_t.zero_()
+        flush.fill_(float(k))
+        t0, t1, t2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        t0.record()
+        forward(mesh, cfg, tal_t, tape=True)
+        t1.record()
+        g_tape = run_adjoint(mesh, cfg, adj_img, 24, tape_id=tal_t.tape_id)
+        t2.record()
+        torch.cuda.synchronize()
+        tape_fwd_ms.append(t0.elapsed_time(t1))
+        tape_adj_ms.append(t1.elapsed_time(t2))
+        tape_same = tape_same and tal_t.tape_id > 0 and all(
+            torch.equal(x, y) for x, y in zip(g_tape, g_full))
     adjoint_info = {"ms_per_solve": statistics.mean(adj_ms),
                     "cost_vs_forward": statistics.mean(adj_ms) / statistics.mean(kern_ms),
                     "packet_steps_per_s": float(ac[0] + ac[1]) / (statistics.mean(adj_ms) / 1e3),
-                    "note": "two replays per packet (measure, deposit); same packets as the forward"}
+                    "note": "two replays per packet (measure, deposit); same packets as the forward",
+                    "taped": {"forward_ms": statistics.mean(tape_fwd_ms),
+                              "gradient_ms": statistics.mean(tape_adj_ms),
+                              "gradients_equal_full_adjoint": tape_same,
+                              "note": "forward with its peel-off rays kept, then the adjoint "
+                                      "from them (autograd step)"}}
 
     # ---- end to end through the C ABI with host buffers ----
     import ctypes

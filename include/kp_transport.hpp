@@ -258,6 +258,24 @@ struct transport
         api( kp_transport_adjoint( m.get(  ), & c, adj_image, grad_fx_shift, grad_len, grad_int,
                                    counters, s ) );
     }
+    // Forward solve that keeps its peel-off rays for adjoint_tape; returns
+    // the tape id (0: too many packets to tape, an untaped solve ran).
+    static long long forward_tape( mesh_t & m, const kp_transport_cfg_t & c,
+                                   const kp_tallies_t & t, stream_t s = nullptr )
+    {
+        long long id = 0;
+        api( kp_transport_forward_tape( m.get(  ), & c, & t, s, & id ) );
+        return id;
+    }
+    // adjoint() of the taped solve `tape_id`, from its tape.
+    static void adjoint_tape( mesh_t & m, long long tape_id, const kp_transport_cfg_t & c,
+                              const float * adj_image, int grad_fx_shift, void * grad_len,
+                              void * grad_int, unsigned long long * counters = nullptr,
+                              stream_t s = nullptr )
+    {
+        api( kp_transport_adjoint_tape( m.get(  ), tape_id, & c, adj_image, grad_fx_shift,
+                                        grad_len, grad_int, counters, s ) );
+    }
     static void trace( mesh_t & m, int precision, long long n, void * x, const void * dir,
                        int * cell, int * ib, const void * proper, int * step, int8_t * todo,
                        int flux_mode, int fx_shift, void * flux, stream_t s = nullptr )
