@@ -604,13 +604,14 @@ k_forward( const __grid_constant__ fwd_params_t P )
 // and its block's origin and spacing (the next face is computed from them,
 // with exit_dist's expression, without a load).
 // MODE 0 deposits each ray into the image (forward solve); MODE 3 does the
-// same and keeps each ray's attenuation w exp(-tau) (-1 beyond the cut) in
-// adj_att for the adjoint of a taped solve.  The deferred
-// adjoint marches the same tasks twice: MODE 1 measures each ray's score G
-// (what the image deposit would be worth to the loss) into adj_G, MODE 2
-// deposits -G * length into the path-length gradient along each segment
-// inside the depth cut; both skip the tasks of packets left to k_adjoint,
-// and MODE 2 the rays with G = 0.
+// same and keeps, for the adjoint of a taped solve, each ray's attenuation
+// w exp(-tau) (-1 beyond the cut) in adj_att and the number of its segments
+// inside the depth cut in the task's cpix.  The deferred adjoint marches the
+// same tasks twice: MODE 1 measures each ray's score G (what the image
+// deposit would be worth to the loss) into adj_G and its segments inside the
+// cut into cpix; MODE 2 walks exactly those segments again, by geometry
+// alone, depositing -G * length into the path-length gradient.  Both skip
+// the tasks of packets left to k_adjoint, and MODE 2 the rays with G = 0.
 template< int TALLY, int MODE >
 __global__ void __launch_bounds__( 256, MODE == 2 ? 3 : KP_PEEL_MINB )
 k_peel( const __grid_constant__ fwd_params_t P )
@@ -628,6 +629,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
     const float2 * sb = P.m.sigma;                // this block's coefficients
     float  ptau = 0.0f;
     float  pG = 0.0f;                             // MODE 2: the ray's score
+    int    n_dep = 0;                             // MODE 2: ... and its segments
     // MODE 2: every ray leaves toward the observer along the same corridor of
     // cells, so the blocks deposit into private copies (summed afterwards)
     // rather than all into one tally
@@ -688,7 +690,10 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 }
                 if constexpr( MODE == 3 )
                     if( task >= 0 )
+                    {   // for the adjoint: attenuation, segments inside the cut
                         P.adj_att[ task ] = att;
+                        P.pq[ task ].cpix = ptau > P.tau_cut ? pk - 1 : pk;
+                    }
                 const unsigned m_dep = __ballot_sync( m_fetch, dep );
                 if( ( int ) lane == leader && m_dep )
                     atomicAdd( cnt_s + KP_CNT_DEPOSITS, ( unsigned long long ) __popc( m_dep ) );
@@ -705,6 +710,8 @@ k_peel( const __grid_constant__ fwd_params_t P )
                                    __fmul_rn( att, o.U ), __fmul_rn( att, o.V ) );
                     }
                     P.adj_G[ task ] = G;
+                    // the segments inside the cut: what the depositing march walks
+                    P.pq[ task ].cpix = ptau > P.tau_cut ? pk - 1 : pk;
                 }
             task = -1;
             const unsigned rank = __popc( m_fetch & ( ( 1u << lane ) - 1u ) );
@@ -726,7 +733,8 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 if constexpr( MODE == 2 )
                 {
                     pG = P.adj_G[ idx ];
-                    if( pG == 0.0f )
+                    n_dep = o.cpix;
+                    if( pG == 0.0f || n_dep <= 0 )
                         continue;
                 }
             }
@@ -763,21 +771,32 @@ k_peel( const __grid_constant__ fwd_params_t P )
         #pragma unroll 1
         for( int it = 0; it < KP_PEEL_INNER; ++ it )
         {
-            const float2 sg = sb[ ci ];
-            const float ext = __fadd_rn( sg.x, sg.y );
             int ax;
             const double t = exit_cached( x, fx, P.o, P.inv_o, ax );
             ++ n_seg_done;
             ++ pk;
-            ptau = __fadd_rn( ptau, __fmul_rn( ext, ( float ) t ) );
-            if( ptau > P.tau_cut )
-            {
-                phase = PH_EMIT;
-                break;
-            }
             if constexpr( MODE == 2 )
+            {   // the measuring march counted the segments inside the cut:
+                // geometry only, no coefficients
                 add_grad< TALLY >( g_dep, ( size_t ) ( sb - P.m.sigma ) + ci,
                                    __dmul_rn( -( double ) pG, t ), P.g_scale );
+                if( pk >= n_dep )
+                {
+                    phase = PH_EMIT;
+                    break;
+                }
+            }
+            else
+            {
+                const float2 sg = sb[ ci ];
+                const float ext = __fadd_rn( sg.x, sg.y );
+                ptau = __fadd_rn( ptau, __fmul_rn( ext, ( float ) t ) );
+                if( ptau > P.tau_cut )
+                {
+                    phase = PH_EMIT;
+                    break;
+                }
+            }
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
                 if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
