@@ -305,14 +305,18 @@ int kp_batch_autotune( kp_batch_t * b, const kp_transport_cfg_t * cfg, double fr
         const int shapes[ ][ 3 ] = { { 256, 6, 100 }, { 256, 4, 100 }, { 256, 8, 100 },
                                      { 256, 12, 100 }, { 128, 6, 100 }, { 128, 8, 100 },
                                      { 256, 6, 75 }, { 128, 4, 100 } };
-        float best = 1e30f;
-        int bi = 0;
+        constexpr int n_shapes = ( int ) ( sizeof( shapes ) / sizeof( shapes[ 0 ] ) );
+        float t_min[ n_shapes ];
+        for( int i = 0; i < n_shapes; ++ i ) t_min[ i ] = 1e30f;
         try
         {
             kp_transport_cfg_t c = * cfg;
             c.lane_batch = 0;
-            for( int rep = 0; rep < 2; ++ rep )        // first pass warms up
-                for( int i = 0; i < ( int ) ( sizeof( shapes ) / sizeof( shapes[ 0 ] ) ); ++ i )
+            // the first pass warms up; each shape keeps its best of three
+            // timed passes (candidates differ by a few percent, a single
+            // timing by about as much)
+            for( int rep = 0; rep < 4; ++ rep )
+                for( int i = 0; i < n_shapes; ++ i )
                 {
                     b->threads = shapes[ i ][ 0 ];
                     b->lane_batch = shapes[ i ][ 1 ];
@@ -325,7 +329,7 @@ int kp_batch_autotune( kp_batch_t * b, const kp_transport_cfg_t * cfg, double fr
                     KP_CUDA( cudaEventSynchronize( e1 ) );
                     float ms = 0;
                     KP_CUDA( cudaEventElapsedTime( & ms, e0, e1 ) );
-                    if( rep == 1 && ms < best ) { best = ms; bi = i; }
+                    if( rep > 0 && ms < t_min[ i ] ) t_min[ i ] = ms;
                 }
         }
         catch( ... )
@@ -337,6 +341,10 @@ int kp_batch_autotune( kp_batch_t * b, const kp_transport_cfg_t * cfg, double fr
         b->prefix = saved;
         cudaEventDestroy( e0 );
         cudaEventDestroy( e1 );
+        int bi = 0;
+        for( int i = 1; i < n_shapes; ++ i )
+            if( t_min[ i ] < t_min[ bi ] ) bi = i;
+        const float best = t_min[ bi ];
         b->threads = shapes[ bi ][ 0 ];
         b->lane_batch = shapes[ bi ][ 1 ];
         b->grid_pct = shapes[ bi ][ 2 ];
