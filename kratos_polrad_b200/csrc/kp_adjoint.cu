@@ -932,14 +932,14 @@ extern "C" int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_c
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         if( P.n_packets == 0 ) return;
+        if( cfg->lane_batch == 0 ) P.ev_batch = 12;
         kp::ensure_peel_queue( mesh, P.n_packets );
         if( P.n_packets > std::max< long long >( mesh->pq_cap / kp::PQ_PER_PACKET, 1 ) )
         {   // more packets than one chunk of the queue: an untaped solve
-            kp::require( kp_transport_forward( mesh, cfg, tallies, stream ) == KP_OK,
-                         kp_last_error(  ), KP_ERR_CUDA );
+            P.work = mesh->workspace(  );
+            kp::launch_deferred_solve( mesh, P, cfg->tally_mode, ( cudaStream_t ) stream );
             return;
         }
-        if( cfg->lane_batch == 0 ) P.ev_batch = 12;
         kp::adjoint_buffers( mesh, P, P.n_packets );
         auto s = ( cudaStream_t ) stream;
         KP_CUDA( cudaMemsetAsync( P.work, 0, 4 * sizeof( unsigned long long ), s ) );

@@ -1083,6 +1083,13 @@ void launch_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
         launch_deferred_chunk< TALLY, false >( C, s );
     }
 }
+
+void launch_deferred_solve( kp_mesh_t * mesh, const fwd_params_t & P, int tally_mode,
+                            cudaStream_t s )
+{
+    if( tally_mode == KP_TALLY_FIXED ) launch_deferred< KP_TALLY_FIXED >( mesh, P, s );
+    else                               launch_deferred< KP_TALLY_FLOAT >( mesh, P, s );
+}
 }   // namespace kp
 
 extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,

@@ -752,6 +752,9 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets );
 // them, so launches that use the mesh's workspace do not touch a tape.
 void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk );
 template< int TALLY, bool TAPE > void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s );
+// A forward solve with its peel-off rays queued for k_peel, in chunks (no tape).
+void launch_deferred_solve( kp_mesh_t * mesh, const fwd_params_t & P, int tally_mode,
+                            cudaStream_t s );
 void launch_forward( const fwd_params_t & P, int tally_mode, cudaStream_t s, int threads,
                      int grid_pct );
 

@@ -71,3 +71,36 @@ def test_tape_is_dropped_by_new_coefficients_and_later_solves():
     with pytest.raises(KPError) as e:
         adjoint(mesh, dataclasses.replace(t, seed=t.seed + 1), _adj(t, 3), 24, tape_id=tid3)
     assert e.value.code == KP_ERR_CONFIG
+
+
+def test_tape_with_overflowing_queue_matches_full_adjoint():
+    """A 1024-ray queue and a thick slab (vertical tau 20, albedo 1: far more
+    than 12 rays per packet): the taped solve flags the packets whose rays
+    found the queue full, and their gradients come from k_adjoint.  Taped
+    tallies equal the plain solve's, tape gradients the full adjoint's."""
+    from kratos_polrad_b200._lib import call
+    mesh, sig, t = case("slab")
+    sig = sig * 10.0
+    t = dataclasses.replace(t, n_packets=85, n_record=0, image_n=16, inclination_deg=60.0,
+                            image_center=(16.0, 16.0, 8.0), image_half_width=24.0)
+    mesh.set_sigma(sig)
+    call("kp_mesh_peel_queue_limit", mesh.handle, 1024)
+    try:
+        plain = forward(mesh, t)
+        taped = forward(mesh, t, Tallies(t), tape=True)
+        torch.cuda.synchronize()
+        assert taped.tape_id > 0
+        for k in ("mu", "image", "image_batch", "counters"):
+            assert torch.equal(getattr(taped, k), getattr(plain, k)), k
+        # every interaction projects into the image (it covers the slab), so
+        # more rays than the queue holds: some packets were flagged
+        assert int(plain.counters[2]) > 1024
+        a = _adj(t, 5)
+        tape = adjoint(mesh, t, a, 24, tape_id=taped.tape_id)
+        full = adjoint(mesh, t, a, 24)
+        torch.cuda.synchronize()
+        assert mesh.status() == 0
+    finally:
+        call("kp_mesh_peel_queue_limit", mesh.handle, 1 << 27)
+    for x, y in zip(tape, full):
+        assert torch.equal(x, y)
