@@ -20,6 +20,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import dataclasses
+import math
 import json
 import os
 import statistics
@@ -44,7 +45,8 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--packets", type=float, default=1e7)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="clump", choices=["clump", "batched", "diff", "large", "decomp"])
+    p.add_argument("--workload", default="clump",
+                   choices=["clump", "batched", "diff", "large", "decomp", "trace", "sph"])
     return p.parse_args()
 
 
@@ -509,6 +511,150 @@ def run_decomp(args):
     _finish_ranks(world)
 
 
+def _walk_bench(args, spherical):
+    """Reference-semantics walks (kp_trace: cart_t::proc; kp_trace_sph:
+    sph_t::proc) on GPU against the reference's own code compiled for the
+    host (oracle/_ref).  Packets start uniformly in the domain with
+    isotropic directions and walk to its boundary or for 4096 steps, one
+    int64 path-length flux deposit per step.  Per precision (float_t of the
+    reference's PRECISION=1 and 2): device time of the walk (pool restored
+    before each step, outside the timed region), the final states of a
+    sample against the reference's (identical packets), and the reference
+    on all host cores over that sample."""
+    import os
+    import time
+    import numpy as np
+    import torch
+    from kratos_polrad_b200 import Mesh, PacketPool, scenes
+    from kratos_polrad_b200.trace import TO_KEEP, trace as gpu_trace, trace_sph as gpu_trace_sph
+    from oracle import refharness
+    two_pi = 2 * math.pi
+    if spherical:
+        from kratos_polrad_b200.mesh import MeshConfig, RefineRegion
+        mcfg = MeshConfig((0.5, 0.4, 0.0), (2.5, 2.7, two_pi), (64, 64, 128), (16, 16, 16),
+                          (False, False, True),
+                          [RefineRegion(1, (1.0, 1.0, 2.0), (1.6, 1.8, 3.6)),
+                           RefineRegion(2, (1.1, 1.2, 2.5), (1.3, 1.4, 3.0))])
+        ratio = 1.0
+        mesh = Mesh(mcfg, spherical=True, r_ratio=ratio)
+        ini = mcfg.to_ini().replace("[boundary]", f"r_ratio = {ratio!r}\n\n[boundary]", 1)
+        name, metric = "trace_sph", "packet-steps/s, spherical-polar walk (sph_t::proc)"
+    else:
+        mcfg = scenes.clump_mesh_config()
+        mesh = Mesh(mcfg)
+        ini = mcfg.to_ini()
+        name, metric = "trace_clump_mesh", "packet-steps/s, reference-semantics walk (cart_t::proc)"
+    n = int(args.packets) if args.packets != 1e7 else 1 << 23
+    dev = torch.device("cuda")
+    lo, hi = np.array(mcfg.x_min, float), np.array(mcfg.x_max, float)
+    per = {}
+    for prec in (1, 2):
+        ftype, tdt = (np.float32, torch.float32) if prec == 1 else (np.float64, torch.float64)
+        rng = np.random.default_rng(17 + prec)
+        pad = np.array([0.01, 0.05, 0.0]) * (hi - lo) if spherical else np.zeros(3)
+        x = lo + pad + rng.random((n, 3)) * (hi - lo - 2 * pad)
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        x, d = x.astype(ftype), d.astype(ftype)
+        ib, cell = mesh.locate(x.astype(np.float64))
+        proper = (rng.random(n) + 0.5).astype(ftype)
+        # a finite budget: a few packets of the spherical walk stall at cell
+        # corners (the reference's own walk does the same) until it runs out
+        steps = np.full(n, 4096, np.int32)
+        T = lambda a, dt=None: torch.tensor(a, dtype=dt, device=dev)
+        orig = [T(x, tdt), T(d, tdt), T(cell), T(ib), T(proper, tdt), T(steps)]
+        pool = PacketPool(*[o.clone() for o in orig])
+        if spherical:
+            r, th, ph = (x[:, k].astype(np.float64) for k in range(3))
+            xc = np.stack([r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)], 1)
+            xc0 = T(xc.astype(ftype), tdt)
+            x_car = xc0.clone()
+        flux = torch.zeros(mesh.n_cells, dtype=torch.int64, device=dev)
+
+        def restore():
+            for dst, src in zip((pool.x, pool.dir, pool.cell, pool.ib, pool.proper, pool.step), orig):
+                dst.copy_(src)
+            pool.todo.fill_(TO_KEEP)
+            if spherical:
+                x_car.copy_(xc0)
+            flux.zero_()
+
+        def walk():
+            if spherical:
+                gpu_trace_sph(mesh, pool, x_car, "fixed", 16, flux)
+            else:
+                gpu_trace(mesh, pool, "fixed", 32, flux)
+
+        for _ in range(max(1, args.warmup)):
+            restore(); walk()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(); walk(); e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        status = mesh.status()
+        done = int((orig[5].long() - pool.step.long()).sum())
+        value = done / (statistics.mean(ms) / 1e3)
+        # the reference on the host: a sample of the same packets, all cores
+        entry = {"value": value, "ms": statistics.mean(ms), "steps": done, "status": status}
+        if refharness.available(prec):
+            ref = (refharness.RefMeshSph if spherical else refharness.RefMesh)(ini, prec)
+            pl, pr = mesh.blocks()
+            rl, rr = ref.blocks()
+            key = {(int(l), *map(int, q)): i for i, (l, q) in enumerate(zip(pl, pr))}
+            perm = np.array([key[(int(l), *map(int, q))] for l, q in zip(rl, rr)])
+            inv = np.argsort(perm)
+            cores = os.cpu_count() or 1
+            refharness.deposits_outside(prec)          # reset the harness's count
+            m = min(n, 1 << 17)
+            for it in range(3):                 # grow the sample to about 1.5 s
+                sel = slice(0, m)
+                t0 = time.perf_counter()
+                if spherical:
+                    rres = ref.trace(x[sel], xc[sel], d[sel], cell[sel], inv[ib[sel]], proper[sel],
+                                     steps[sel], fx_shift=16, n_threads=cores)
+                else:
+                    rres = ref.trace(x[sel], d[sel], cell[sel], inv[ib[sel]], proper[sel],
+                                     steps[sel], fx_shift=32, n_threads=cores)
+                dt = time.perf_counter() - t0
+                if dt >= 1.0 or m == n or it == 2:
+                    break
+                m = min(n, int(m * 1.5 / max(dt, 1e-3)))
+            rib = rres["ib"]
+            # the same walk: cells, blocks, steps and end flags; positions are
+            # bit-identical for the Cartesian walk and within the float
+            # transcendentals' ulps for the spherical one (cos/sin/acos/atan2)
+            walk = ((pool.cell[:m].cpu().numpy() == rres["cell"]).all(1)
+                    & (pool.ib[:m].cpu().numpy() == np.where(rib >= 0, perm[np.maximum(rib, 0)], rib))
+                    & (pool.step[:m].cpu().numpy() == rres["step"])
+                    & (pool.todo[:m].cpu().numpy().astype(np.int32) == rres["todo"]))
+            xs = pool.x[:m].cpu().numpy().astype(np.float64)
+            bit = walk & (xs == rres["x"]).all(1)
+            rel = np.abs(xs[walk] - rres["x"][walk]) / np.maximum(np.abs(rres["x"][walk]), 1e-6)
+            rsteps = int((steps[:m].astype(np.int64) - rres["step"]).sum())
+            entry["parity"] = {"packets": m, "same_walk": float(walk.mean()),
+                               "bit_identical_final_state": float(bit.mean()),
+                               "position_rel_diff_q99_same_walk": float(np.quantile(rel, 0.99))
+                               if rel.size else 0.0,
+                               "reference_deposits_beyond_flux_pool_skipped":
+                                   refharness.deposits_outside(prec)}
+            entry["cpu_baseline"] = {"value": rsteps / dt, "unit": "packet-steps/s", "cores": cores,
+                                     "kind": "reference",
+                                     "sample": f"packets 0..{m - 1} of the same set, {rsteps:.3g} "
+                                               f"packet-steps in {dt:.2f} s"}
+        per[str(prec)] = entry
+    line = {"metric": metric, "unit": "packet-steps/s", "value": per["1"]["value"],
+            "higher_is_better": True, "n_gpus": 1,
+            "config": {"workload": name, "packets": n, "blocks": mesh.n_blocks,
+                       "cells": mesh.n_cells, "budget": "to the domain boundary, at most 4096 steps",
+                       "flux": "int64 fixed point", "value_precision": "PRECISION=1 (float_t float)"},
+            "precisions": per}
+    print(json.dumps(line), flush=True)
+
+
 def run_large(args):
     """Large workload: 256^3 root, 3 levels on a lognormal field (std of ln
     rho 1.5, seed 5; ~2e7 cells, 166 MB of coefficients: beyond L2), HG g=0.6
@@ -556,6 +702,8 @@ def main():
         return run_large(args)
     if args.workload == "decomp":
         return run_decomp(args)
+    if args.workload in ("trace", "sph"):
+        return _walk_bench(args, args.workload == "sph")
     if args.impl == "reference":     # host cores only: rank 0 runs, the others exit
         run_reference(args, int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)))
         return

@@ -43,6 +43,23 @@ def root_refine_boxes(field_fn, n_root, block, box_lo, box_hi, threshold, level=
     return boxes
 
 
+def clump_mesh_config(n_root=128, block=16, peak=100.0, fwhm=0.1) -> MeshConfig:
+    """Mesh of the 2-level AMR clump: root n_root^3 in block^3, refined x2
+    where the Gaussian clump's density (peak, FWHM in box units, on a unit
+    background) exceeds 3x its mean."""
+    s = fwhm / (2.0 * math.sqrt(2.0 * math.log(2.0)))
+
+    def rho(x):
+        r2 = ((np.asarray(x) - 0.5) ** 2).sum(-1)
+        return 1.0 + (peak - 1.0) * np.exp(-r2 / (2 * s * s))
+
+    n3 = (n_root,) * 3
+    g = (np.arange(n_root) + 0.5) / n_root
+    mean = (1.0 + (peak - 1.0) * np.exp(-((g - 0.5) ** 2) / (2 * s * s)).mean() ** 3)
+    boxes = root_refine_boxes(rho, n3, (block,) * 3, (0, 0, 0), (1, 1, 1), 3.0 * mean)
+    return MeshConfig((0, 0, 0), (1, 1, 1), n3, (block,) * 3, (False,) * 3, boxes)
+
+
 def clump_amr(n_packets=10_000_000, n_root=128, block=16, peak=100.0, fwhm=0.1, tau_edge=5.0,
               albedo=(0.5, 0.99), seed=2, image_n=128, inclination=90.0):
     """Static 2-level AMR clump: root n_root^3 in block^3, refined x2 where the
@@ -56,11 +73,7 @@ def clump_amr(n_packets=10_000_000, n_root=128, block=16, peak=100.0, fwhm=0.1, 
         r2 = ((np.asarray(x) - 0.5) ** 2).sum(-1)
         return 1.0 + (peak - 1.0) * np.exp(-r2 / (2 * s * s))
 
-    n3 = (n_root,) * 3
-    g = (np.arange(n_root) + 0.5) / n_root
-    mean = (1.0 + (peak - 1.0) * np.exp(-((g - 0.5) ** 2) / (2 * s * s)).mean() ** 3)
-    boxes = root_refine_boxes(rho, n3, (block,) * 3, (0, 0, 0), (1, 1, 1), 3.0 * mean)
-    mesh = Mesh(MeshConfig((0, 0, 0), (1, 1, 1), n3, (block,) * 3, (False,) * 3, boxes))
+    mesh = Mesh(clump_mesh_config(n_root, block, peak, fwhm))
     c = cell_centers(mesh)
     # extinction coefficient: integral of kappa*rho from the centre to a face = tau_edge
     col = 0.5 + (peak - 1.0) * s * math.sqrt(math.pi / 2) * math.erf(0.5 / (s * math.sqrt(2)))

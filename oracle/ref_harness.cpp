@@ -121,6 +121,7 @@ struct harness_t
     bmap_t                          bmap;
     std::vector< f_t >              flux;       // reference float sums
     std::vector< long long >        flux_fx;    // int64 fixed point sums
+    std::atomic< long long >        n_outside { 0 };  // deposits beyond the flux pool
     std::vector< f_t >              sigma;      // 2 comps per cell (mfp_i)
     int                             fx_shift = 32;
     int                             n_cell_blk = 0;
@@ -162,6 +163,12 @@ static inline void deposit_impl( f_t * p, f_t v )
 {
     auto & h = * g_h;
     const ptrdiff_t k = p - h.flux.data(  );
+    if( k < 0 || k >= ( ptrdiff_t ) h.flux.size(  ) )
+    {   // the spherical walk deposits with an out-of-range cell index after
+        // some corner crossings; beyond the pool it would corrupt the heap
+        h.n_outside.fetch_add( 1, std::memory_order_relaxed );
+        return;
+    }
     const long long q = std::llrint( std::ldexp( ( double ) v, h.fx_shift ) );
     if( h.serial )
         h.flux[ k ] += v;           // packet order, as one host thread
@@ -326,6 +333,12 @@ int kpref_mesh_load( const char * ini_path )
 }
 
 int kpref_n_blocks( void ) { return g_h ? ( int ) g_h->blocks.size(  ) : 0; }
+
+// Deposits since the last call whose cell lay beyond the flux pool (skipped).
+long long kpref_deposits_outside( void )
+{
+    return g_h ? g_h->n_outside.exchange( 0 ) : 0;
+}
 
 int kpref_block_cells( int * n3 )
 {

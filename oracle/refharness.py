@@ -108,6 +108,14 @@ class RefMesh:
         return out
 
 
+def deposits_outside(precision: int) -> int:
+    """Reference deposits skipped since the last call because their cell lay
+    beyond the flux pool (the spherical walk after some corner crossings)."""
+    L = RefMesh._lib_for(precision)
+    L.kpref_deposits_outside.restype = ctypes.c_longlong
+    return int(L.kpref_deposits_outside())
+
+
 class RefMeshSph(RefMesh):
     """Spherical-polar mesh built by the reference's meshgen::sph_t; axes
     (r, theta, phi); [mesh] r_ratio sets the radial spacing."""
