@@ -46,7 +46,8 @@ def parse():
     p.add_argument("--packets", type=float, default=1e7)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="clump",
-                   choices=["clump", "batched", "diff", "large", "decomp", "trace", "sph"])
+                   choices=["clump", "batched", "diff", "large", "decomp", "trace", "sph",
+                            "refine", "bio"])
     return p.parse_args()
 
 
@@ -655,6 +656,95 @@ def _walk_bench(args, spherical):
     print(json.dumps(line), flush=True)
 
 
+def run_refine(args):
+    """Runtime refinement of the clump scene: per-block flags from the
+    extinction depth across a cell (device), the refined and coarsened mesh
+    with 2:1 balance and neighbour tables (host), its upload, and the
+    coefficients carried onto it (device)."""
+    import time
+    import torch
+    from kratos_polrad_b200 import scenes
+    mesh, sig, cfg = scenes.clump_amr(n_packets=1)
+    mesh.set_sigma(sig)
+    dev = torch.device("cuda")
+    src = torch.tensor(sig, device=dev)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    res = {}
+    for k in range(max(1, args.warmup) + args.steps):
+        e0, e1, e2, e3 = ev(), ev(), ev(), ev()
+        e0.record()
+        flags = mesh.flag_tau(0.1, 0.02)
+        e1.record()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fine = mesh.adapt(flags)
+        t1 = time.perf_counter()
+        fine.upload()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        e2.record()
+        dst = mesh.remap_to(fine, src)
+        e3.record()
+        torch.cuda.synchronize()
+        if k >= max(1, args.warmup):
+            for key, v in (("flag_ms", e0.elapsed_time(e1)), ("adapt_host_ms", (t1 - t0) * 1e3),
+                           ("upload_ms", (t2 - t1) * 1e3), ("remap_ms", e2.elapsed_time(e3))):
+                res.setdefault(key, []).append(v)
+    f = flags.cpu().numpy()
+    out = {k: statistics.mean(v) for k, v in res.items()}
+    total = sum(out.values())
+    line = {"metric": "runtime refinement step, 2-level AMR clump", "unit": "ms", "value": total,
+            "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": "refine_clump", "blocks": mesh.n_blocks, "cells": mesh.n_cells,
+                       "tau_refine": 0.1, "tau_coarsen": 0.02},
+            "flagged_refine": int((f > 0).sum()), "flagged_coarsen": int((f < 0).sum()),
+            "blocks_after": fine.n_blocks, "cells_after": fine.n_cells, **out,
+            "remap_cells_per_s": fine.n_cells / (out["remap_ms"] / 1e3),
+            "finite": bool(torch.isfinite(dst).all()),
+            # the remap copies where a new cell lies in one old cell and
+            # averages octants elsewhere: the field's range is kept
+            "range_kept": bool(dst.min() >= src.min() and dst.max() <= src.max())}
+    print(json.dumps(line), flush=True)
+
+
+def run_bio(args):
+    """The binary container (the reference's binary_io format): a clump
+    solution (block keys, per-block flux fields, coefficients, tallies,
+    config) written and read back, byte sizes and rates, values checked."""
+    import tempfile
+    import time
+    import numpy as np
+    import torch
+    from kratos_polrad_b200 import bio, scenes
+    from kratos_polrad_b200.transport import forward
+    mesh, sig, cfg = scenes.clump_amr(n_packets=1_000_000)
+    mesh.set_sigma(sig)
+    tal = forward(mesh, cfg)
+    torch.cuda.synchronize()
+    flux = (sig[:, 0].astype(np.float64) + sig[:, 1])
+    wr, rd, ok = [], [], True
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "solution.bin")
+        for k in range(max(1, args.warmup) + args.steps):
+            t0 = time.perf_counter()
+            bio.save_solution(path, mesh, sig, tal, cfg, flux=flux)
+            t1 = time.perf_counter()
+            got = bio.load_solution(path)
+            t2 = time.perf_counter()
+            if k >= max(1, args.warmup):
+                wr.append(t1 - t0)
+                rd.append(t2 - t1)
+            ok = ok and np.array_equal(got["sigma"], sig) and np.array_equal(
+                got["image"], tal.image.cpu().numpy())
+        size = os.path.getsize(path)
+    line = {"metric": "binary container write + read, clump solution", "unit": "MB/s",
+            "value": size / 1e6 / statistics.mean(wr), "higher_is_better": True, "n_gpus": 1,
+            "config": {"workload": "bio_clump", "bytes": size, "blocks": mesh.n_blocks},
+            "write_ms": statistics.mean(wr) * 1e3, "read_ms": statistics.mean(rd) * 1e3,
+            "read_mb_per_s": size / 1e6 / statistics.mean(rd), "values_equal": bool(ok)}
+    print(json.dumps(line), flush=True)
+
+
 def run_large(args):
     """Large workload: 256^3 root, 3 levels on a lognormal field (std of ln
     rho 1.5, seed 5; ~2e7 cells, 166 MB of coefficients: beyond L2), HG g=0.6
@@ -704,6 +794,10 @@ def main():
         return run_decomp(args)
     if args.workload in ("trace", "sph"):
         return _walk_bench(args, args.workload == "sph")
+    if args.workload == "refine":
+        return run_refine(args)
+    if args.workload == "bio":
+        return run_bio(args)
     if args.impl == "reference":     # host cores only: rank 0 runs, the others exit
         run_reference(args, int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)))
         return
