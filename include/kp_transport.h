@@ -326,7 +326,11 @@ typedef struct kp_tallies
 } kp_tallies_t;
 
 /* Asynchronous on `stream`.  Calls that share a mesh handle must not
- * overlap on the GPU (they share the mesh's packet counter). */
+ * overlap on the GPU (they share the mesh's packet counter and peel-off
+ * queue).  With an image, the first solve of a mesh allocates its peel-off
+ * queue: 80 B per ray, 12 rays per packet, at most kp_mesh_peel_queue_limit
+ * rays (default 2^27, 10.7 GB); later solves reuse it, and the mesh frees it
+ * with the mesh. */
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
