@@ -420,7 +420,10 @@ int kp_batch_autotune( kp_batch_t * batch, const kp_transport_cfg_t * cfg, doubl
  * marches measure their scores and deposit along them; packets whose rays
  * do not fit the queue (kp_mesh_peel_queue_limit) are replayed with their
  * rays inline, with the same results.  counters (optional) receives the
- * KP_CNT_* counts of both replays. */
+ * KP_CNT_* counts of both replays.  Besides the queue, the mesh keeps the
+ * adjoint's buffers from the first call on: 8 B per queued ray, 20 B per
+ * packet of a chunk, and 8 private int64 path-length tallies (64 B per
+ * cell). */
 int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const float * adj_image, int grad_fx_shift,
                           void * grad_len, void * grad_int,
