@@ -38,6 +38,9 @@ namespace cg = cooperative_groups;
 #ifndef KP_PEEL_BATCH
 #define KP_PEEL_BATCH 24             // k_peel: lanes that wait for a fetch batch
 #endif
+#ifndef KP_HOP_BATCH
+#define KP_HOP_BATCH 6               // lanes that wait for a batched block hand-off
+#endif
 #ifndef KP_PEEL_INNER
 #define KP_PEEL_INNER 8              // k_peel: segments per scheduling round
 #endif
@@ -907,10 +910,11 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     P.max_scatter = c.max_scatter;
     P.max_steps = std::min< long long >( c.max_steps, 0x7fffffff );
     P.ev_batch = c.lane_batch > 0 ? c.lane_batch : 6;
-    // Block hand-offs wait for 8 lanes (measured best on AMR and on uniform
-    // scenes, whatever the event batch): the neighbour lookup and the new
-    // block's geometry are dependent loads, paid once per batch.
-    P.hop_batch = 8;
+    // Block hand-offs wait for a batch of lanes (6 measured best for the
+    // deferred walk and the peel-off march, 8 for the single-kernel walk
+    // before it): the neighbour lookup and the new block's geometry are
+    // dependent loads, paid once per batch.
+    P.hop_batch = KP_HOP_BATCH;
     P.peel_batch = KP_PEEL_BATCH;
     P.mu_tally = t.mu;
     P.image = t.image;
