@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define KP_ABI_VERSION 1
+#define KP_ABI_VERSION 2
 
 enum kp_status
 {
@@ -292,6 +292,10 @@ typedef struct kp_transport_cfg
     long long n_record;        /* final-state records for the first n packets  */
     int       lane_batch;      /* scheduling: lanes of a warp that wait for an
                                   interaction or emission batch (0: default 6)  */
+    int       flux_fx_shift;   /* fixed point of the flux tally (kp_tallies_t::
+                                  flux): round(value * 2^flux_fx_shift); 0 takes
+                                  fx_shift.  A cell's sum must stay below
+                                  2^(63 - flux_fx_shift).                       */
 } kp_transport_cfg_t;
 
 typedef struct kp_packet_record
@@ -315,7 +319,16 @@ typedef struct kp_packet_record
  *   image_batch [n_batches][image_batch_n][image_batch_n][4]  coarse image
  *                                          per batch (pixel i -> i*bn/n)
  *   counters    [KP_NCOUNTERS] uint64 (optional)
- *   records     [n_record] (optional) */
+ *   records     [n_record] (optional)
+ *   flux        [n_cells] (optional) path-length estimator of the mean
+ *               intensity, the reference's rad_t::flx: every walk segment of
+ *               length dl in cell i adds w * dl / volume(i), w the packet's
+ *               weight along the segment (photon::cart_t::proc_phys,
+ *               modules/particle/radiation/photon.h:73-83, and its field,
+ *               radiation/rad_data.cpp:13-25).  Block-id order, x fastest in
+ *               a block; int64 with scale 2^flux_fx_shift, or float.  Peel-off
+ *               rays deposit nothing.  In a decomposed solve the array is the
+ *               rank's own blocks in local order (kp_dd_round_t::block_local). */
 typedef struct kp_tallies
 {
     void * mu;
@@ -323,6 +336,7 @@ typedef struct kp_tallies
     void * image_batch;
     unsigned long long * counters;
     kp_packet_record_t * records;
+    void * flux;
 } kp_tallies_t;
 
 /* Asynchronous on `stream`.  Calls that share a mesh handle must not

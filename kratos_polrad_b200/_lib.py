@@ -115,6 +115,13 @@ _SIGS = {
 
 lib.kp_last_error.restype = ctypes.c_char_p
 lib.kp_last_error.argtypes = []
+
+# Layout of the structs mirrored below (kp_transport_cfg_t, kp_tallies_t):
+# a library built from another header would read them wrongly.
+ABI_VERSION = 2
+if lib.kp_abi_version() != ABI_VERSION:
+    raise ImportError(f"{LIB_PATH} has ABI version {lib.kp_abi_version()}, this package "
+                      f"expects {ABI_VERSION}: rebuild it with `make -C kratos_polrad_b200/csrc`")
 for _name, _args in _SIGS.items():
     _f = getattr(lib, _name, None)
     if _f is not None:

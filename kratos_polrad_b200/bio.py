@@ -12,13 +12,16 @@ mesh_t::save and the restart load do (mesh/mesh.cpp:63-69, 99-112):
 
 * per block, the reference's own tags: ``block_<id>|i_logic`` (3 int32) and
   ``block_<id>|level`` (int32) as block_t::write stores them
-  (mesh/block/block.cpp:31-38), and, for a geometric-walk flux, the rad_t
-  flux field ``block_<id>|rad_flx_flux_{n_int,n_step,n_cell,n_gh,field}``
-  as dat_3d_t::write lays it out (mesh/types/dat_3d.h:117-125,
-  modules/particle/radiation/rad_data.cpp:45-49);
+  (mesh/block/block.cpp:31-38), and the rad_t flux field
+  ``block_<id>|rad_flx_flux_{n_int,n_step,n_cell,n_gh,field}`` as
+  dat_3d_t::write lays it out (mesh/types/dat_3d.h:117-125,
+  modules/particle/radiation/rad_data.cpp:45-49): the ``flux`` argument (a
+  geometric walk's deposits), or else the transport's path-length flux tally
+  (``tallies.flux``, as float32 sums of w * dl / volume);
 * the transport's arrays under ``kp|<name>`` (flat, with their shape under
   ``kp|shape|<name>``): ``sigma`` [n_cells, 2], the tallies ``mu``,
-  ``image``, ``image_batch``, ``counters``, gradients ``grad_sca``,
+  ``image``, ``image_batch``, ``counters``, ``flux`` (raw, int64 when fixed
+  point, so that a restart keeps accumulating exactly), gradients ``grad_sca``,
   ``grad_abs``, and ``kp|config`` (JSON of the TransportConfig) with
   ``kp|packets_done``.  A restart reloads sigma and the int64 tallies and
   continues with ``packet_offset = packets_done``: fixed-point tallies of the
@@ -151,6 +154,12 @@ def save_solution(path: str, mesh, sigma2=None, tallies=None, cfg=None, grads=No
     lev, reg = mesh.blocks()
     cpb = mesh.cells_per_block
     fl = _np(flux)
+    if fl is None and getattr(tallies, "flux", None) is not None:
+        fl = _np(tallies.flux).astype(np.float64)
+        if fl.dtype != np.float32 and np.issubdtype(_np(tallies.flux).dtype, np.integer):
+            c = cfg if cfg is not None else tallies.cfg
+            fl *= 2.0 ** -(c.flux_fx_shift or c.fx_shift)
+        fl = fl.astype(np.float32)
     for b in range(mesh.n_blocks):
         p = f"block_{b}|"
         ent.append((p + "i_logic", reg[b].astype(np.int32)))
@@ -169,7 +178,7 @@ def save_solution(path: str, mesh, sigma2=None, tallies=None, cfg=None, grads=No
 
     put("sigma", sigma2)
     if tallies is not None:
-        for name in ("mu", "image", "image_batch", "counters"):
+        for name in ("mu", "image", "image_batch", "counters", "flux"):
             put(name, getattr(tallies, name, None))
     if grads is not None:
         put("grad_sca", grads[0])

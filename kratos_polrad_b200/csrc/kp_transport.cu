@@ -61,7 +61,14 @@ namespace cg = cooperative_groups;
 // TAPE (with DEFER): the rays are also linked per packet, in vertex order,
 // for the adjoint of this solve (kp_transport_adjoint_tape); a packet with a
 // ray that found the queue full is flagged and listed instead.
-template< int TALLY, int NT, bool DD = false, bool DEFER = false, bool TAPE = false >
+// FLUX: every walk segment adds w * dl / volume to its cell's flux tally,
+// the path-length estimator of photon::cart_t::proc_phys
+// (modules/particle/radiation/photon.h:73-83) with the packet's weight as
+// its `proper`; w / volume of the walk's block waits in shared memory (set
+// at emission, interactions and block hand-offs), so a segment adds one
+// multiply and one atomic.
+template< int TALLY, int NT, bool DD = false, bool DEFER = false, bool TAPE = false,
+          bool FLUX = false >
 __global__ void __launch_bounds__( NT, KP_FWD_RESIDENT / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
@@ -140,6 +147,31 @@ k_forward( const __grid_constant__ fwd_params_t P )
         }
         else
             return P.m.sigma[ cell_index( P.m, b, c ) ];
+    };
+
+    // FLUX: w / volume of block b for the walk's later segments
+    auto set_wv = [ & ]( float w, int b )
+    {
+        if constexpr( FLUX )
+            sc.wv[ threadIdx.x ] = __ddiv_rn( ( double ) w, P.m.geo_d[ 16 * ( size_t ) b + 6 ] );
+    };
+    // FLUX: deposit of the walk's segment of length dl in its current cell
+    // (DD: the rank's own blocks, stored compactly like the coefficients)
+    auto add_flux = [ & ]( double dl )
+    {
+        if constexpr( FLUX )
+        {
+            size_t i;
+            if constexpr( DD )
+            {
+                const int l = P.dd_loc[ p.b ];
+                if( l < 0 ) return;                      // flagged by sigma_at
+                i = ( size_t ) l * P.m.cpb + p.c[ 0 ] + P.m.nc[ 0 ] * ( p.c[ 1 ] + P.m.nc[ 1 ] * p.c[ 2 ] );
+            }
+            else
+                i = cell_index( P.m, p.b, p.c );
+            add_grad< TALLY >( P.flux, i, __dmul_rn( dl, sc.wv[ threadIdx.x ] ), P.flux_scale );
+        }
     };
 
     // After the active ray crossed a face (or stopped): the end of a peel-off
@@ -306,6 +338,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                         continue;
                     }
                 }
+                if( ! peel && p.b != b_old ) set_wv( sc.w[ threadIdx.x ], p.b );
                 faces_all( P.m, p.b, p.c, p.d, fx );
             }
             phase = PH_SEGMENT;
@@ -345,6 +378,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sc.batch[ t ] = o.batch;
                     set_inv( p );
                     store_cold( sc, p );
+                    set_wv( p.w, p.b );
                     faces_all( P.m, p.b, p.c, p.d, fx );
                     peel = false; solo = false;
                     phase = PH_SEGMENT;
@@ -456,6 +490,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             faces_all( P.m, p.b, p.c, p.d, fx );
             store_cold( sc, p );
+            set_wv( p.w, p.b );
             continue;
         }
 
@@ -528,6 +563,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             {
                 faces_all( P.m, p.b, p.c, p.d, fx );
                 store_cold( sc, p );
+                set_wv( p.w, p.b );
             }
             continue;
         }
@@ -564,6 +600,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             {
                 double ti = ( double ) __fdiv_rn( p.tau, ext );
                 ti = ti > t ? t : ti;
+                add_flux( ti );
                 p.x[ 0 ] = __fma_rn( ti, ( double ) p.d.x, p.x[ 0 ] );
                 p.x[ 1 ] = __fma_rn( ti, ( double ) p.d.y, p.x[ 1 ] );
                 p.x[ 2 ] = __fma_rn( ti, ( double ) p.d.z, p.x[ 2 ] );
@@ -572,7 +609,11 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             if( ! peel_cut )
             {   // advance to the exit face and into the next cell (shared code)
-                if( ! peel ) p.tau = __fsub_rn( p.tau, et );
+                if( ! peel )
+                {
+                    p.tau = __fsub_rn( p.tau, et );
+                    add_flux( t );
+                }
                 #pragma unroll
                 for( int a = 0; a < 3; ++ a )
                     if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
@@ -852,6 +893,7 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     require( c.phase == KP_PHASE_RAYLEIGH || c.phase == KP_PHASE_HG_POL, "unknown phase" );
     require( c.tally_mode == KP_TALLY_FIXED || c.tally_mode == KP_TALLY_FLOAT, "unknown tally mode" );
     require( c.fx_shift >= 0 && c.fx_shift <= 48, "fx_shift out of range" );
+    require( c.flux_fx_shift >= 0 && c.flux_fx_shift <= 48, "flux_fx_shift out of range" );
     require( c.n_batches >= 1 && c.n_batches <= KP_MAX_BATCHES, "n_batches out of range",
              KP_ERR_CAPACITY );
     require( c.n_mu_bins >= 0 && ( c.n_mu_bins == 0 || ( t.mu && c.mu_hi > c.mu_lo ) ),
@@ -922,6 +964,8 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     P.counters = t.counters;
     P.records = t.records;
     P.n_record = c.n_record;
+    P.flux = t.flux;
+    P.flux_scale = std::ldexp( 1.0, c.flux_fx_shift > 0 ? c.flux_fx_shift : c.fx_shift );
 }
 
 // Converts one C source to its device form; point sources are located in
@@ -965,21 +1009,29 @@ int persistent_grid( const void * kernel, int threads )
     return n_sm * std::max( per_sm, 1 );
 }
 
-template< int NT >
-void launch_forward_nt( const fwd_params_t & P, int tally_mode, cudaStream_t s, int grid_pct )
+template< int TALLY, int NT, bool FLUX >
+void launch_forward_k( const fwd_params_t & P, cudaStream_t s, int grid_pct )
 {
-    const void * k = tally_mode == KP_TALLY_FIXED ? ( const void * ) k_forward< KP_TALLY_FIXED, NT >
-                                                  : ( const void * ) k_forward< KP_TALLY_FLOAT, NT >;
+    const void * k = ( const void * ) k_forward< TALLY, NT, false, false, false, FLUX >;
     long long grid = persistent_grid( k, NT );
     grid = std::max< long long >( 1, grid * grid_pct / 100 );
     grid = std::min< long long >( grid, ( P.n_packets + NT - 1 ) / NT );
     KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
     // whole warps only: the scheduler ballots over full warps
-    if( tally_mode == KP_TALLY_FIXED )
-        k_forward< KP_TALLY_FIXED, NT ><<< ( unsigned ) grid, NT, 0, s >>>( P );
-    else
-        k_forward< KP_TALLY_FLOAT, NT ><<< ( unsigned ) grid, NT, 0, s >>>( P );
+    k_forward< TALLY, NT, false, false, false, FLUX ><<< ( unsigned ) grid, NT, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
+}
+
+template< int NT >
+void launch_forward_nt( const fwd_params_t & P, int tally_mode, cudaStream_t s, int grid_pct )
+{
+    const bool fl = P.flux != nullptr;
+    if( tally_mode == KP_TALLY_FIXED )
+        fl ? launch_forward_k< KP_TALLY_FIXED, NT, true  >( P, s, grid_pct )
+           : launch_forward_k< KP_TALLY_FIXED, NT, false >( P, s, grid_pct );
+    else
+        fl ? launch_forward_k< KP_TALLY_FLOAT, NT, true  >( P, s, grid_pct )
+           : launch_forward_k< KP_TALLY_FLOAT, NT, false >( P, s, grid_pct );
 }
 
 // Launches the forward kernel with `threads` per block (128 or 256) and a
@@ -1024,17 +1076,24 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets )
     }
 }
 
+template< int TALLY, bool TAPE, bool FLUX >
+void launch_deferred_walk( const fwd_params_t & P, cudaStream_t s )
+{
+    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true, TAPE, FLUX >;
+    long long grid = persistent_grid( kf, 256 );
+    grid = std::min< long long >( grid, ( P.n_packets + 255 ) / 256 );
+    k_forward< TALLY, 256, false, true, TAPE, FLUX ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+
 template< int TALLY, bool TAPE >
 void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s )
 {
     P.pq_count = P.work + 1;
     P.pq_next = P.work + 2;
     KP_CUDA( cudaMemsetAsync( P.work, 0, 3 * sizeof( unsigned long long ), s ) );
-    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true, TAPE >;
-    long long grid = persistent_grid( kf, 256 );
-    grid = std::min< long long >( grid, ( P.n_packets + 255 ) / 256 );
-    k_forward< TALLY, 256, false, true, TAPE ><<< ( unsigned ) grid, 256, 0, s >>>( P );
-    KP_CUDA( cudaGetLastError(  ) );
+    if( P.flux ) launch_deferred_walk< TALLY, TAPE, true  >( P, s );
+    else         launch_deferred_walk< TALLY, TAPE, false >( P, s );
     if( split_event ) KP_CUDA( cudaEventRecord( split_event, s ) );
     constexpr int MODE = TAPE ? 3 : 0;
     const long long gp = persistent_grid( ( const void * ) k_peel< TALLY, MODE >, 256 );
@@ -1152,6 +1211,19 @@ extern "C" int kp_transport_split_event( void * event )
 // One round of a domain-decomposed solve (k_forward<..., DD = true>).
 
 static_assert( sizeof( kp::dd_walk_t ) == KP_DD_WALK_BYTES, "walk record size" );
+
+namespace kp
+{
+template< int TALLY, bool FLUX >
+void launch_dd( const fwd_params_t & P, long long items, cudaStream_t s )
+{
+    const void * k = ( const void * ) k_forward< TALLY, 256, true, false, false, FLUX >;
+    long long grid = persistent_grid( k, 256 );
+    grid = std::min< long long >( grid, ( items + 255 ) / 256 );
+    k_forward< TALLY, 256, true, false, false, FLUX ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+}   // namespace kp
 static_assert( sizeof( kp::dd_peel_t ) == KP_DD_PEEL_BYTES, "peel-off record size" );
 
 extern "C" int kp_transport_forward_dd( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
@@ -1191,17 +1263,14 @@ extern "C" int kp_transport_forward_dd( kp_mesh_t * mesh, const kp_transport_cfg
         const long long items = r->n_in_walk + r->n_in_peel + ( r->emit ? cfg->n_packets : 0 );
         if( items == 0 ) return;
         cudaStream_t s = ( cudaStream_t ) stream;
-        const void * k = cfg->tally_mode == KP_TALLY_FIXED
-                       ? ( const void * ) kp::k_forward< KP_TALLY_FIXED, 256, true >
-                       : ( const void * ) kp::k_forward< KP_TALLY_FLOAT, 256, true >;
-        long long grid = kp::persistent_grid( k, 256 );
-        grid = std::min< long long >( grid, ( items + 255 ) / 256 );
         KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
-        if( cfg->tally_mode == KP_TALLY_FIXED )
-            kp::k_forward< KP_TALLY_FIXED, 256, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+        const bool fx = cfg->tally_mode == KP_TALLY_FIXED;
+        if( P.flux )
+            fx ? kp::launch_dd< KP_TALLY_FIXED, true  >( P, items, s )
+               : kp::launch_dd< KP_TALLY_FLOAT, true  >( P, items, s );
         else
-            kp::k_forward< KP_TALLY_FLOAT, 256, true ><<< ( unsigned ) grid, 256, 0, s >>>( P );
-        KP_CUDA( cudaGetLastError(  ) );
+            fx ? kp::launch_dd< KP_TALLY_FIXED, false >( P, items, s )
+               : kp::launch_dd< KP_TALLY_FLOAT, false >( P, items, s );
     } );
 }
 

@@ -78,6 +78,8 @@ struct fwd_params_t
     unsigned long long * counters;
     kp_packet_record_t * records;
     long long   n_record;
+    void      * flux;              // path-length flux tally [n_cells] (null: off)
+    double      flux_scale;        // its fixed point scale
     unsigned long long * work;     // scratch: next packet index
     // adjoint only
     const float4 * adj_img;        // dL/d(image) [img_n * img_n] (I, Q, U, V)
@@ -423,6 +425,7 @@ struct cold_park_t
     int      n_scat[ NT ];
     uint32_t k1[ NT ], pid_lo[ NT ], pid_hi[ NT ], draw[ NT ];
     int      batch[ NT ];          // pid % n_batches, set at emission
+    double   wv[ NT ];             // flux tally: w / volume of the walk's block
 };
 
 template< class SC >

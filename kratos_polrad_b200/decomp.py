@@ -107,7 +107,10 @@ class Rank:
         self.out_count = torch.zeros(2, dtype=torch.int64, device=device)
         self.in_walk = torch.empty((0, WALK_BYTES), dtype=torch.uint8, device=device)
         self.in_peel = torch.empty((0, PEEL_BYTES), dtype=torch.uint8, device=device)
-        self.tallies = Tallies(cfg, device=device)
+        # the flux tally (cfg.flux) holds this rank's own blocks, local order
+        self.mine = mine
+        self.tallies = Tallies(cfg, device=device, n_cells=len(mine) * cpb)
+        self.tallies.flux_blocks = mine
 
     def _ensure(self, cap_walk, cap_peel):
         if cap_walk > self.cap_walk:
@@ -164,10 +167,15 @@ class Rank:
 
 
 def _sum_tallies(ranks):
-    out = Tallies(ranks[0].cfg, device=ranks[0].tallies.mu.device)
+    mesh = ranks[0].mesh
+    out = Tallies(ranks[0].cfg, device=ranks[0].tallies.mu.device, n_cells=mesh.n_cells)
     for rk in ranks:
         for name in ("mu", "image", "image_batch", "counters"):
             getattr(out, name).add_(getattr(rk.tallies, name))
+        if out.flux is not None:      # ranks own disjoint blocks
+            cpb = mesh.cells_per_block
+            idx = torch.as_tensor(rk.mine, dtype=torch.long, device=out.flux.device)
+            out.flux.view(-1, cpb)[idx] = rk.tallies.flux.view(-1, cpb)
     return out
 
 
@@ -220,7 +228,9 @@ def solve_distributed(mesh, sigma2, cfg: TransportConfig, owner=None, chunk: int
     """One rank per process (torch.distributed initialised; NCCL on GPUs).
     Every rank takes the same collective steps each round: two all-to-alls
     per record kind and one all-reduce of the records left.  Returns (this
-    rank's Tallies summed over all ranks, rounds)."""
+    rank's Tallies summed over all ranks, rounds).  The flux tally (cfg.flux)
+    is not summed: it holds this rank's own blocks (``tallies.flux_blocks``,
+    local order)."""
     import torch.distributed as dist
     rank, n = dist.get_rank(group), dist.get_world_size(group)
     owner = partition_blocks(mesh, n) if owner is None else np.asarray(owner, np.int32)

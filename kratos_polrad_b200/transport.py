@@ -46,12 +46,12 @@ class CTransportCfg(ctypes.Structure):
                 ("n_batches", c_int), ("image_batch_n", c_int), ("w_min", c_float),
                 ("rr_survive", c_float),
                 ("max_scatter", c_int), ("max_steps", c_ll), ("n_record", c_ll),
-                ("lane_batch", c_int)]
+                ("lane_batch", c_int), ("flux_fx_shift", c_int)]
 
 
 class CTallies(ctypes.Structure):
     _fields_ = [("mu", c_void_p), ("image", c_void_p), ("image_batch", c_void_p),
-                ("counters", c_void_p), ("records", c_void_p)]
+                ("counters", c_void_p), ("records", c_void_p), ("flux", c_void_p)]
 
 
 # numpy view of kp_packet_record_t (88 bytes)
@@ -101,6 +101,9 @@ class TransportConfig:
     max_steps: int = 1 << 24
     n_record: int = 0
     lane_batch: int = 0
+    flux_fx_shift: int = 24
+    # Python side only: keep the per-cell path-length flux tally (rad_t::flx)
+    flux: bool = False
 
     def to_c(self):
         src = (CSource * max(1, len(self.sources)))()
@@ -122,9 +125,13 @@ class TransportConfig:
 
 
 class Tallies:
-    """Device output buffers of a transport run (accumulated across calls)."""
+    """Device output buffers of a transport run (accumulated across calls).
 
-    def __init__(self, cfg: TransportConfig, device="cuda"):
+    ``n_cells`` sizes the path-length flux tally when ``cfg.flux`` is set
+    (the mesh's cell count; a decomposed rank's own cells).
+    """
+
+    def __init__(self, cfg: TransportConfig, device="cuda", n_cells: int = 0):
         dt = torch.int64 if cfg.tally_mode == TALLY_FIXED else torch.float32
         self.cfg = cfg
         self.mu = torch.zeros((cfg.n_batches, max(cfg.n_mu_bins, 1), 4), dtype=dt, device=device)
@@ -135,10 +142,15 @@ class Tallies:
         self.counters = torch.zeros(len(COUNTERS), dtype=torch.int64, device=device)
         self.records = (torch.zeros((max(cfg.n_record, 1), 88), dtype=torch.uint8, device=device)
                         if cfg.n_record else None)
+        if cfg.flux and n_cells <= 0:
+            raise ValueError("the flux tally needs the mesh's cell count (n_cells)")
+        self.flux = torch.zeros(n_cells, dtype=dt, device=device) if cfg.flux else None
 
     def zero_(self):
         for t in (self.mu, self.image, self.image_batch, self.counters):
             t.zero_()
+        if self.flux is not None:
+            self.flux.zero_()
         if self.records is not None:
             self.records.zero_()
         return self
@@ -150,10 +162,21 @@ class Tallies:
         t.image_batch = ptr(self.image_batch) if self.cfg.image_n else None
         t.counters = ptr(self.counters)
         t.records = ptr(self.records) if self.records is not None else None
+        t.flux = ptr(self.flux) if self.flux is not None else None
         return t
 
     def scale(self) -> float:
         return 2.0 ** -self.cfg.fx_shift if self.cfg.tally_mode == TALLY_FIXED else 1.0
+
+    def flux_scale(self) -> float:
+        """Factor that turns the flux tally into w * dl / volume sums."""
+        if self.cfg.tally_mode != TALLY_FIXED:
+            return 1.0
+        return 2.0 ** -(self.cfg.flux_fx_shift or self.cfg.fx_shift)
+
+    def flux_values(self) -> np.ndarray:
+        """Flux tally as float64 sums of w * dl / volume per cell."""
+        return self.flux.cpu().numpy().astype(np.float64) * self.flux_scale()
 
     def counts(self) -> dict:
         c = self.counters.cpu().numpy()
@@ -172,7 +195,7 @@ def forward(mesh, cfg: TransportConfig, tallies: Tallies | None = None,
     the solve was too large to tape (more packets than one queue chunk).
     """
     if tallies is None:
-        tallies = Tallies(cfg)
+        tallies = Tallies(cfg, n_cells=mesh.n_cells if cfg.flux else 0)
     c, t = cfg.to_c(), tallies.to_c()
     s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
     tallies.tape_id = 0

@@ -31,16 +31,21 @@ static void gl_shift_##S( const kpo_mesh_t * m, int b, const int * i,           
     if( rhs ) { xl[ ax ] = xr[ ax ]; xr[ ax ] = x_fc_##S( m, b, ax, i[ ax ] + 1 ); } \
     else      { xr[ ax ] = xl[ ax ]; xl[ ax ] = x_fc_##S( m, b, ax, i[ ax ] ); }     \
 }                                                                                \
-static void gl_fix_##S( const kpo_mesh_t * m, int b, const int * i,              \
-                        const F * x, F * xl, F * xr )                            \
-{   /* geo_loc_t::fix (particle_base.h:117-126): the cell index is left as is */ \
+static int gl_fix_##S( const kpo_mesh_t * m, int b, const int * i,               \
+                       const F * x, F * xl, F * xr )                             \
+{   /* geo_loc_t::fix (particle_base.h:117-126): the cell index is left as is;   \
+       returns the number of axes it shifted (the cached cell is then not the   \
+       indexed one) */                                                           \
+    int n = 0;                                                                   \
     for( int a = 0; a < 3; ++ a )                                                \
-        if( x[ a ] > xr[ a ] )      gl_shift_##S( m, b, i, xl, xr, a, 1 );       \
-        else if( x[ a ] < xl[ a ] ) gl_shift_##S( m, b, i, xl, xr, a, 0 );       \
+        if( x[ a ] > xr[ a ] )      { gl_shift_##S( m, b, i, xl, xr, a, 1 ); ++ n; } \
+        else if( x[ a ] < xl[ a ] ) { gl_shift_##S( m, b, i, xl, xr, a, 0 ); ++ n; } \
+    return n;                                                                    \
 }                                                                                \
 static void walk_##S( const kpo_mesh_t * m, F * x, const F * dir, int * i,       \
                       int * ibp, F proper, int * stepp, int * todop,             \
-                      double scale, double * flux_f, long long * flux_fx )       \
+                      double scale, double * flux_f, long long * flux_fx,        \
+                      int * fixp )                                               \
 {                                                                                \
     const int cpb = m->nc[ 0 ] * m->nc[ 1 ] * m->nc[ 2 ];                       \
     int ib = * ibp, step = * stepp, todo = -1;   /* photon.h:108 */              \
@@ -51,7 +56,7 @@ static void walk_##S( const kpo_mesh_t * m, F * x, const F * dir, int * i,      
         if( ib != ib_old && ib >= 0 )                                            \
         {                                                                        \
             gl_load_##S( m, ib, i, xl, xr );                                     \
-            gl_fix_##S( m, ib, i, x, xl, xr );                                   \
+            * fixp += gl_fix_##S( m, ib, i, x, xl, xr );                         \
             ib_old = ib;                                                         \
         }                                                                        \
         const int b = ib;                        /* prx = bmap[ib_l] */          \
@@ -130,7 +135,7 @@ static void walk_##S( const kpo_mesh_t * m, F * x, const F * dir, int * i,      
         if( ok && wrapped )                      /* photon.h:96-100 */           \
         {                                                                        \
             gl_load_##S( m, ib, i, xl, xr );                                     \
-            gl_fix_##S( m, ib, i, x, xl, xr );                                   \
+            * fixp += gl_fix_##S( m, ib, i, x, xl, xr );                         \
         }                                                                        \
         if( ! ok ) break;                                                        \
     }                                                                            \
@@ -146,9 +151,20 @@ int kpo_trace( const kpo_mesh_t * m, int precision, long n, double * x,
                int * step, int * todo, int fx_shift, double * flux_f,
                long long * flux_fx )
 {
+    return kpo_trace_ex( m, precision, n, x, dir, cell, ib, proper, step, todo, fx_shift,
+                         flux_f, flux_fx, NULL );
+}
+
+int kpo_trace_ex( const kpo_mesh_t * m, int precision, long n, double * x,
+                  const double * dir, int * cell, int * ib, const double * proper,
+                  int * step, int * todo, int fx_shift, double * flux_f,
+                  long long * flux_fx, int * fix_shifts )
+{
     const double scale = ldexp( 1.0, fx_shift );
     for( long p = 0; p < n; ++ p )
     {
+        int fx_dummy = 0;
+        int * fixp = fix_shifts ? fix_shifts + p : & fx_dummy;
         if( todo[ p ] != TO_KEEP )          /* integrator.h:90-92 */
             continue;
         if( ib[ p ] < 0 || ib[ p ] >= m->n_blocks )
@@ -159,12 +175,12 @@ int kpo_trace( const kpo_mesh_t * m, int precision, long n, double * x,
             for( int a = 0; a < 3; ++ a )
             { xf[ a ] = ( float ) x[ 3 * p + a ]; df[ a ] = ( float ) dir[ 3 * p + a ]; }
             walk_f32( m, xf, df, cell + 3 * p, ib + p, ( float ) proper[ p ], step + p,
-                      todo + p, scale, flux_f, flux_fx );
+                      todo + p, scale, flux_f, flux_fx, fixp );
             for( int a = 0; a < 3; ++ a ) x[ 3 * p + a ] = xf[ a ];
         }
         else
             walk_f64( m, x + 3 * p, dir + 3 * p, cell + 3 * p, ib + p, proper[ p ],
-                      step + p, todo + p, scale, flux_f, flux_fx );
+                      step + p, todo + p, scale, flux_f, flux_fx, fixp );
     }
     return 0;
 }
@@ -199,6 +215,8 @@ typedef struct
     int                max_scatter;
     long long          max_steps;
     long long         *mu, *image, *img_batch;
+    long long         *flux;           /* path-length tally (null: off) */
+    double             flux_scale;
 } tctx;
 
 typedef struct
@@ -314,6 +332,19 @@ static float tpeel_tau( const tctx * t, int b, const int * c0, const double * x0
 static void tadd( long long * base, long i, float v, double sc )
 {
     base[ i ] += llrint( ( double ) v * sc );
+}
+
+/* Path-length flux estimator of a walk segment of length dl in the packet's
+ * cell: w dl / volume, as photon::cart_t::proc_phys deposits proper * dl /
+ * volume (modules/particle/radiation/photon.h:73-83), the packet's weight
+ * being its `proper`.  The kernel keeps w / volume per packet and multiplies
+ * by dl, so this does the same. */
+static void tflux( const tctx * t, const tpk * p, double dl )
+{
+    if( ! t->flux ) return;
+    const double wv = ( double ) p->w / t->m->vol0[ p->b ];
+    const double v = dl * wv;
+    t->flux[ tcell( t, p->b, p->c ) ] += llrint( v * t->flux_scale );
 }
 
 /* Image pixel (iy * n + ix) under x, or -1 outside the image. */
@@ -490,6 +521,7 @@ static int tsetup( tctx * tp, const kpo_mesh_t * m, const float * sigma2, const 
     t.img_inv_pix = c->image_n > 0 ? c->image_n / ( 2.0 * c->image_half_width ) : 0.0;
     t.tau_cut = c->tau_peel_max > 0 ? c->tau_peel_max : 40.0f;
     t.fx_scale = ldexp( 1.0, c->fx_shift );
+    t.flux_scale = ldexp( 1.0, c->flux_fx_shift > 0 ? c->flux_fx_shift : c->fx_shift );
     t.n_batch = c->n_batches;
     t.img_bn = c->image_batch_n >= 1 ? c->image_batch_n : 1;
     t.w_min = c->w_min;
@@ -503,11 +535,11 @@ static int tsetup( tctx * tp, const kpo_mesh_t * m, const float * sigma2, const 
 int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
                    const int * lookup_n, const kpo_cfg_t * c, long long * mu,
                    long long * image, long long * img_batch,
-                   unsigned long long * counters, kpo_record_t * rec )
+                   unsigned long long * counters, kpo_record_t * rec, long long * flux )
 {
     tctx t;
     if( tsetup( & t, m, sigma2, lookup, lookup_n, c ) ) return -2;
-    t.mu = mu; t.image = image; t.img_batch = img_batch;
+    t.mu = mu; t.image = image; t.img_batch = img_batch; t.flux = flux;
     unsigned long long cnt[ 10 ] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 0 };
     for( long long k = 0; k < c->n_packets; ++ k )
     {
@@ -546,6 +578,7 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
             {
                 double ti = ( double ) ( p.tau / ext );
                 ti = ti > tt ? tt : ti;
+                tflux( & t, & p, ti );
                 p.x[ 0 ] = fma( ti, ( double ) p.d.x, p.x[ 0 ] );
                 p.x[ 1 ] = fma( ti, ( double ) p.d.y, p.x[ 1 ] );
                 p.x[ 2 ] = fma( ti, ( double ) p.d.z, p.x[ 2 ] );
@@ -584,6 +617,7 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
             else
             {
                 p.tau = p.tau - dtau;
+                tflux( & t, & p, tt );
                 for( int a = 0; a < 3; ++ a )
                     if( a != ax ) p.x[ a ] = fma( tt, ( double ) om_comp( p.d, a ), p.x[ a ] );
                 int lost;

@@ -45,6 +45,15 @@ int kpo_trace( const kpo_mesh_t * m, int precision, long n, double * x,
                const double * dir, int * cell, int * ib, const double * proper,
                int * step, int * todo, int fx_shift, double * flux_f,
                long long * flux_fx );
+/* Same walk; fix_shifts[n] (may be null) adds, per packet, the number of
+ * axes on which geo_loc_t::fix shifted the cached cell faces without moving
+ * the cell index (particle_base.h:117-126).  A packet with none walks the
+ * cells its position crosses; one with some deposits into cells other than
+ * the ones it crosses, and on a collapsed axis no longer stops at faces. */
+int kpo_trace_ex( const kpo_mesh_t * m, int precision, long n, double * x,
+                  const double * dir, int * cell, int * ib, const double * proper,
+                  int * step, int * todo, int fx_shift, double * flux_f,
+                  long long * flux_fx, int * fix_shifts );
 
 #ifdef __cplusplus
 }
@@ -91,6 +100,7 @@ typedef struct kpo_cfg
     int       max_scatter;
     long long max_steps;
     long long n_record;
+    int       flux_fx_shift;    /* flux tally scale 2^flux_fx_shift (0: fx_shift) */
 } kpo_cfg_t;
 
 typedef struct kpo_record
@@ -108,11 +118,13 @@ typedef struct kpo_record
 } kpo_record_t;
 
 /* sigma2: [n_cells][2] (sca, abs); lookup: finest-level leaf ids.
- * Outputs are accumulated into (int64 fixed point). */
+ * Outputs are accumulated into (int64 fixed point); flux ([n_cells], may be
+ * null) receives the path-length estimator w * dl / volume of every walk
+ * segment. */
 int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
                    const int * lookup_n, const kpo_cfg_t * c, long long * mu,
                    long long * image, long long * img_batch,
-                   unsigned long long * counters, kpo_record_t * rec );
+                   unsigned long long * counters, kpo_record_t * rec, long long * flux );
 
 #ifdef __cplusplus
 }

@@ -87,7 +87,9 @@ class Tables:
 
 
 def trace(tab: Tables, precision: int, x, dir, cell, ib, proper, steps, fx_shift=32, todo=None):
-    """Restated cart_t::proc walk; returns final state and both flux sums."""
+    """Restated cart_t::proc walk; returns final state, both flux sums and,
+    per packet, the number of cached-face shifts of geo_loc_t::fix that left
+    the cell index behind (``fix``)."""
     n = len(ib)
     x = np.array(x, np.float64).reshape(n, 3)
     dir = np.ascontiguousarray(dir, np.float64).reshape(n, 3)
@@ -98,16 +100,18 @@ def trace(tab: Tables, precision: int, x, dir, cell, ib, proper, steps, fx_shift
     todo = np.full(n, -2, np.int32) if todo is None else np.array(todo, np.int32)
     ncell = tab.n_blocks * tab.cells_per_block
     flux_f, flux_fx = np.zeros(ncell), np.zeros(ncell, np.int64)
+    fix = np.zeros(n, np.int32)
     s = tab._struct()
     L = lib()
-    L.kpo_trace.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_long] + [ctypes.c_void_p] * 7 + \
-        [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.kpo_trace_ex.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_long] + \
+        [ctypes.c_void_p] * 7 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     p = lambda a: a.ctypes.data
-    st = L.kpo_trace(ctypes.byref(s), precision, n, p(x), p(dir), p(cell), p(ib), p(proper),
-                     p(steps), p(todo), fx_shift, p(flux_f), p(flux_fx))
+    st = L.kpo_trace_ex(ctypes.byref(s), precision, n, p(x), p(dir), p(cell), p(ib), p(proper),
+                        p(steps), p(todo), fx_shift, p(flux_f), p(flux_fx), p(fix))
     if st != 0:
         raise RuntimeError("kpo_trace: bad block id")
-    return dict(x=x, cell=cell, ib=ib, step=steps, todo=todo, flux=flux_f, flux_fx=flux_fx)
+    return dict(x=x, cell=cell, ib=ib, step=steps, todo=todo, flux=flux_f, flux_fx=flux_fx,
+                fix=fix)
 
 
 # ---------------------------------------------------------------------------
@@ -130,7 +134,7 @@ class _Cfg(ctypes.Structure):
                 ("n_batches", ctypes.c_int), ("image_batch_n", ctypes.c_int),
                 ("w_min", ctypes.c_float), ("rr_survive", ctypes.c_float),
                 ("max_scatter", ctypes.c_int), ("max_steps", ctypes.c_longlong),
-                ("n_record", ctypes.c_longlong)]
+                ("n_record", ctypes.c_longlong), ("flux_fx_shift", ctypes.c_int)]
 
 
 def lookup_grid(levels, regs, nc_root_blocks):
@@ -144,11 +148,12 @@ def lookup_grid(levels, regs, nc_root_blocks):
     return g, n
 
 
-def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
+def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, flux=False):
     """Runs the restated transport for a TransportConfig-like ``cfg``.
 
     ``source_cells``: (ib, cell[3]) per source (point sources), located by
-    the caller.  Returns dict of int64 tallies, counters and records.
+    the caller.  Returns dict of int64 tallies, counters and records; with
+    ``flux`` also the int64 path-length flux tally ([n_cells]).
     """
     src = (_Source * max(1, len(cfg.sources)))()
     for k, s in enumerate(cfg.sources):
@@ -163,7 +168,7 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
     for name, _ in _Cfg._fields_:
         if name in ("sources", "n_sources", "image_center"):
             continue
-        setattr(c, name, getattr(cfg, name))
+        setattr(c, name, getattr(cfg, name, 0))
     c.n_sources = len(cfg.sources)
     c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
     for a in range(3):
@@ -182,11 +187,13 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells):
     lk_n = np.ascontiguousarray(lookup_n, np.int32)
     s = tab._struct()
     L = lib()
-    L.kpo_transport.argtypes = [ctypes.c_void_p] * 10
+    if flux:
+        out["flux"] = np.zeros(tab.n_blocks * tab.cells_per_block, np.int64)
+    L.kpo_transport.argtypes = [ctypes.c_void_p] * 11
     p = lambda a: ctypes.c_void_p(a.ctypes.data)
     st = L.kpo_transport(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
                          p(out["mu"]), p(out["image"]), p(out["image_batch"]), p(out["counters"]),
-                         p(rec))
+                         p(rec), p(out["flux"]) if flux else None)
     if st != 0:
         raise RuntimeError(f"kpo_transport failed ({st})")
     out["records"] = rec[:cfg.n_record]
@@ -211,7 +218,7 @@ def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, g
     for name, _ in _Cfg._fields_:
         if name in ("sources", "n_sources", "image_center"):
             continue
-        setattr(c, name, getattr(cfg, name))
+        setattr(c, name, getattr(cfg, name, 0))
     c.n_sources = len(cfg.sources)
     c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
     for a in range(3):

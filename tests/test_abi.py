@@ -12,7 +12,7 @@ def test_every_header_symbol_is_exported():
 
 
 def test_abi_version_and_error_channel():
-    assert _lib.lib.kp_abi_version() == 1
+    assert _lib.lib.kp_abi_version() == _lib.ABI_VERSION == 2
     # a failing call reports a status and a message, without touching a GPU
     st = _lib.lib.kp_mesh_create(None, None)
     assert st == _lib.KP_ERR_ARG

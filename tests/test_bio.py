@@ -117,3 +117,30 @@ def test_reference_reads_solution_file(tmp_path):
     data, unit = refharness.bio_read(p, "block_3|rad_flx_flux_field")
     cpb = mesh.cells_per_block
     assert unit == 4 and data == flux[3 * cpb:4 * cpb].tobytes()
+
+
+@pytest.mark.skipif(not port.available(), reason="oracle not built")
+def test_flux_tally_restart(tmp_path):
+    """The transport's path-length flux tally is saved raw (int64) and as the
+    rad_t flux field per block; a restart adds up to one run, bit for bit."""
+    from transport_cases import case, oracle_inputs
+    mesh, sig, t = case("amr_point")
+    t = dataclasses.replace(t, n_record=0, n_packets=600, flux=True, flux_fx_shift=24)
+    half = dataclasses.replace(t, n_packets=300)
+    tab, grid, gn, cells = oracle_inputs(mesh, t)
+    first = port.transport(tab, sig, grid, gn, half, cells, flux=True)
+    p = str(tmp_path / "flux.bin")
+    tal = types.SimpleNamespace(**{k: first[k] for k in ("mu", "image", "image_batch",
+                                                         "counters", "flux")})
+    bio.save_solution(p, mesh, sig, tal, half)
+    s = bio.load_solution(p)
+    second = port.transport(tab, sig, grid, gn, dataclasses.replace(half, packet_offset=300),
+                            cells, flux=True)
+    full = port.transport(tab, sig, grid, gn, t, cells, flux=True)
+    np.testing.assert_array_equal(s["flux"] + second["flux"], full["flux"])
+    with bio.BinaryFile(p) as f:
+        cpb = mesh.cells_per_block
+        b = 7
+        np.testing.assert_array_equal(
+            f.as_array(f"block_{b}|rad_flx_flux_field", "f"),
+            (first["flux"][b * cpb:(b + 1) * cpb] * 2.0 ** -24).astype(np.float32))

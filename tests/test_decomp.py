@@ -91,3 +91,23 @@ def test_queue_overflow_is_reported():
     with pytest.raises(RuntimeError, match="overflow"):
         decomp.solve_emulated(mesh, sig, t, 2, peel_factor=0, min_cap=1)
     assert mesh.status() == 0          # the flag was read and cleared
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_ranks", [2, 3])
+def test_emulated_ranks_flux_tally(n_ranks):
+    """Each rank tallies the path-length flux of its own blocks; put together
+    they equal the replicated solve's flux bit for bit."""
+    from kratos_polrad_b200.transport import Tallies, forward
+    from transport_cases import case
+    mesh, sig, t = case("amr_point")
+    t = dataclasses.replace(t, n_record=0, flux=True, flux_fx_shift=24)
+    mesh.set_sigma(sig)
+    ref = forward(mesh, t, Tallies(t, n_cells=mesh.n_cells))
+    torch.cuda.synchronize()
+    got, rounds = decomp.solve_emulated(mesh, sig, t, n_ranks, chunk=t.n_packets // 3 + 1)
+    torch.cuda.synchronize()
+    assert mesh.status() == 0 and rounds > 1
+    assert int(ref.flux.sum()) > 0
+    assert torch.equal(got.flux, ref.flux)
+    assert torch.equal(got.image, ref.image)
