@@ -151,9 +151,9 @@ def algorithmic_bytes(c):
 
 def cpu_baseline(mesh, sigma2, cfg, budget_s=20.0, threads=None):
     """Times the oracle's C restatement on the host cores over a bounded
-    sample of the same workload (packets 0..n of the same scene)."""
+    sample of the same workload (packets 0..n of the same scene), on the
+    product mesh's tables."""
     from oracle import port
-    threads = threads or os.cpu_count() or 1
     tab = port.Tables.from_mesh(mesh, 8)
     lev, reg = mesh.blocks()
     roots = [int(round((mesh.x_max[a] - mesh.x_min[a]) / (tab.dx0[0, a] * mesh.nc[a] * 2 ** lev[0])))
@@ -163,10 +163,18 @@ def cpu_baseline(mesh, sigma2, cfg, budget_s=20.0, threads=None):
     for s in cfg.sources:
         ib, cell = mesh.locate([s.pos])
         cells.append((ib[0], cell[0]))
+    return cpu_baseline_tables(tab, sigma2, grid, gn, cfg, cells, budget_s, threads)
+
+
+def cpu_baseline_tables(tab, sigma2, grid, gn, cfg, cells, budget_s=20.0, threads=None):
+    """The restatement timed on the host cores over a bounded sample
+    (packets 0..n of the scene), sized to about budget_s of CPU work."""
+    from oracle import port
+    threads = threads or os.cpu_count() or 1
     # calibrate on a small sample, then size the timed sample to the budget
     probe = dataclasses.replace(cfg, n_packets=2000, n_record=0)
     t0 = time.perf_counter()
-    r = port.transport(tab, sigma2, grid, gn, probe, cells)
+    port.transport(tab, sigma2, grid, gn, probe, cells)
     per_pkt = (time.perf_counter() - t0) / 2000
     chunk = max(50, int(budget_s / per_pkt / threads / 4))
     n_chunks = threads * 4
@@ -190,14 +198,16 @@ def run_reference(args, rank, world):
     """--impl reference: the CPU implementation of this path on the host cores.
 
     The reference has no scattering physics for this workload, so the timed
-    CPU implementation is the oracle's restatement (kind "port")."""
+    CPU implementation is the oracle's restatement (kind "port").  The scene
+    is built on the reference's own tree/meshgen/proxy code (oracle/_ref);
+    this arm never loads the product library."""
     if rank != 0:
         return
-    from kratos_polrad_b200 import scenes
-    mesh, sigma2, cfg = scenes.clump_amr(n_packets=int(args.packets))
+    from oracle import ref_scene
+    tab, sigma2, grid, gn, cfg, cells = ref_scene.clump(int(args.packets))
     vals = []
     for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(mesh, sigma2, cfg, budget_s=8.0)
+        cb = cpu_baseline_tables(tab, sigma2, grid, gn, cfg, cells, budget_s=8.0)
         if k >= args.warmup:
             vals.append(cb["value"])
     v = statistics.mean(vals)
@@ -206,25 +216,29 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 positions / f32 Stokes",
             "data": "synthetic", "config": workload_config(cfg, args.packets),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port",
-                             "sample": cb["sample"]},
+                             "sample": cb["sample"],
+                             "tables": "built by the reference's tree/meshgen/proxy code "
+                                       "(oracle/_ref/libkpref_p2.so)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args):
-    """Batched workload: 256 independent uniform cubes (sides from
-    {16,32,48,64,96}, tau log-uniform [0.1,20], albedo uniform [0.3,1], seed 3,
-    1e5-1e6 packets in proportion to tau, 32-bin mu tallies) in one autotuned,
-    graph-replayed persistent launch, against 256 sequential single-scene
-    launches of the same packets (same tallies, bit for bit).  Under torchrun
-    each rank solves a contiguous range of the scenes (no collective in the
-    data path); the per-scene tallies are gathered on rank 0."""
+def measure_batched(steps, warmup, clocks=None):
+    """The 256-scene batched solve (scenes.batched_cubes: uniform cubes with
+    sides from {16,32,48,64,96}, tau log-uniform [0.1,20], albedo uniform
+    [0.3,1], seed 3, 1e5-1e6 packets in proportion to tau, 32-bin mu tallies)
+    in one autotuned, graph-replayed persistent launch, against sequential
+    single-scene launches of the same packets (same tallies, bit for bit).
+    Under torchrun each rank solves a contiguous range of the scenes (no
+    collective in the data path); the per-scene tallies are gathered on rank
+    0.  Every rank returns the same dict."""
+    import contextlib
     import torch
-    import torch.distributed as dist
     from kratos_polrad_b200 import scenes, shard
     from kratos_polrad_b200.batch import Batch
     from kratos_polrad_b200.transport import Tallies, forward
-    rank, world, _ = _init_ranks()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
     sc_all, cfg = scenes.batched_cubes()
     lo, hi = shard.scene_range(len(sc_all), rank, world)
     sc = sc_all[lo:hi]
@@ -236,15 +250,16 @@ def run_batched(args):
     cnt = torch.zeros(10, dtype=torch.int64, device="cuda")
     mu = b.new_mu(cfg)
     with torch.cuda.stream(s):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             mu.zero_()
             b.forward(cfg, mu=mu, graph=True, stream=s.cuda_stream)
     s.synchronize()
     times = []
     if world > 1:
+        import torch.distributed as dist
         dist.barrier()
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
-        for k in range(args.steps):
+    with (clocks if clocks is not None else contextlib.nullcontext()):
+        for k in range(steps):
             mu.zero_()
             cnt.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -254,14 +269,12 @@ def run_batched(args):
                 e1.record(s)
             s.synchronize()
             times.append(e0.elapsed_time(e1))
-    if world > 1:
-        dist.barrier()
     red = torch.tensor([statistics.mean(times)], dtype=torch.float64, device="cuda")
     shard_max(red)
     batched_ms = float(red.item())
     shard.reduce_tallies([cnt])
     c = cnt.cpu().numpy()
-    steps = int(c[0] + c[1])
+    n_steps = int(c[0] + c[1])
     mu_all = shard.gather_scene_tallies(mu, len(sc_all), rank, world)
     # sequential plain launches of the same scenes
     seq_mu = torch.zeros_like(mu)
@@ -286,26 +299,36 @@ def run_batched(args):
         seq_mu[k] = tl.mu
     differs = torch.tensor([0 if torch.equal(seq_mu, mu) else 1], dtype=torch.int64, device="cuda")
     shard_max(differs)                                   # any rank whose scenes differ
-    same = bool(differs.item() == 0)
-    if rank != 0:
-        _finish_ranks(world)
-        return
-    line = {"metric": "packet-steps/s, 256-scene batched solve", "value": steps / (batched_ms / 1e3),
-            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 positions / f32 Stokes", "data": "synthetic",
+    return {"value": n_steps / (batched_ms / 1e3), "unit": UNIT, "ms_per_step": batched_ms,
+            "steps": steps, "warmup": warmup,
             "config": {"workload": "batched_cubes_256", "scenes": len(sc_all),
                        "packets": int(sum(n for _, _, n, _, _ in sc_all)),
                        "cells": int(sum(m.n_cells for m, *_ in sc_all)),
                        "tallies": "int64 fixed point",
                        "launch": "one persistent launch replayed from a CUDA graph",
                        "split": "contiguous scene ranges per rank, tallies gathered on rank 0"},
-            "gathered_scenes": int(mu_all.shape[0]),
-            "autotune": tune, "sequential_ms": seq_ms,
-            "sequential_value": steps / (seq_ms / 1e3),
+            "gathered_scenes": int(mu_all.shape[0]), "autotune": tune,
+            "sequential_ms": seq_ms, "sequential_value": n_steps / (seq_ms / 1e3),
             "batched_over_sequential": seq_ms / batched_ms,
-            "tallies_identical_to_sequential": same, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+            "tallies_identical_to_sequential": bool(differs.item() == 0)}
+
+
+def run_batched(args):
+    """--workload batched: the batched solve on its own JSON line."""
+    rank, world, local = _init_ranks()
+    clk = ClockSampler(local)
+    r = measure_batched(args.steps, args.warmup, clk)
+    if rank == 0:
+        line = {"metric": "packet-steps/s, 256-scene batched solve", "value": r["value"],
+                "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 positions / f32 Stokes", "data": "synthetic",
+                "config": r["config"],
+                **{k: r[k] for k in ("gathered_scenes", "autotune", "sequential_ms",
+                                     "sequential_value", "batched_over_sequential",
+                                     "tallies_identical_to_sequential")},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
     _finish_ranks(world)
 
 
@@ -527,7 +550,7 @@ def _walk_bench(args, spherical):
     import numpy as np
     import torch
     from kratos_polrad_b200 import Mesh, PacketPool, scenes
-    from kratos_polrad_b200.trace import TO_KEEP, trace as gpu_trace, trace_sph as gpu_trace_sph
+    from kratos_polrad_b200.walk import TO_KEEP, trace as gpu_trace, trace_sph as gpu_trace_sph
     from oracle import refharness
     two_pi = 2 * math.pi
     if spherical:
@@ -941,6 +964,37 @@ def main():
                               "note": "forward with its peel-off rays kept, then the adjoint "
                                       "from them (autograd step)"}}
 
+    # ---- the path-length flux tally (rad_t::flx): same solves with it on ----
+    fcfg = dataclasses.replace(cfg, flux=True, flux_fx_shift=20)
+    ftal = Tallies(fcfg, n_cells=mesh.n_cells)
+    forward(mesh, fcfg, ftal)
+    torch.cuda.synchronize()
+    flux_ms = []
+    for k in range(max(1, min(args.steps, 3))):
+        ftal.zero_()
+        flush.fill_(float(k))
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        forward(mesh, fcfg, ftal)
+        f1.record()
+        torch.cuda.synchronize()
+        flux_ms.append(f0.elapsed_time(f1))
+    fc = ftal.counts()
+    flux_same = all(torch.equal(getattr(ftal, n), getattr(tal, n)) for n in ("image", "mu"))
+    flux_info = {"ms_per_solve": statistics.mean(flux_ms),
+                 "cost_vs_forward": statistics.mean(flux_ms) / statistics.mean(kern_ms),
+                 "algorithmic_bytes": algorithmic_bytes(fc) + 8 * fc["steps"],
+                 "achieved_gbs": (algorithmic_bytes(fc) + 8 * fc["steps"])
+                 / (statistics.mean(flux_ms) / 1e3) / 1e9,
+                 "cells_visited": int((ftal.flux != 0).sum()),
+                 "other_tallies_unchanged": flux_same,
+                 "note": "int64 w*dl/volume per walk segment (scale 2^20); +8 B per walk "
+                         "segment (read + write of the cell's tally)"}
+    assert mesh.status() == 0
+
+    # ---- the batched solve (256 scenes), its own numbers ----
+    batched_info = measure_batched(max(1, min(args.steps, 3)), 1)
+
     # ---- end to end through the C ABI with host buffers ----
     import ctypes
     n_cells = mesh.n_cells
@@ -993,7 +1047,7 @@ def main():
                "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
-               "adjoint": adjoint_info,
+               "adjoint": adjoint_info, "flux_tally": flux_info, "batched": batched_info,
                "gpu_launches": args.steps * (2 if cfg.image_n > 0 else 1),
                "clocks": clk.summary()}
         print(json.dumps(out), flush=True)

@@ -262,6 +262,25 @@ typedef struct kp_source
     double pos[ 3 ];
 } kp_source_t;
 
+/* One packet made by a user generator: what the reference's generator
+ * functor writes into the pool for each packet (x, dir, cell, block,
+ * proper; modules/particle/evolve/generate_par.h:10-15, launched by ker_gen
+ * over n_par packets, generate_par.h:51-62).  64 bytes, device memory. */
+typedef struct kp_packet_init
+{
+    double x[ 3 ];       /* position inside the mesh                          */
+    float  d[ 3 ];       /* unit direction                                    */
+    float  w;            /* weight (the reference's `proper`)                 */
+    float  stokes[ 3 ];  /* q, u, v relative to I, reference vector e1 =
+                            normalize(z x d) if |d.z| < 0.9 else
+                            normalize(x x d); 0 for unpolarized light          */
+    int    ib;           /* block id, or -1 to locate x on the device         */
+    float  peel_I;       /* emitted intensity per steradian toward the
+                            observer per unit weight (1/(4 pi) for isotropic
+                            emission); 0: no peel-off ray at emission          */
+    int    pad;
+} kp_packet_init_t;
+
 typedef struct kp_transport_cfg
 {
     long long n_packets;       /* packets of this call                         */
@@ -296,6 +315,12 @@ typedef struct kp_transport_cfg
                                   flux): round(value * 2^flux_fx_shift); 0 takes
                                   fx_shift.  A cell's sum must stay below
                                   2^(63 - flux_fx_shift).                       */
+    const kp_packet_init_t * packets;  /* device [n_packets] or NULL: when set,
+                                  packet k of the call (global id
+                                  packet_offset + k) starts from packets[k]
+                                  instead of a source (sources are then not
+                                  used and n_sources may be 0); its RNG stream
+                                  is still keyed by its global id              */
 } kp_transport_cfg_t;
 
 typedef struct kp_packet_record
@@ -474,7 +499,12 @@ int kp_mesh_tape_id( const kp_mesh_t * mesh, long long * tape_id );
  * cudaFree or allocating library routine.  The kernel's only scratch, the
  * 64-bit counter that hands out packet indices, lives in a static device
  * array of KP_NOALLOC_SCRATCH_BYTES that the library holds on every GPU
- * that loads it, until the process exits.  Inputs and outputs are the
+ * that loads it, until the process exits.  With an image, the peel-off rays
+ * are marched inside the walk kernel, where they start (kp_transport_forward
+ * queues them for a second kernel, and the queue is an allocation): the
+ * int64 tallies are the same bit for bit, float tallies agree within float
+ * rounding (another summation order), and the solve is slower.  A
+ * kp_transport_split_event event is recorded after the walk.  Inputs and outputs are the
  * caller's: the mesh must already be on the current device (kp_mesh_upload,
  * or an earlier kp_mesh_set_sigma, at set-up time), else KP_ERR_CONFIG; a
  * solve whose scratch would not fit is rejected with KP_ERR_CAPACITY.  The

@@ -71,15 +71,15 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
     auto begin_pass1 = [ & ](  )
     {
         const long long pid = cold_pid( sc );
-        emit_packet( P, pid, p, P.src[ pid % P.n_src ], P.stream );
+        float peel_I;
+        emit_any( P, pid, p, peel_I );
         p.tau = sample_tau( p.rng );
         store_cold( sc, p );
         pass = 1;
         nv = 0;
         phase = PH_SEGMENT;
         ray = RAY_WALK;
-        const src_dev_t & s = P.src[ pid % P.n_src ];
-        if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC && G0 != 0.0f )
+        if( P.img_n > 0 && peel_I > 0.0f && G0 != 0.0f )
         {
             park_walk( sp, p );
             park_dir( sd, p, P.o, P.inv_o );
@@ -219,7 +219,8 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             }
             const long long pid = P.pid0 + ( P.adj_list ? ( long long ) P.adj_list[ idx ]
                                                         : ( long long ) idx );
-            if( ! emit_packet( P, pid, p, P.src[ pid % P.n_src ], P.stream ) )
+            float peel_I;
+            if( ! emit_any( P, pid, p, peel_I ) )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
                 continue;
@@ -230,13 +231,12 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             pass = 0; nv = 0; R = 0.0; G0 = 0.f;
             phase = PH_SEGMENT;
             ray = RAY_WALK;
-            const src_dev_t & s = P.src[ p.pid(  ) % P.n_src ];
-            if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
+            if( P.img_n > 0 && peel_I > 0.0f )
             {
                 const int pix = image_pixel( P, p.x );
                 if( pix >= 0 )
                 {
-                    sp.w[ th ] = 1.0f; sp.I[ th ] = 0x1.45f306p-4f;    // 1 / (4 pi)
+                    sp.w[ th ] = p.w; sp.I[ th ] = peel_I;
                     sp.Q[ th ] = sp.U[ th ] = sp.V[ th ] = 0.0f;
                     sp.pix[ th ] = pix;
                     pend = 0; ptau = 0.0f; pk = 0;
@@ -517,8 +517,8 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
                 if( P.adj_flag[ lp ] )
                     continue;                     // replayed by k_adjoint
             const long long pid = P.pid0 + ( long long ) idx;
-            const src_dev_t & s = P.src[ pid % P.n_src ];
-            if( ! emit_packet( P, pid, p, s, P.stream ) )
+            float peel_I;
+            if( ! emit_any( P, pid, p, peel_I ) )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
                 continue;
@@ -535,13 +535,13 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
             }
             p.tau = sample_tau( p.rng );
             store_cold( sc, p );
-            if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
-            {   // direct light of an isotropic, unpolarized point source
+            if( P.img_n > 0 && peel_I > 0.0f )
+            {   // direct light of the emission (unpolarized)
                 const int pix = image_pixel( P, p.x );
                 if( pix >= 0 )
                 {
                     if constexpr( PASS == 0 )
-                        queue_ray( pix, 1.0f, 0x1.45f306p-4f, 0.0f, 0.0f, 0.0f, 0 );
+                        queue_ray( pix, p.w, peel_I, 0.0f, 0.0f, 0.0f, 0 );
                     else if( link >= 0 )
                         link = P.pq[ link ].next;     // its ray is deposited by k_peel
                 }
@@ -863,7 +863,8 @@ bool same_solve( const kp_transport_cfg_t & a, const kp_source_t * sa, const kp_
            && a.azimuth_deg == b.azimuth_deg && a.image_half_width == b.image_half_width
            && a.tau_peel_max == b.tau_peel_max && a.w_min == b.w_min
            && a.rr_survive == b.rr_survive && a.max_scatter == b.max_scatter
-           && a.max_steps == b.max_steps && b.sources != nullptr;
+           && a.max_steps == b.max_steps && a.packets == b.packets
+           && ( b.sources != nullptr || b.packets != nullptr );
     for( int k = 0; eq && k < 3; ++ k ) eq = a.image_center[ k ] == b.image_center[ k ];
     for( int k = 0; eq && k < b.n_sources; ++ k )
     {

@@ -76,6 +76,7 @@ void make_batch_params( kp_batch_t * b, const kp_transport_cfg_t & c, void * mu,
 {
     require( c.image_n == 0, "batched solves tally escapes only (image_n must be 0)" );
     require( c.n_mu_bins > 0 && mu, "batched solves need escape tallies (n_mu_bins > 0, mu)" );
+    require( c.packets == nullptr, "batched scenes emit from their point sources (packets must be null)" );
     kp_tallies_t t {  };
     t.mu = mu;
     t.counters = counters;

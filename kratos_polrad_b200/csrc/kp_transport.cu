@@ -402,11 +402,13 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 }
                 idx -= nw + npl;
                 // each packet is emitted once over the ranks: point sources by
-                // the owner of the source's block, plane sources by pid modulo
+                // the owner of the source's block, plane sources and the
+                // caller's packets by pid modulo
                 const long long pid = P.pid0 + ( long long ) idx;
-                const src_dev_t & s0 = P.src[ pid % P.n_src ];
-                if( s0.kind == KP_SOURCE_POINT ? P.dd_owner[ s0.ib ] != P.dd_rank
-                                               : ( int ) ( pid % P.dd_ranks ) != P.dd_rank )
+                const bool point = P.pk_table == nullptr
+                                && P.src[ pid % P.n_src ].kind == KP_SOURCE_POINT;
+                if( point ? P.dd_owner[ P.src[ pid % P.n_src ].ib ] != P.dd_rank
+                          : ( int ) ( pid % P.dd_ranks ) != P.dd_rank )
                     continue;
             }
             else if( idx >= ( unsigned long long ) P.n_packets )
@@ -415,6 +417,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             bool ok;
+            float peel_I = 0.0f;          // emission's intensity toward the observer
             if( P.n_scenes > 0 )
             {   // batched launch: scene of this packet index, then its local id
                 int lo = 0, hi = P.n_scenes;
@@ -425,11 +428,13 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 }
                 si = lo;
                 const long long pid = P.pid0 + ( ( long long ) idx - P.scene_prefix[ si ] );
-                ok = emit_packet( P, pid, p, P.scenes[ si ].src, P.scenes[ si ].stream );
+                const src_dev_t & s = P.scenes[ si ].src;
+                ok = emit_packet( P, pid, p, s, P.scenes[ si ].stream );
+                peel_I = s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC ? 0x1.45f306p-4f
+                                                                                  : 0.0f;
             }
             else
-                ok = emit_packet( P, P.pid0 + ( long long ) idx, p,
-                                  P.src[ ( P.pid0 + ( long long ) idx ) % P.n_src ], P.stream );
+                ok = emit_any( P, P.pid0 + ( long long ) idx, p, peel_I );
             if( ! ok )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
@@ -465,14 +470,13 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     continue;
                 }
             }
-            const src_dev_t & s = P.n_scenes > 0 ? P.scenes[ si ].src : P.src[ p.pid(  ) % P.n_src ];
-            if( P.img_n > 0 && s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC )
-            {   // direct light of an isotropic, unpolarized point source
+            if( P.img_n > 0 && peel_I > 0.0f )
+            {   // direct light of the emission (unpolarized)
                 const int pix = image_pixel( P, p.x );
                 if( pix >= 0 )
                 {
                     const int t = threadIdx.x;
-                    sp.w[ t ] = 1.0f; sp.I[ t ] = 0x1.45f306p-4f;     // 1 / (4 pi)
+                    sp.w[ t ] = p.w; sp.I[ t ] = peel_I;
                     sp.Q[ t ] = sp.U[ t ] = sp.V[ t ] = 0.0f;
                     sp.pix[ t ] = pix;
                     sd.cpix[ t ] = coarse_pixel( P, pix, sc.batch[ t ] );
@@ -988,14 +992,18 @@ void make_source( kp_mesh_t * mesh, const kp_source_t & s, src_dev_t & d )
 void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
                       const kp_tallies_t & t, fwd_params_t & P )
 {
-    require( c.n_sources >= 1 && c.n_sources <= MAX_SOURCES && c.sources,
-             "need 1..KP_MAX_SOURCES sources", KP_ERR_CAPACITY );
+    if( c.packets == nullptr )
+        require( c.n_sources >= 1 && c.n_sources <= MAX_SOURCES && c.sources,
+                 "need 1..KP_MAX_SOURCES sources", KP_ERR_CAPACITY );
     fill_common_params( c, t, P );
     const auto & tab = mesh->tree->tables(  );
     P.m = mesh->view(  );
-    P.n_src = c.n_sources;
-    for( int k = 0; k < c.n_sources; ++ k )
-        make_source( mesh, c.sources[ k ], P.src[ k ] );
+    P.pk_table = c.packets;
+    P.pk_pid0 = c.packet_offset;
+    P.n_src = c.packets ? 1 : c.n_sources;        // P.src[ 0 ] unused with a table
+    if( c.packets == nullptr )
+        for( int k = 0; k < c.n_sources; ++ k )
+            make_source( mesh, c.sources[ k ], P.src[ k ] );
     for( int a = 0; a < 3; ++ a )
         P.lk_inv[ a ] = tab.lookup_n[ a ] / tab.l_box_d[ a ];
 }
@@ -1335,5 +1343,6 @@ extern "C" int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transpor
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = static_cast< unsigned long long * >( kp::noalloc_scratch(  ) );
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
+        if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
     } );
 }

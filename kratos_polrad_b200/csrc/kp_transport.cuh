@@ -54,6 +54,8 @@ struct fwd_params_t
     uint32_t    seed, stream;
     phys::phase_t ph;
     int         n_src;
+    const kp_packet_init_t * pk_table;  // caller's packets (null: the sources)
+    long long   pk_pid0;                // global id of pk_table[0]
     int         n_mu;
     float       mu_lo, mu_inv_w;
     int         img_n;
@@ -265,7 +267,13 @@ __device__ __forceinline__ bool cross_face( const mesh_view_t & m, int & b, int 
     const int4 q = reinterpret_cast< const int4 * >( m.nb + 24 * ( size_t ) b )[ ax * 2 + side ];
     const blk_meta_t md = m.meta[ b ];
     if( ( md.phybnd >> ( 2 * ax + side ) ) & 1 )
+    {   // leaves the domain: the position ends on the boundary face
+        #pragma unroll
+        for( int a = 0; a < 3; ++ a )
+            if( a == ax )
+                x[ a ] = __fma_rn( ( double ) ( pos ? cax + 1 : cax ), g[ 3 + a ], g[ a ] );
         return false;
+    }
     const int a1 = ax == 2 ? 0 : ax + 1;
     const int a2 = ax == 0 ? 2 : ax - 1;
     int ca1 = 0, ca2 = 0;
@@ -613,6 +621,40 @@ __device__ __forceinline__ phys::v3 sample_emission_dir( phys::rng_t & rng, int 
     return phys::dir_from( mu, __fdiv_rn( a, rr ), __fdiv_rn( b, rr ) );
 }
 
+// Cell of block b holding x: floor((x - xf0) / dx0) per axis, clamped to
+// the block.
+__device__ __forceinline__ void cell_of( const mesh_view_t & m, int b, const double x[ 3 ],
+                                         int c[ 3 ] )
+{
+    const double * h = m.geo_d + 16 * ( size_t ) b;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        const double f = floor( __dmul_rn( __dsub_rn( x[ a ], h[ a ] ), h[ 8 + a ] ) );
+        c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( m.nc[ a ] - 1 ) ? m.nc[ a ] - 1 : ( int ) f );
+    }
+}
+
+// Block and cell holding x, through the finest-level lookup grid; false
+// when no block is found there.
+__device__ __forceinline__ bool locate_point( const fwd_params_t & P, const double x[ 3 ],
+                                              int & b, int c[ 3 ] )
+{
+    int li[ 3 ];
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        const double f = floor( __dmul_rn( __dsub_rn( x[ a ], P.m.xlim_d[ 0 ][ a ] ),
+                                           P.lk_inv[ a ] ) );
+        li[ a ] = f < 0.0 ? 0 : ( f >= P.m.lookup_n[ a ] ? P.m.lookup_n[ a ] - 1 : ( int ) f );
+    }
+    b = P.m.lookup[ ( ( size_t ) li[ 2 ] * P.m.lookup_n[ 1 ] + li[ 1 ] )
+                    * P.m.lookup_n[ 0 ] + li[ 0 ] ];
+    if( b < 0 || b >= P.m.n_blocks ) return false;
+    cell_of( P.m, b, x, c );
+    return true;
+}
+
 // Creates packet `pid` at source `s` with RNG key (seed, stream).  Returns
 // false if the source position lies outside the mesh.
 __device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long pid, packet_t & p,
@@ -631,24 +673,7 @@ __device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long p
         p.x[ 0 ] = __fma_rn( ( double ) phys::u01( r.x ), P.m.lbox_d[ 0 ], P.m.xlim_d[ 0 ][ 0 ] );
         p.x[ 1 ] = __fma_rn( ( double ) phys::u01( r.y ), P.m.lbox_d[ 1 ], P.m.xlim_d[ 0 ][ 1 ] );
         p.x[ 2 ] = P.m.xlim_d[ 0 ][ 2 ];
-        int li[ 3 ];
-        #pragma unroll
-        for( int a = 0; a < 3; ++ a )
-        {
-            const double f = floor( __dmul_rn( __dsub_rn( p.x[ a ], P.m.xlim_d[ 0 ][ a ] ),
-                                               P.lk_inv[ a ] ) );
-            li[ a ] = f < 0.0 ? 0 : ( f >= P.m.lookup_n[ a ] ? P.m.lookup_n[ a ] - 1 : ( int ) f );
-        }
-        p.b = P.m.lookup[ ( ( size_t ) li[ 2 ] * P.m.lookup_n[ 1 ] + li[ 1 ] )
-                          * P.m.lookup_n[ 0 ] + li[ 0 ] ];
-        if( p.b < 0 || p.b >= P.m.n_blocks ) return false;
-        const double * h = P.m.geo_d + 16 * ( size_t ) p.b;
-        #pragma unroll
-        for( int a = 0; a < 3; ++ a )
-        {
-            const double f = floor( __dmul_rn( __dsub_rn( p.x[ a ], h[ a ] ), h[ 8 + a ] ) );
-            p.c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( P.m.nc[ a ] - 1 ) ? P.m.nc[ a ] - 1 : ( int ) f );
-        }
+        if( ! locate_point( P, p.x, p.b, p.c ) ) return false;
     }
     if( p.b < 0 || p.b >= P.m.n_blocks ) return false;
     p.d  = sample_emission_dir( p.rng, s.emit );
@@ -658,6 +683,46 @@ __device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long p
     p.n_scat  = 0;
     p.n_steps = 0;
     set_inv( p );
+    return true;
+}
+
+// Creates packet `pid` of a single-mesh launch: from the caller's packet
+// table when the launch has one (pid - pk_pid0 is its entry), else from
+// source pid % n_src.  peel_I receives the emitted intensity per steradian
+// toward the observer per unit weight, 0 for no peel-off ray at emission:
+// 1 / (4 pi) for an isotropic point source, the entry's own for a table.
+// Returns false when the packet's position lies in no block.
+__device__ __forceinline__ bool emit_any( const fwd_params_t & P, long long pid, packet_t & p,
+                                          float & peel_I )
+{
+    if( P.pk_table == nullptr )
+    {
+        const src_dev_t & s = P.src[ pid % P.n_src ];
+        peel_I = s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC ? 0x1.45f306p-4f : 0.0f;
+        return emit_packet( P, pid, p, s, P.stream );
+    }
+    const kp_packet_init_t & e = P.pk_table[ pid - P.pk_pid0 ];
+    p.rng = phys::rng_t { P.seed, P.stream, ( uint32_t ) pid, ( uint32_t ) ( pid >> 32 ), 0u };
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) p.x[ a ] = e.x[ a ];
+    p.b = e.ib;
+    if( p.b < 0 )
+    {
+        if( ! locate_point( P, p.x, p.b, p.c ) ) return false;
+    }
+    else
+    {
+        if( p.b >= P.m.n_blocks ) return false;
+        cell_of( P.m, p.b, p.x, p.c );
+    }
+    p.d  = phys::v3 { e.d[ 0 ], e.d[ 1 ], e.d[ 2 ] };
+    p.e1 = phys::frame_for( p.d );
+    p.S  = phys::stokes_t { e.stokes[ 0 ], e.stokes[ 1 ], e.stokes[ 2 ] };
+    p.w  = e.w;
+    p.n_scat  = 0;
+    p.n_steps = 0;
+    set_inv( p );
+    peel_I = e.peel_I;
     return true;
 }
 

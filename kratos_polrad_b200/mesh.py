@@ -9,46 +9,12 @@ table, built by the C++ host code behind ``kp_mesh_create``.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
 
 import numpy as np
 
 from . import _lib
 from ._lib import call, ptr
-
-
-@dataclass
-class RefineRegion:
-    """One ``[refine_region*]`` section (meshgen.cpp:111-142)."""
-    level: int
-    x_min: tuple
-    x_max: tuple
-
-
-@dataclass
-class MeshConfig:
-    """The ``[mesh]`` / ``[boundary]`` / ``[refine_region*]`` keys."""
-    x_min: tuple
-    x_max: tuple
-    n_cell_global: tuple
-    n_cell_block: tuple = (16, 16, 16)
-    periodic: tuple = (False, False, False)
-    refine: list = field(default_factory=list)
-
-    def to_ini(self) -> str:
-        """INI text with the reference's section and key names."""
-        f = lambda v: " ".join(repr(float(t)) for t in v)
-        kinds = []
-        for a in range(3):
-            kinds += ["periodic", "periodic"] if self.periodic[a] else ["outflow", "outflow"]
-        lines = ["[mesh]", f"x_min = {f(self.x_min)}", f"x_max = {f(self.x_max)}",
-                 "n_cell_global = " + " ".join(str(int(v)) for v in self.n_cell_global),
-                 "n_cell_block = " + " ".join(str(int(v)) for v in self.n_cell_block),
-                 "", "[boundary]", "kinds = " + " ".join(kinds)]
-        for k, r in enumerate(self.refine):
-            lines += ["", f"[refine_region_{k:05d}]", f"level = {int(r.level)}",
-                      f"x_min = {f(r.x_min)}", f"x_max = {f(r.x_max)}"]
-        return "\n".join(lines) + "\n"
+from .config import MeshConfig, RefineRegion  # noqa: F401  (re-exported)
 
 
 class Mesh:

@@ -11,7 +11,9 @@ import math
 
 import numpy as np
 
+from . import problems
 from .mesh import Mesh, MeshConfig, RefineRegion
+from .problems import clump_mesh_config, root_refine_boxes  # noqa: F401  (re-exported)
 from .transport import (EMIT_ISOTROPIC, EMIT_UP_UNIFORM, PHASE_HG_POL, PHASE_RAYLEIGH,
                         SOURCE_PLANE_BASE, SOURCE_POINT, Source, TransportConfig)
 
@@ -25,69 +27,14 @@ def cell_centers(mesh: Mesh) -> np.ndarray:
     return (xf0[:, None, :] + idx[None] * dx0[:, None, :]).reshape(-1, 3)
 
 
-def root_refine_boxes(field_fn, n_root, block, box_lo, box_hi, threshold, level=1):
-    """One refine region per root block whose field exceeds ``threshold`` at
-    any root-cell centre (static, data-driven refinement expressed as the
-    reference's [refine_region*] boxes)."""
-    nb = [n_root[a] // block[a] for a in range(3)]
-    h = [(box_hi[a] - box_lo[a]) / n_root[a] for a in range(3)]
-    axes = [box_lo[a] + (np.arange(n_root[a]) + 0.5) * h[a] for a in range(3)]
-    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
-    f = field_fn(np.stack([X, Y, Z], -1)).reshape(nb[2], block[2], nb[1], block[1], nb[0], block[0])
-    fmax = f.max(axis=(1, 3, 5))
-    boxes = []
-    for kz, ky, kx in zip(*np.nonzero(fmax > threshold)):
-        lo = [box_lo[a] + (k + 0.25) * block[a] * h[a] for a, k in enumerate((kx, ky, kz))]
-        hi = [box_lo[a] + (k + 0.75) * block[a] * h[a] for a, k in enumerate((kx, ky, kz))]
-        boxes.append(RefineRegion(level, tuple(lo), tuple(hi)))
-    return boxes
-
-
-def clump_mesh_config(n_root=128, block=16, peak=100.0, fwhm=0.1) -> MeshConfig:
-    """Mesh of the 2-level AMR clump: root n_root^3 in block^3, refined x2
-    where the Gaussian clump's density (peak, FWHM in box units, on a unit
-    background) exceeds 3x its mean."""
-    s = fwhm / (2.0 * math.sqrt(2.0 * math.log(2.0)))
-
-    def rho(x):
-        r2 = ((np.asarray(x) - 0.5) ** 2).sum(-1)
-        return 1.0 + (peak - 1.0) * np.exp(-r2 / (2 * s * s))
-
-    n3 = (n_root,) * 3
-    g = (np.arange(n_root) + 0.5) / n_root
-    mean = (1.0 + (peak - 1.0) * np.exp(-((g - 0.5) ** 2) / (2 * s * s)).mean() ** 3)
-    boxes = root_refine_boxes(rho, n3, (block,) * 3, (0, 0, 0), (1, 1, 1), 3.0 * mean)
-    return MeshConfig((0, 0, 0), (1, 1, 1), n3, (block,) * 3, (False,) * 3, boxes)
-
-
 def clump_amr(n_packets=10_000_000, n_root=128, block=16, peak=100.0, fwhm=0.1, tau_edge=5.0,
               albedo=(0.5, 0.99), seed=2, image_n=128, inclination=90.0):
-    """Static 2-level AMR clump: root n_root^3 in block^3, refined x2 where the
-    density exceeds 3x its mean; Gaussian clump (peak, FWHM in box units) on a
-    unit background with centre-to-edge extinction depth tau_edge; per-cell
-    albedo log-uniform in [albedo]; isotropic point source at the centre;
-    peel-off image and int64 tallies."""
-    s = fwhm / (2.0 * math.sqrt(2.0 * math.log(2.0)))
-
-    def rho(x):
-        r2 = ((np.asarray(x) - 0.5) ** 2).sum(-1)
-        return 1.0 + (peak - 1.0) * np.exp(-r2 / (2 * s * s))
-
-    mesh = Mesh(clump_mesh_config(n_root, block, peak, fwhm))
-    c = cell_centers(mesh)
-    # extinction coefficient: integral of kappa*rho from the centre to a face = tau_edge
-    col = 0.5 + (peak - 1.0) * s * math.sqrt(math.pi / 2) * math.erf(0.5 / (s * math.sqrt(2)))
-    ext = (tau_edge / col) * rho(c)
-    rng = np.random.default_rng(seed)
-    alb = np.exp(rng.uniform(math.log(albedo[0]), math.log(albedo[1]), mesh.n_cells))
-    sigma2 = np.stack([ext * alb, ext * (1.0 - alb)], 1).astype(np.float32)
-    cfg = TransportConfig(n_packets=n_packets, seed=seed,
-                          sources=[Source(SOURCE_POINT, EMIT_ISOTROPIC, (0.5, 0.5, 0.5))],
-                          phase=PHASE_RAYLEIGH, n_mu_bins=20, mu_lo=-1.0, mu_hi=1.0,
-                          image_n=image_n, inclination_deg=inclination,
-                          image_center=(0.5, 0.5, 0.5), image_half_width=0.5,
-                          image_batch_n=8, n_batches=32, w_min=0.01, fx_shift=32)
-    return mesh, sigma2, cfg
+    """Static 2-level AMR clump (see problems.clump_spec): the mesh, its
+    per-cell coefficients and the transport configuration."""
+    mcfg, sigma_of, cfg = problems.clump_spec(n_packets, n_root, block, peak, fwhm, tau_edge,
+                                              albedo, seed, image_n, inclination)
+    mesh = Mesh(mcfg)
+    return mesh, sigma_of(cell_centers(mesh)), cfg
 
 
 def slab(n_packets=1_000_000, nx=128, ny=128, nz=64, block=16, tau=10.0, seed=1, n_mu=20):

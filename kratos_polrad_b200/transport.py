@@ -10,118 +10,19 @@ from __future__ import annotations
 
 import ctypes
 import math
-from dataclasses import dataclass, field
 
 import numpy as np
 import torch
 
 from . import _lib
 from ._lib import call, ptr
+from .config import (COUNTERS, EMIT_ISOTROPIC, EMIT_UP_UNIFORM, MAX_BATCHES,  # noqa: F401
+                     MAX_SOURCES, PACKET_INIT_DTYPE, PHASE_HG_POL, PHASE_RAYLEIGH, RECORD_DTYPE,
+                     SOURCE_PLANE_BASE, SOURCE_POINT, TALLY_FIXED, TALLY_FLOAT, CSource, CTallies,
+                     CTransportCfg, Source, TransportConfig)
 
-c_int, c_ll, c_float, c_double, c_void_p, c_u32 = (ctypes.c_int, ctypes.c_longlong,
-                                                   ctypes.c_float, ctypes.c_double,
-                                                   ctypes.c_void_p, ctypes.c_uint32)
-
-PHASE_RAYLEIGH, PHASE_HG_POL = 0, 1
-SOURCE_POINT, SOURCE_PLANE_BASE = 0, 1
-EMIT_ISOTROPIC, EMIT_UP_UNIFORM = 0, 1
-TALLY_FIXED, TALLY_FLOAT = 0, 1
-MAX_SOURCES, MAX_BATCHES = 64, 64
-COUNTERS = ("steps", "peel_steps", "scatter", "escaped", "absorbed", "capped", "lost",
-            "emitted", "hops", "deposits")
-
-
-class CSource(ctypes.Structure):
-    _fields_ = [("kind", c_int), ("emit", c_int), ("pos", c_double * 3)]
-
-
-class CTransportCfg(ctypes.Structure):
-    _fields_ = [("n_packets", c_ll), ("packet_offset", c_ll), ("seed", c_u32),
-                ("stream_id", c_u32), ("phase", c_int), ("hg_g", c_float),
-                ("pol_max", c_float), ("n_sources", c_int), ("sources", ctypes.POINTER(CSource)),
-                ("n_mu_bins", c_int), ("mu_lo", c_float), ("mu_hi", c_float),
-                ("image_n", c_int), ("inclination_deg", c_double), ("azimuth_deg", c_double),
-                ("image_center", c_double * 3), ("image_half_width", c_double),
-                ("tau_peel_max", c_float), ("tally_mode", c_int), ("fx_shift", c_int),
-                ("n_batches", c_int), ("image_batch_n", c_int), ("w_min", c_float),
-                ("rr_survive", c_float),
-                ("max_scatter", c_int), ("max_steps", c_ll), ("n_record", c_ll),
-                ("lane_batch", c_int), ("flux_fx_shift", c_int)]
-
-
-class CTallies(ctypes.Structure):
-    _fields_ = [("mu", c_void_p), ("image", c_void_p), ("image_batch", c_void_p),
-                ("counters", c_void_p), ("records", c_void_p), ("flux", c_void_p)]
-
-
-# numpy view of kp_packet_record_t (88 bytes)
-RECORD_DTYPE = np.dtype([("x", "<f8", 3), ("d", "<f4", 3), ("stokes", "<f4", 3), ("w", "<f4"),
-                         ("ib", "<i4"), ("cell", "<i4", 3), ("n_scatter", "<i4"),
-                         ("status", "<i4"), ("rng_draws", "<u4"), ("n_steps", "<i8")])
-assert RECORD_DTYPE.itemsize == 88
-
-_lib.register("kp_transport_forward", [c_void_p, ctypes.POINTER(CTransportCfg),
-                                       ctypes.POINTER(CTallies), c_void_p])
-
-
-@dataclass
-class Source:
-    kind: int = SOURCE_POINT
-    emit: int = EMIT_ISOTROPIC
-    pos: tuple = (0.0, 0.0, 0.0)
-
-
-@dataclass
-class TransportConfig:
-    """Python form of ``kp_transport_cfg_t`` (see include/kp_transport.h)."""
-    n_packets: int
-    sources: list
-    seed: int = 1
-    stream_id: int = 0
-    packet_offset: int = 0
-    phase: int = PHASE_RAYLEIGH
-    hg_g: float = 0.0
-    pol_max: float = 1.0
-    n_mu_bins: int = 0
-    mu_lo: float = 0.0
-    mu_hi: float = 1.0
-    image_n: int = 0
-    inclination_deg: float = 90.0
-    azimuth_deg: float = 0.0
-    image_center: tuple = (0.0, 0.0, 0.0)
-    image_half_width: float = 1.0
-    tau_peel_max: float = 40.0
-    tally_mode: int = TALLY_FIXED
-    fx_shift: int = 32
-    n_batches: int = 32
-    image_batch_n: int = 1
-    w_min: float = 0.0
-    rr_survive: float = 0.1
-    max_scatter: int = 100000
-    max_steps: int = 1 << 24
-    n_record: int = 0
-    lane_batch: int = 0
-    flux_fx_shift: int = 24
-    # Python side only: keep the per-cell path-length flux tally (rad_t::flx)
-    flux: bool = False
-
-    def to_c(self):
-        src = (CSource * max(1, len(self.sources)))()
-        for k, s in enumerate(self.sources):
-            src[k].kind, src[k].emit = int(s.kind), int(s.emit)
-            for a in range(3):
-                src[k].pos[a] = float(s.pos[a])
-        c = CTransportCfg()
-        for name, _ in CTransportCfg._fields_:
-            if name in ("sources", "n_sources", "image_center"):
-                continue
-            setattr(c, name, getattr(self, name))
-        c.n_sources = len(self.sources)
-        c.sources = ctypes.cast(src, ctypes.POINTER(CSource))
-        for a in range(3):
-            c.image_center[a] = float(self.image_center[a])
-        c._keep = src
-        return c
+_lib.register("kp_transport_forward", [ctypes.c_void_p, ctypes.POINTER(CTransportCfg),
+                                       ctypes.POINTER(CTallies), ctypes.c_void_p])
 
 
 class Tallies:
@@ -207,6 +108,29 @@ def forward(mesh, cfg: TransportConfig, tallies: Tallies | None = None,
     else:
         call("kp_transport_forward", mesh.handle, ctypes.byref(c), ctypes.byref(t), s)
     return tallies
+
+
+def packet_array(x, d, w=1.0, stokes=None, ib=-1, peel_I=0.0) -> np.ndarray:
+    """Host array of kp_packet_init_t records (PACKET_INIT_DTYPE): positions
+    x [n, 3], unit directions d [n, 3], weights w, Stokes (q, u, v) relative
+    to the packet's frame (default unpolarized), block ids (-1: located on the
+    device) and the emission's intensity per steradian toward the observer
+    per unit weight (0: no peel-off ray at emission)."""
+    x = np.asarray(x, np.float64).reshape(-1, 3)
+    a = np.zeros(len(x), PACKET_INIT_DTYPE)
+    a["x"] = x
+    a["d"] = np.asarray(d, np.float32).reshape(-1, 3)
+    a["w"] = w
+    if stokes is not None:
+        a["stokes"] = np.asarray(stokes, np.float32).reshape(-1, 3)
+    a["ib"] = ib
+    a["peel_I"] = peel_I
+    return a
+
+
+def packet_table(records: np.ndarray, device="cuda") -> torch.Tensor:
+    """Device copy ([n, 64] uint8) of packet_array records, for cfg.packets."""
+    return torch.from_numpy(np.ascontiguousarray(records).view(np.uint8).reshape(-1, 64)).to(device)
 
 
 def polarization(I, Q, U):

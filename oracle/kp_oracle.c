@@ -276,7 +276,12 @@ static int tcross( const tctx * t, int * b, int * c, double * x, int ax, int pos
         return 1;
     }
     const int side = pos ? 1 : 0;
-    if( m->phybnd[ 6 * * b + 2 * ax + side ] ) return 0;
+    if( m->phybnd[ 6 * * b + 2 * ax + side ] )
+    {   /* leaves the domain: the position ends on the boundary face */
+        x[ ax ] = fma( ( double ) ( pos ? c[ ax ] + 1 : c[ ax ] ), m->dx0[ 3 * * b + ax ],
+                       m->xf0[ 3 * * b + ax ] );
+        return 0;
+    }
     const int a1 = ( ax + 1 ) % 3, a2 = ( ax + 2 ) % 3;
     int j0 = 0, j1 = 0;
     if( m->d_lvl[ 6 * * b + 2 * ax + side ] > 0 )
@@ -422,14 +427,71 @@ static om_v3 temit_dir( om_rng * g, int emit )
     return om_dir_from( mu, a / rr, b / rr );
 }
 
-static int temit( const tctx * t, const kpo_cfg_t * c, long long pid, tpk * p )
+/* Cell of block b holding x (floor, clamped to the block). */
+static void tcell_of( const tctx * t, int b, const double * x, int * c )
+{
+    const kpo_mesh_t * m = t->m;
+    for( int a = 0; a < 3; ++ a )
+    {
+        const double f = floor( ( x[ a ] - m->xf0[ 3 * b + a ] ) * t->inv_dx[ 3 * b + a ] );
+        c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( m->nc[ a ] - 1 ) ? m->nc[ a ] - 1 : ( int ) f );
+    }
+}
+
+/* Block and cell of x through the finest-level lookup grid; 0 if none. */
+static int tlocate( const tctx * t, const double * x, int * b, int * c )
+{
+    const kpo_mesh_t * m = t->m;
+    int li[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+    {
+        const double f = floor( ( x[ a ] - m->xlim[ 0 ][ a ] ) * t->lk_inv[ a ] );
+        li[ a ] = f < 0.0 ? 0 : ( f >= t->lk_n[ a ] ? t->lk_n[ a ] - 1 : ( int ) f );
+    }
+    * b = t->lookup[ ( ( long ) li[ 2 ] * t->lk_n[ 1 ] + li[ 1 ] ) * t->lk_n[ 0 ] + li[ 0 ] ];
+    if( * b < 0 || * b >= m->n_blocks ) return 0;
+    tcell_of( t, * b, x, c );
+    return 1;
+}
+
+/* Creates packet pid: from the caller's packet table (entry pid -
+ * packet_offset) when the cfg has one, else from source pid % n_sources.
+ * peel_I receives the emission's intensity per steradian toward the
+ * observer per unit weight (1/(4 pi) for an isotropic point source, the
+ * entry's own for a table; 0: no peel-off at emission). */
+static int temit( const tctx * t, const kpo_cfg_t * c, long long pid, tpk * p, float * peel_I )
 {
     const kpo_mesh_t * m = t->m;
     p->pid = pid;
     p->rng.k0 = c->seed; p->rng.k1 = c->stream_id;
     p->rng.pid_lo = ( uint32_t ) pid; p->rng.pid_hi = ( uint32_t ) ( pid >> 32 );
     p->rng.draw = 0;
+    if( c->packets )
+    {
+        const kpo_packet_init_t * e = c->packets + ( pid - c->packet_offset );
+        for( int a = 0; a < 3; ++ a ) p->x[ a ] = e->x[ a ];
+        p->b = e->ib;
+        if( p->b < 0 )
+        {
+            if( ! tlocate( t, p->x, & p->b, p->c ) ) return 0;
+        }
+        else
+        {
+            if( p->b >= m->n_blocks ) return 0;
+            tcell_of( t, p->b, p->x, p->c );
+        }
+        p->d.x = e->d[ 0 ]; p->d.y = e->d[ 1 ]; p->d.z = e->d[ 2 ];
+        p->e1 = om_frame_for( p->d );
+        p->S.q = e->stokes[ 0 ]; p->S.u = e->stokes[ 1 ]; p->S.v = e->stokes[ 2 ];
+        p->w = e->w;
+        p->n_scat = 0;
+        p->n_steps = 0;
+        tset_inv( p );
+        * peel_I = e->peel_I;
+        return 1;
+    }
     const kpo_source_t * s = c->sources + pid % c->n_sources;
+    * peel_I = s->kind == 0 && s->emit == 0 ? 0x1.45f306p-4f : 0.0f;
     if( s->kind == 0 )
     {
         for( int a = 0; a < 3; ++ a ) { p->x[ a ] = s->pos[ a ]; p->c[ a ] = s->cell[ a ]; }
@@ -441,19 +503,7 @@ static int temit( const tctx * t, const kpo_cfg_t * c, long long pid, tpk * p )
         p->x[ 0 ] = fma( ( double ) om_u01( r.x ), m->lbox[ 0 ], m->xlim[ 0 ][ 0 ] );
         p->x[ 1 ] = fma( ( double ) om_u01( r.y ), m->lbox[ 1 ], m->xlim[ 0 ][ 1 ] );
         p->x[ 2 ] = m->xlim[ 0 ][ 2 ];
-        int li[ 3 ];
-        for( int a = 0; a < 3; ++ a )
-        {
-            const double f = floor( ( p->x[ a ] - m->xlim[ 0 ][ a ] ) * t->lk_inv[ a ] );
-            li[ a ] = f < 0.0 ? 0 : ( f >= t->lk_n[ a ] ? t->lk_n[ a ] - 1 : ( int ) f );
-        }
-        p->b = t->lookup[ ( ( long ) li[ 2 ] * t->lk_n[ 1 ] + li[ 1 ] ) * t->lk_n[ 0 ] + li[ 0 ] ];
-        if( p->b < 0 || p->b >= m->n_blocks ) return 0;
-        for( int a = 0; a < 3; ++ a )
-        {
-            const double f = floor( ( p->x[ a ] - m->xf0[ 3 * p->b + a ] ) * t->inv_dx[ 3 * p->b + a ] );
-            p->c[ a ] = f < 0.0 ? 0 : ( f > ( double ) ( m->nc[ a ] - 1 ) ? m->nc[ a ] - 1 : ( int ) f );
-        }
+        if( ! tlocate( t, p->x, & p->b, p->c ) ) return 0;
     }
     if( p->b < 0 || p->b >= m->n_blocks ) return 0;
     p->d = temit_dir( & p->rng, s->emit );
@@ -544,10 +594,10 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
     for( long long k = 0; k < c->n_packets; ++ k )
     {
         tpk p;
-        if( ! temit( & t, c, c->packet_offset + k, & p ) ) { free( t.inv_dx ); return -1; }
+        float peel_I;
+        if( ! temit( & t, c, c->packet_offset + k, & p, & peel_I ) ) { free( t.inv_dx ); return -1; }
         ++ cnt[ 7 ];
-        const kpo_source_t * s = c->sources + p.pid % c->n_sources;
-        if( t.img_n > 0 && s->kind == 0 && s->emit == 0 )
+        if( t.img_n > 0 && peel_I > 0.0f )
         {   /* direct light: peel-off rays start only inside the image */
             const int pix = timage_pixel( & t, p.x );
             if( pix >= 0 )
@@ -555,8 +605,8 @@ int kpo_transport( const kpo_mesh_t * m, const float * sigma2, const int * looku
                 const float tau = tpeel_tau( & t, p.b, p.c, p.x, & cnt[ 1 ], & cnt[ 8 ] );
                 if( tau <= t.tau_cut )
                 {
-                    const float att = 1.0f * ( float ) om_exp_neg( -( double ) tau );
-                    tdeposit_pixel( & t, pix, p.pid, att * 0x1.45f306p-4f, att * 0.0f,
+                    const float att = p.w * ( float ) om_exp_neg( -( double ) tau );
+                    tdeposit_pixel( & t, pix, p.pid, att * peel_I, att * 0.0f,
                                     att * 0.0f, att * 0.0f );
                     ++ cnt[ 9 ];
                 }
@@ -747,12 +797,12 @@ static int tadjoint_pass( const tctx * t, const kpo_cfg_t * c, long long pid, in
                           unsigned long long * cnt )
 {
     tpk p;
-    if( ! temit( t, c, pid, & p ) ) return -1;
-    const kpo_source_t * s = c->sources + pid % c->n_sources;
+    float peel_I;
+    if( ! temit( t, c, pid, & p, & peel_I ) ) return -1;
     p.tau = tsample_tau( & p.rng );
     double R = pass == 1 ? * Rp : 0.0;
     int nv = 0;
-    if( t->img_n > 0 && s->kind == 0 && s->emit == 0 )
+    if( t->img_n > 0 && peel_I > 0.0f )
     {
         const int pix = timage_pixel( t, p.x );
         if( pix >= 0 )
@@ -763,8 +813,8 @@ static int tadjoint_pass( const tctx * t, const kpo_cfg_t * c, long long pid, in
                 float G = 0.0f;
                 if( tau <= t->tau_cut )
                 {
-                    const float att = 1.0f * ( float ) om_exp_neg( -( double ) tau );
-                    G = tscore( g, pix, att * 0x1.45f306p-4f, att * 0.0f, att * 0.0f, att * 0.0f );
+                    const float att = p.w * ( float ) om_exp_neg( -( double ) tau );
+                    G = tscore( g, pix, att * peel_I, att * 0.0f, att * 0.0f, att * 0.0f );
                 }
                 * G0 = G;
             }

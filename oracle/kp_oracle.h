@@ -78,6 +78,18 @@ typedef struct kpo_source
     int    cell[ 3 ];
 } kpo_source_t;
 
+/* A caller-made packet (the layout of kp_packet_init_t). */
+typedef struct kpo_packet_init
+{
+    double x[ 3 ];
+    float  d[ 3 ];
+    float  w;
+    float  stokes[ 3 ];
+    int    ib;
+    float  peel_I;
+    int    pad;
+} kpo_packet_init_t;
+
 typedef struct kpo_cfg
 {
     long long n_packets, packet_offset;
@@ -101,6 +113,7 @@ typedef struct kpo_cfg
     long long max_steps;
     long long n_record;
     int       flux_fx_shift;    /* flux tally scale 2^flux_fx_shift (0: fx_shift) */
+    const kpo_packet_init_t * packets;  /* [n_packets] or NULL: the sources */
 } kpo_cfg_t;
 
 typedef struct kpo_record

@@ -134,7 +134,33 @@ class _Cfg(ctypes.Structure):
                 ("n_batches", ctypes.c_int), ("image_batch_n", ctypes.c_int),
                 ("w_min", ctypes.c_float), ("rr_survive", ctypes.c_float),
                 ("max_scatter", ctypes.c_int), ("max_steps", ctypes.c_longlong),
-                ("n_record", ctypes.c_longlong), ("flux_fx_shift", ctypes.c_int)]
+                ("n_record", ctypes.c_longlong), ("flux_fx_shift", ctypes.c_int),
+                ("packets", ctypes.c_void_p)]
+
+
+def _cfg_struct(cfg, src):
+    """kpo_cfg_t of a TransportConfig-like cfg; a packet table (cfg.packets,
+    records of kp_packet_init_t's layout, host or device) is copied to the
+    host and kept alive by the struct."""
+    c = _Cfg()
+    for name, _ in _Cfg._fields_:
+        if name in ("sources", "n_sources", "image_center", "packets"):
+            continue
+        setattr(c, name, getattr(cfg, name, 0))
+    c.n_sources = len(cfg.sources)
+    c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
+    for a in range(3):
+        c.image_center[a] = float(cfg.image_center[a])
+    pk = getattr(cfg, "packets", None)
+    if pk is not None:
+        if hasattr(pk, "cpu"):
+            pk = pk.cpu().numpy()
+        pk = np.ascontiguousarray(pk).view(np.uint8).reshape(-1)
+        if pk.size < 64 * cfg.n_packets:
+            raise ValueError("packet table shorter than n_packets")
+        c.packets = pk.ctypes.data
+        c._keep = pk
+    return c
 
 
 def lookup_grid(levels, regs, nc_root_blocks):
@@ -164,15 +190,7 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, flux=Fal
         src[k].ib = int(ib)
         for a in range(3):
             src[k].cell[a] = int(cell[a])
-    c = _Cfg()
-    for name, _ in _Cfg._fields_:
-        if name in ("sources", "n_sources", "image_center"):
-            continue
-        setattr(c, name, getattr(cfg, name, 0))
-    c.n_sources = len(cfg.sources)
-    c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
-    for a in range(3):
-        c.image_center[a] = float(cfg.image_center[a])
+    c = _cfg_struct(cfg, src)
     nm = max(cfg.n_mu_bins, 1)
     ni = max(cfg.image_n, 1)
     out = dict(mu=np.zeros((cfg.n_batches, nm, 4), np.int64),
@@ -214,15 +232,7 @@ def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, g
         src[k].ib = int(ib)
         for a in range(3):
             src[k].cell[a] = int(cell[a])
-    c = _Cfg()
-    for name, _ in _Cfg._fields_:
-        if name in ("sources", "n_sources", "image_center"):
-            continue
-        setattr(c, name, getattr(cfg, name, 0))
-    c.n_sources = len(cfg.sources)
-    c.sources = ctypes.cast(src, ctypes.POINTER(_Source))
-    for a in range(3):
-        c.image_center[a] = float(cfg.image_center[a])
+    c = _cfg_struct(cfg, src)
     n_cells = tab.n_blocks * tab.cells_per_block
     g_len, g_int = np.zeros(n_cells, np.int64), np.zeros(n_cells, np.int64)
     cnt = np.zeros(10, np.uint64)

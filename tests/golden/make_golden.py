@@ -176,7 +176,10 @@ def make_sph(precision, n=256, budget=120):
 if __name__ == "__main__":
     if not refharness.available(1):
         sys.exit("oracle/_ref not built: make -C oracle ref REF=<reference tree>")
-    ref_tree = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the reference checkout: argument, $KP_REFERENCE_SRC, or a "reference"
+    # directory beside this repository
+    ref_tree = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get(
+        "KP_REFERENCE_SRC", os.path.join(os.path.dirname(ROOT), "reference")))
     for name, prec in FIXTURES:
         print(*make(name, prec))
     for p in make_bio(ref_tree):

@@ -9,12 +9,12 @@ import torch
 from kratos_polrad_b200.adjoint import TransportImage, adjoint, gradients
 from kratos_polrad_b200.transport import TALLY_FLOAT
 from oracle import port
-from transport_cases import case, run_oracle_adjoint
+from transport_cases import case, run_oracle_adjoint, to_device
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not port.available(), reason="oracle not built")]
 
 
-@pytest.mark.parametrize("name", ["amr_point", "hg_multi"])
+@pytest.mark.parametrize("name", ["amr_point", "hg_multi", "table"])
 def test_adjoint_bit_exact(name):
     mesh, sig, t = case(name)
     t = dataclasses.replace(t, n_record=0)
@@ -22,7 +22,7 @@ def test_adjoint_bit_exact(name):
     rng = np.random.default_rng(1)
     adj = rng.normal(size=(t.image_n, t.image_n, 4)).astype(np.float32)
     cnt = torch.zeros(10, dtype=torch.int64, device="cuda")
-    gl, gi = adjoint(mesh, t, torch.tensor(adj, device="cuda"), 24, counters=cnt)
+    gl, gi = adjoint(mesh, to_device(t), torch.tensor(adj, device="cuda"), 24, counters=cnt)
     torch.cuda.synchronize()
     assert mesh.status() == 0
     rl, ri, rc = run_oracle_adjoint(mesh, sig, t, adj, 24)
@@ -79,7 +79,7 @@ def test_autograd_backward_is_the_adjoint():
     assert torch.isfinite(sca.grad).all() and sca.grad.abs().sum() > 0
 
 
-@pytest.mark.parametrize("name", ["amr_point", "hg_multi"])
+@pytest.mark.parametrize("name", ["amr_point", "hg_multi", "table"])
 def test_adjoint_small_queue_bit_exact(name):
     """A queue of 1024 vertex rays: the adjoint runs in chunks of 85 packets,
     and the packets whose rays find the queue full are replayed inline by
@@ -92,7 +92,7 @@ def test_adjoint_small_queue_bit_exact(name):
     cnt = torch.zeros(10, dtype=torch.int64, device="cuda")
     call("kp_mesh_peel_queue_limit", mesh.handle, 1024)
     try:
-        gl, gi = adjoint(mesh, t, torch.tensor(adj, device="cuda"), 24, counters=cnt)
+        gl, gi = adjoint(mesh, to_device(t), torch.tensor(adj, device="cuda"), 24, counters=cnt)
         torch.cuda.synchronize()
         assert mesh.status() == 0
     finally:

@@ -3,6 +3,10 @@ traffic read from the committed ncu summary, the algorithmic bytes of a
 solve, and the workload description."""
 import importlib.util
 import os
+import sys
+
+import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -35,3 +39,33 @@ def test_workload_names_the_configuration():
     w = b.workload_config(cfg, 10_000_000)
     assert w["workload"] == "clump_amr_2level" and w["packets_per_gpu"] == 10_000_000
     assert w["l2"].startswith("flushed")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libkpref_p2.so")),
+                    reason="reference walk not built")
+def test_reference_arm_does_not_load_the_product():
+    """The CPU arm builds its scene on the reference's own mesh code and runs
+    the restatement: in a fresh process, libkp_b200.so is never mapped, and
+    the scene equals the product's (same blocks, coefficients, source cell)."""
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from oracle import ref_scene\n"
+            "tab, sig, grid, gn, cfg, cells = ref_scene.clump(1000)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libkp_b200' not in maps, 'product library mapped'\n"
+            "assert 'libkpref_p2' in maps\n"
+            "import numpy as np\n"
+            "np.save(sys.argv[1], np.concatenate([sig.ravel().astype(np.float64), "
+            "tab.xf0.ravel(), [cells[0][0]], cells[0][1]]))\n" % ROOT)
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "scene.npy")
+        r = subprocess.run([sys.executable, "-c", code, out], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        got = np.load(out)
+    from kratos_polrad_b200 import scenes
+    mesh, sig, cfg = scenes.clump_amr(n_packets=1000)
+    ib, cell = mesh.locate([cfg.sources[0].pos])
+    xf0, _, _, _ = mesh.geometry(8)
+    want = np.concatenate([sig.ravel().astype(np.float64), xf0.ravel(), [ib[0]], cell[0]])
+    np.testing.assert_array_equal(got, want)

@@ -138,7 +138,7 @@ def test_gpu_sph_walk_matches_golden(path, tmp_path):
     the same state."""
     import torch
     from kratos_polrad_b200 import PacketPool
-    from kratos_polrad_b200.trace import trace_sph
+    from kratos_polrad_b200.walk import trace_sph
     g, mesh, perm = load_sph(path, tmp_path)
     tdt = torch.float32 if int(g["precision"]) == 1 else torch.float64
     dev = torch.device("cuda")

@@ -95,3 +95,34 @@ def test_hg_mean_cosine(g):
     # polarization at 90 degrees: -pmax (1-mu^2)/(1+mu^2) for unpolarized light
     m = np.abs(mu) < 0.05
     np.testing.assert_allclose(o[m, 6], -0.5 * (1 - mu[m] ** 2) / (1 + mu[m] ** 2), atol=3e-6)
+
+
+def test_packet_table_emission_restatement():
+    """Packets from a caller's table start where the table says: with zero
+    coefficients each walks straight from its entry, its record keeps the
+    entry's direction, weight and Stokes vector, and located and given
+    blocks agree."""
+    import dataclasses
+    import sys, os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from transport_cases import case, run_oracle
+    mesh, sig, t = case("table")
+    t = dataclasses.replace(t, image_n=0, n_mu_bins=0)
+    o = run_oracle(mesh, np.zeros_like(sig), t)
+    rec, tab = o["records"], t.packets
+    np.testing.assert_array_equal(rec["d"], tab["d"])
+    np.testing.assert_array_equal(rec["w"], tab["w"])
+    np.testing.assert_array_equal(rec["stokes"], tab["stokes"])
+    assert (rec["status"] == 1).all() and (rec["n_scatter"] == 0).all()
+    # every packet left along its straight line from the entry's position,
+    # through the boundary
+    lo, hi = np.array(mesh.x_min), np.array(mesh.x_max)
+    assert (np.isclose(rec["x"], lo, atol=1e-12) | np.isclose(rec["x"], hi, atol=1e-12)).any(1).all()
+    r = rec["x"] - tab["x"]
+    cr = np.cross(r, tab["d"].astype(np.float64))
+    assert np.abs(cr).max() < 1e-6
+    # the same packets with every block left to the device: same walks
+    t2 = dataclasses.replace(t, packets=tab.copy())
+    t2.packets["ib"] = -1
+    o2 = run_oracle(mesh, np.zeros_like(sig), t2)
+    np.testing.assert_array_equal(o2["records"], rec)

@@ -101,7 +101,7 @@ def packets(mesh, cfg, n, ftype, seed, budget=400):
 def _gpu_walk(prod, arrays, sel, tdt, fx_shift=16):
     import torch
     from kratos_polrad_b200 import PacketPool
-    from kratos_polrad_b200.trace import trace_sph
+    from kratos_polrad_b200.walk import trace_sph
     x, xc, d, cell, ib, proper, steps = (a[sel] for a in arrays)
     dev = torch.device("cuda")
     T = lambda a, dt=None: torch.tensor(a, dtype=dt, device=dev)

@@ -12,16 +12,18 @@ import torch
 
 from kratos_polrad_b200.transport import TALLY_FLOAT, Tallies, forward
 from oracle import port
-from transport_cases import case, run_oracle
+from transport_cases import case, run_oracle, to_device
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not port.available(), reason="oracle not built")]
 
 
-@pytest.mark.parametrize("name", ["slab", "amr_point", "hg_multi"])
+@pytest.mark.parametrize("name", ["slab", "amr_point", "hg_multi", "table"])
 def test_transport_bit_exact(name):
+    """"table": packets made by a user generator (kp_packet_init_t) instead
+    of a source."""
     mesh, sig, t = case(name)
     mesh.set_sigma(sig)
-    tal = forward(mesh, t)
+    tal = forward(mesh, to_device(t))
     torch.cuda.synchronize()
     assert mesh.status() == 0
     ref = run_oracle(mesh, sig, t)
@@ -67,7 +69,7 @@ def test_float_tally_mode_close_to_fixed():
     np.testing.assert_allclose(img_fl[..., 0].sum(), img_fx[..., 0].sum(), rtol=1e-6)
 
 
-@pytest.mark.parametrize("name", ["amr_point", "hg_multi"])
+@pytest.mark.parametrize("name", ["amr_point", "hg_multi", "table"])
 def test_chunked_solve_with_small_peel_queue(name):
     """A peel-off queue of 1024 rays: the solve runs in chunks of 85 packets,
     and chunks whose packets queue more rays than that march the rest where
@@ -77,7 +79,7 @@ def test_chunked_solve_with_small_peel_queue(name):
     mesh.set_sigma(sig)
     call("kp_mesh_peel_queue_limit", mesh.handle, 1024)
     try:
-        tal = forward(mesh, t)
+        tal = forward(mesh, to_device(t))
         torch.cuda.synchronize()
         assert mesh.status() == 0
     finally:

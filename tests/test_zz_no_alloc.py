@@ -31,23 +31,50 @@ def _noalloc(mesh, cfg, tallies, stream):
 
 
 @pytest.mark.gpu
-def test_noalloc_matches_forward_on_two_calls():
+@pytest.mark.parametrize("name", ["amr_point", "slab"])
+def test_noalloc_matches_forward_on_two_calls(name):
+    """With an image (amr_point: the walk marches its peel-off rays inline,
+    the ordinary entry point queues them) and without (slab: both run the
+    same kernel); the flux tally too.  int64 tallies: no tolerance."""
+    import dataclasses
     import torch
-    mesh, sig, cfg = case("amr_point")
+    mesh, sig, cfg = case(name)
+    cfg = dataclasses.replace(cfg, flux=True, flux_fx_shift=24)
     mesh.set_sigma(sig)                      # set-up: puts the mesh on the device
     ref = forward(mesh, cfg)
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(2):
-        tal = Tallies(cfg)
+        tal = Tallies(cfg, n_cells=mesh.n_cells)
         _noalloc(mesh, cfg, tal, stream)
         torch.cuda.synchronize()
         assert mesh.status() == 0
-        for name in ("mu", "image", "image_batch", "counters"):
+        for name in ("mu", "image", "image_batch", "counters", "flux"):
             assert torch.equal(getattr(tal, name), getattr(ref, name)), name
         a, b = tal.record_array(), ref.record_array()
         for f in a.dtype.names:
             np.testing.assert_array_equal(a[f], b[f], err_msg=f)
+
+
+@pytest.mark.gpu
+def test_noalloc_float_tallies_within_rounding():
+    """Float tallies: the inline peel-off rays add into the image in another
+    order than the queued ones, so the two agree within float rounding."""
+    import dataclasses
+    import torch
+    from kratos_polrad_b200.transport import TALLY_FLOAT
+    mesh, sig, cfg = case("amr_point")
+    cfg = dataclasses.replace(cfg, tally_mode=TALLY_FLOAT, n_record=0)
+    mesh.set_sigma(sig)
+    ref = forward(mesh, cfg)
+    tal = Tallies(cfg)
+    _noalloc(mesh, cfg, tal, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert mesh.status() == 0
+    a, b = tal.image.cpu().numpy(), ref.image.cpu().numpy()
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(b).max())
+    assert abs(a[..., 0].sum() - b[..., 0].sum()) <= 1e-6 * abs(b[..., 0].sum())
+    assert torch.equal(tal.counters, ref.counters)
 
 
 def test_noalloc_refuses_mesh_not_on_device():

@@ -4,7 +4,7 @@ import numpy as np
 from kratos_polrad_b200 import Mesh
 from kratos_polrad_b200.transport import (EMIT_ISOTROPIC, EMIT_UP_UNIFORM, PHASE_HG_POL,
                                           PHASE_RAYLEIGH, SOURCE_PLANE_BASE, SOURCE_POINT,
-                                          Source, TransportConfig)
+                                          Source, TransportConfig, packet_array)
 from meshcases import AMR_BOX, AMR_PERIODIC
 from kratos_polrad_b200.mesh import MeshConfig
 from oracle import port
@@ -53,9 +53,45 @@ def case(name):
                             image_center=(0, 0, 1.5), image_half_width=2.5, w_min=0.02,
                             n_mu_bins=16, mu_lo=-1, mu_hi=1, n_record=1500, max_scatter=200,
                             tau_peel_max=20.0)
+    elif name == "table":
+        # a user generator's packets: a ring of emitters with directions,
+        # weights and polarization of its own; half give their block, half
+        # are located on the device; half peel off toward the observer
+        mesh = Mesh(AMR_BOX)
+        c = cell_centers(mesh)
+        rng = np.random.default_rng(8)
+        ext = 2.0 + 6.0 * np.exp(-((c - 0.5) ** 2).sum(1) / (2 * 0.1 ** 2))
+        alb = rng.uniform(0.6, 0.95, mesh.n_cells)
+        sig = np.stack([ext * alb, ext * (1 - alb)], 1).astype(np.float32)
+        n = 1500
+        ang = rng.uniform(0, 2 * np.pi, n)
+        x = np.stack([0.5 + 0.2 * np.cos(ang), 0.5 + 0.2 * np.sin(ang),
+                      rng.uniform(0.3, 0.7, n)], 1)
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pol = np.zeros((n, 3))
+        pol[::3, 0] = 0.4
+        pol[1::3, 1] = -0.3
+        ib, _ = mesh.locate(x)
+        ib = np.where(np.arange(n) % 2 == 0, ib, -1)
+        table = packet_array(x, d, w=rng.uniform(0.5, 2.0, n), stokes=pol, ib=ib,
+                             peel_I=np.where(np.arange(n) % 2 == 0, 1 / (4 * np.pi), 0.0))
+        t = TransportConfig(n_packets=n, sources=[], seed=9, image_n=32, inclination_deg=45.0,
+                            azimuth_deg=30.0, image_center=(0.5, 0.5, 0.5), image_half_width=0.87,
+                            w_min=0.05, image_batch_n=4, n_mu_bins=8, mu_lo=-1, mu_hi=1,
+                            n_record=n, packets=table)
     else:
         raise KeyError(name)
     return mesh, sig, t
+
+
+def to_device(t):
+    """The cfg with its packet table (if any) copied to the GPU."""
+    import dataclasses
+    from kratos_polrad_b200.transport import packet_table
+    if t.packets is None or hasattr(t.packets, "data_ptr"):
+        return t
+    return dataclasses.replace(t, packets=packet_table(t.packets))
 
 
 def run_oracle(mesh, sig, t):
