@@ -568,6 +568,36 @@ int kp_transport_forward_dd( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                              void * stream );
 
 /* ------------------------------------------------------------------ */
+/* The particle radiation module's configuration: the [particle],        */
+/* [particles] and [device] keys that particle::base_t and its drivers   */
+/* read in their init() (reference defaults in parentheses).  The module */
+/* layer above the ABI (include/kp_module.hpp) uses n_par (packets per   */
+/* cycle), step_max (segments per packet), n_hv (flux fields; the walk   */
+/* deposits into field 0 as photon.h:81 does), n_cycle_stp (cycles per   */
+/* step), seed_rng, idx_device and n_th (generator threads per block);   */
+/* max_round, static_proxy, output and f_par are read and kept for the  */
+/* caller.                                                               */
+
+typedef struct kp_particle_cfg
+{
+    double n_par;        /* [particle] n_par (1.0)        generate_par.h:38   */
+    double f_par;        /* [particle] f_par (1.0)        generate_par.h:40   */
+    int    step_max;     /* [particle] step_max (100)     generate_par.h:36   */
+    int    n_hv;         /* [particle] n_hv (1)           radiation.h:26      */
+    int    n_cycle_stp;  /* [particle] n_cycle_stp (1)    driver.cpp:18       */
+    int    n_th;         /* [particle] n_th (64)          driver_base.h:30    */
+    int    max_round;    /* [particle] max_round (16)     integrator.h:35     */
+    int    static_proxy; /* [particle] static_proxy (0)   block_map.h:39      */
+    int    output;       /* [particles] output (1)        particle_pool.h:50  */
+    int    seed_rng;     /* [device] seed_rng (7)         device.cpp:69       */
+    int    idx_device;   /* [device] idx_device (-1)      device.cpp:67       */
+} kp_particle_cfg_t;
+
+/* Reads those keys from an INI file with the reference's syntax (later
+ * values override earlier ones, io/args/input.cpp:72-108). */
+int kp_particle_read( const char * ini_path, kp_particle_cfg_t * out );
+
+/* ------------------------------------------------------------------ */
 /* Binary container of the reference's binary_io (io/binary/            */
 /* binary_io.h:6-32; save/load in binary_io_base.cpp:89-131): a byte of */
 /* (little-endian | sizeof(size_t)), the header size, a tag-sorted map  */

@@ -142,6 +142,8 @@ class Rank:
         self.out_count.zero_()
         cfg = dataclasses.replace(self.cfg, packet_offset=self.cfg.packet_offset + emit_offset,
                                   n_packets=emit_n)
+        if self.cfg.packets is not None and emit_n > 0:   # this round's table entries
+            cfg.packets = self.cfg.packets[emit_offset:emit_offset + emit_n]
         r = CDDRound()
         r.rank, r.n_ranks = self.rank, self.n_ranks
         r.owner, r.block_local, r.sigma_local = ptr(self.owner), ptr(self.loc), ptr(self.sigma_local)

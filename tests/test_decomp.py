@@ -66,13 +66,13 @@ def test_exchange_delivers_every_record(world):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["amr_point", "hg_multi", "slab"])
+@pytest.mark.parametrize("name", ["amr_point", "hg_multi", "slab", "table"])
 @pytest.mark.parametrize("n_ranks", [2, 3])
 def test_emulated_ranks_equal_replicated_solve(name, n_ranks):
     from kratos_polrad_b200.transport import Tallies, forward
-    from transport_cases import case
+    from transport_cases import case, to_device
     mesh, sig, t = case(name)
-    t = dataclasses.replace(t, n_record=0)
+    t = to_device(dataclasses.replace(t, n_record=0))
     mesh.set_sigma(sig)
     ref = forward(mesh, t, Tallies(t))
     torch.cuda.synchronize()
