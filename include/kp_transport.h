@@ -367,14 +367,14 @@ typedef struct kp_tallies
 /* Asynchronous on `stream`.  Calls that share a mesh handle must not
  * overlap on the GPU (they share the mesh's packet counter and peel-off
  * queue).  With an image, the first solve of a mesh allocates its peel-off
- * queue: 80 B per ray, 12 rays per packet, at most kp_mesh_peel_queue_limit
- * rays (default 2^27, 10.7 GB); later solves reuse it, and the mesh frees it
+ * queue: 64 B per ray, 12 rays per packet, at most kp_mesh_peel_queue_limit
+ * rays (default 2^27, 8.6 GB); later solves reuse it, and the mesh frees it
  * with the mesh. */
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
-/* Upper bound on the mesh's peel-off queue (device memory, 80 B per ray;
- * default 2^27 rays = 10.7 GB).  With an image, kp_transport_forward queues
+/* Upper bound on the mesh's peel-off queue (device memory, 64 B per ray;
+ * default 2^27 rays = 8.6 GB).  With an image, kp_transport_forward queues
  * the peel-off rays of its packets and marches them in a second kernel; the
  * queue holds 12 rays per packet, so solves of more than limit/12 packets
  * run in chunks of that many packets, and a chunk that queues more rays
@@ -460,7 +460,7 @@ int kp_batch_autotune( kp_batch_t * batch, const kp_transport_cfg_t * cfg, doubl
  * do not fit the queue (kp_mesh_peel_queue_limit) are replayed with their
  * rays inline, with the same results.  counters (optional) receives the
  * KP_CNT_* counts of both replays.  Besides the queue, the mesh keeps the
- * adjoint's buffers from the first call on: 8 B per queued ray, 20 B per
+ * adjoint's buffers from the first call on: 20 B per queued ray, 20 B per
  * packet of a chunk, and 8 private int64 path-length tallies (64 B per
  * cell). */
 int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,

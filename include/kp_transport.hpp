@@ -216,7 +216,7 @@ public:
     {
         api( kp_mesh_set_sigma( m_, src, n_values, on_device ? 1 : 0, s ) );
     }
-    // Upper bound on the peel-off queue in rays (80 B each); larger solves
+    // Upper bound on the peel-off queue in rays (64 B each); larger solves
     // run in chunks of limit / 12 packets.
     void peel_queue_limit( long long max_rays ) { api( kp_mesh_peel_queue_limit( m_, max_rays ) ); }
     // Device error bits of the last kernels (0: none); throws if any is set

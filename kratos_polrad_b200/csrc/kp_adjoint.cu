@@ -441,13 +441,9 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
             P.adj_list[ atomicAdd( P.adj_list_n, 1ull ) ] = lp;
             return;
         }
-        peel_task_t & o = P.pq[ k ];
-        #pragma unroll
-        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
-        o.b = p.b;
-        o.w = w; o.I = I; o.Q = Q; o.U = U; o.V = V;
-        o.pix = pix; o.cpix = 0; o.lp = lp; o.kv = kv; o.next = -1;
-        if( link >= 0 ) P.pq[ link ].next = ( int ) k;
+        store_task( P.pq, k, p.x, p.b, p.c, w, I, Q, U, V, pix, 0 );
+        P.pq_link[ k ] = peel_link_t { lp, kv, -1 };
+        if( link >= 0 ) P.pq_link[ link ].next = ( int ) k;
         else P.adj_head[ lp ] = ( int ) k;
         link = ( int ) k;
     };
@@ -543,7 +539,7 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
                     if constexpr( PASS == 0 )
                         queue_ray( pix, p.w, peel_I, 0.0f, 0.0f, 0.0f, 0 );
                     else if( link >= 0 )
-                        link = P.pq[ link ].next;     // its ray is deposited by k_peel
+                        link = P.pq_link[ link ].next;     // its ray is deposited by k_peel
                 }
             }
             faces_all( P.m, p.b, p.c, p.d, fx );
@@ -583,7 +579,7 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
                     else if( link >= 0 )
                     {   // this vertex's score leaves R once its ray is deposited
                         const float G = P.adj_G[ link ];
-                        link = P.pq[ link ].next;
+                        link = P.pq_link[ link ].next;
                         if( G != 0.0f )
                             R = __dsub_rn( R, ( double ) G );
                     }
@@ -684,7 +680,7 @@ __global__ void k_adj_fold( const __grid_constant__ fwd_params_t P )
         double R = 0.0;
         for( int t = P.adj_head[ lp ]; t >= 0; )
         {
-            const peel_task_t & o = P.pq[ t ];
+            const peel_link_t o = P.pq_link[ t ];
             if( o.kv > 0 )
                 R = __dadd_rn( R, ( double ) P.adj_G[ t ] );
             const int nx = o.next;
@@ -703,8 +699,8 @@ __global__ void k_adj_score( const __grid_constant__ fwd_params_t P )
     for( long long t = blockIdx.x * ( long long ) blockDim.x + threadIdx.x; t < n;
          t += ( long long ) gridDim.x * blockDim.x )
     {
-        const peel_task_t & o = P.pq[ t ];
-        if( P.adj_flag[ o.lp ] ) continue;
+        if( P.adj_flag[ P.pq_link[ t ].lp ] ) continue;
+        const task_dep_t o = load_task_deposit( P.pq, t );
         const float att = P.adj_att[ t ];
         float G = 0.0f;
         if( att >= 0.0f )
@@ -754,7 +750,8 @@ void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk )
     // 256 B of counters, the per-packet and per-task arrays, then the private
     // tallies (256-byte aligned)
     const size_t adj_bytes = ( 256 + ( size_t ) n_pk * ( sizeof( double ) + 3 * sizeof( int ) )
-                               + ( size_t ) cap * 2 * sizeof( float ) + 255 ) & ~( size_t ) 255;
+                               + ( size_t ) cap * ( 2 * sizeof( float ) + sizeof( peel_link_t ) )
+                               + 255 ) & ~( size_t ) 255;
     if( mesh->adj_bytes < adj_bytes + priv_bytes )
     {
         cudaFree( mesh->d_adj );
@@ -776,6 +773,7 @@ void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk )
     P.adj_head = reinterpret_cast< int * >( P.adj_att + cap );
     P.adj_flag = P.adj_head + n_pk;
     P.adj_list = P.adj_flag + n_pk;
+    P.pq_link  = reinterpret_cast< peel_link_t * >( P.adj_list + n_pk );
     P.adj_priv = n_priv > 1 ? static_cast< char * >( mesh->d_adj ) + adj_bytes : nullptr;
     P.adj_npriv = n_priv > 1 ? n_priv : 0;
     P.pq = static_cast< peel_task_t * >( mesh->d_pq );

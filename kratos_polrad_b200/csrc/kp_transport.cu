@@ -116,15 +116,12 @@ k_forward( const __grid_constant__ fwd_params_t P )
             return false;
         }
         const int t = threadIdx.x;
-        peel_task_t & o = P.pq[ k ];
-        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
-        o.b = p.b;
-        o.w = sp.w[ t ]; o.I = sp.I[ t ]; o.Q = sp.Q[ t ]; o.U = sp.U[ t ]; o.V = sp.V[ t ];
-        o.pix = sp.pix[ t ]; o.cpix = sd.cpix[ t ];
+        store_task( P.pq, k, p.x, p.b, p.c, sp.w[ t ], sp.I[ t ], sp.Q[ t ], sp.U[ t ], sp.V[ t ],
+                    sp.pix[ t ], sd.cpix[ t ] );
         if constexpr( TAPE )
         {
-            o.lp = lp; o.kv = kv; o.next = -1;
-            if( tlink >= 0 ) P.pq[ tlink ].next = ( int ) k;
+            P.pq_link[ k ] = peel_link_t { lp, kv, -1 };
+            if( tlink >= 0 ) P.pq_link[ tlink ].next = ( int ) k;
             else P.adj_head[ lp ] = ( int ) k;
             tlink = ( int ) k;
         }
@@ -730,7 +727,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 float att = -1.0f;                    // MODE 3: -1 marks a ray beyond the cut
                 if( dep )
                 {   // deposit of the ray that just ended (after_crossing's)
-                    const peel_task_t & o = P.pq[ task ];
+                    const task_dep_t o = load_task_deposit( P.pq, task );
                     att = __fmul_rn( o.w, ( float ) phys::kp_exp_neg( -( double ) ptau ) );
                     deposit_pixel< TALLY >( P, o.pix, o.cpix, __fmul_rn( att, o.I ),
                                             __fmul_rn( att, o.Q ), __fmul_rn( att, o.U ),
@@ -749,7 +746,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
             if constexpr( MODE == 1 )
                 if( task >= 0 )
                 {   // score of the ray that just ended (k_adjoint's measure ray)
-                    const peel_task_t & o = P.pq[ task ];
+                    const task_dep_t o = load_task_deposit( P.pq, task );
                     float G = 0.0f;
                     if( ptau <= P.tau_cut )
                     {
@@ -773,22 +770,19 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 phase = PH_DONE;
                 continue;
             }
-            const peel_task_t & o = P.pq[ idx ];
             if constexpr( MODE == 1 || MODE == 2 )
             {   // rays of packets left to k_adjoint, and rays worth nothing
-                if( P.adj_flag[ o.lp ] )
+                if( P.adj_flag[ P.pq_link[ idx ].lp ] )
                     continue;
                 if constexpr( MODE == 2 )
                 {
                     pG = P.adj_G[ idx ];
-                    n_dep = o.cpix;
+                    n_dep = P.pq[ idx ].cpix;
                     if( pG == 0.0f || n_dep <= 0 )
                         continue;
                 }
             }
-            #pragma unroll
-            for( int a = 0; a < 3; ++ a ) { x[ a ] = o.x[ a ]; c[ a ] = o.c[ a ]; }
-            b = o.b;
+            load_task_ray( P.pq, ( long long ) idx, x, b, c );
             task = ( long long ) idx;
             ptau = 0.0f; pk = 0;
             enter(  );
@@ -1065,13 +1059,16 @@ thread_local cudaEvent_t split_event = nullptr;
 // and queues their peel-off rays (marching them inline only if the queue is
 // full), then k_peel marches the queue.  The queue belongs to the mesh and
 // holds 12 rays per packet, at most the mesh's limit (default 2^27 rays,
-// 10.7 GB); larger solves run in chunks of packets (cap / 12 packets each,
+// 8.6 GB); larger solves run in chunks of packets (cap / 12 packets each,
 // walk then march), so the queue is sized for the chunk, not the solve.
 
 // Grows the mesh's peel-off queue to 12 rays per packet of a solve of
 // n_packets (at least 2^16 rays, at most the mesh's limit).
 void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets )
 {
+    const auto v = mesh->view(  );
+    require( v.nc[ 0 ] <= PQ_MAX_CELLS && v.nc[ 1 ] <= PQ_MAX_CELLS && v.nc[ 2 ] <= PQ_MAX_CELLS,
+             "peel-off queue: blocks of at most 1024 cells a side", KP_ERR_CAPACITY );
     const long long want = std::min( std::max< long long >( PQ_PER_PACKET * n_packets, 1 << 16 ),
                                      mesh->pq_limit );
     if( mesh->pq_cap < want )

@@ -109,6 +109,7 @@ struct fwd_params_t
     unsigned long long * dd_out_count;  // [2]: walks, peel-off rays
     // peel-off rays deferred to k_peel (plain forward solves)
     struct peel_task_t * pq;            // [pq_cap] tasks
+    struct peel_link_t * pq_link;       // [pq_cap] per-packet links (tape, adjoint)
     unsigned long long * pq_count;      // tasks written (may exceed pq_cap: those ran inline)
     unsigned long long * pq_next;       // k_peel's task counter
     long long   pq_cap;
@@ -128,19 +129,78 @@ struct fwd_params_t
 };
 
 // A peel-off ray waiting for k_peel: where it starts (the interaction or
-// emission point) and its pending contribution.  When the rays are linked
-// per packet (the deferred adjoint, a taped forward solve), `next` holds the
-// packet's next task (-1: last), `lp` the packet's index in the launch and
-// `kv` the vertex (0: emission).
+// emission point, its block and cell) and its pending contribution.  64
+// bytes, two whole 32-byte sectors, written and read as 16-byte vectors
+// (store_task, load_task_ray, load_task_deposit); the cell indices are
+// packed 10 bits each (blocks of at most 1024 cells a side).
 struct __align__( 16 ) peel_task_t
 {
-    double x[ 3 ];
-    int    b, c[ 3 ];
-    float  w, I, Q, U, V;
-    int    pix, cpix;
-    int    lp, kv;
-    int    next;
+    double   x[ 3 ];
+    int      b;
+    unsigned c;                    // c0 | c1 << 10 | c2 << 20
+    float    w, I, Q, U, V;
+    int      pix, cpix;
+    int      pad;
 };
+static_assert( sizeof( peel_task_t ) == 64, "peel-off task: two sectors" );
+constexpr int PQ_MAX_CELLS = 1024;   // cells per block side a task can hold
+
+// When the rays are linked per packet (the deferred adjoint, a taped forward
+// solve), the task's entry of this array, parallel to the queue, holds the
+// packet's index in the launch (lp), the vertex (kv, 0: emission) and the
+// packet's next task (next, -1: last).
+struct peel_link_t
+{
+    int lp, kv, next;
+};
+
+__device__ __forceinline__ void store_task( peel_task_t * q, unsigned long long k,
+                                            const double x[ 3 ], int b, const int c[ 3 ],
+                                            float w, float I, float Q, float U, float V,
+                                            int pix, int cpix )
+{
+    char * t = reinterpret_cast< char * >( q + k );
+    const long long x2 = __double_as_longlong( x[ 2 ] );
+    const unsigned cp = ( unsigned ) c[ 0 ] | ( ( unsigned ) c[ 1 ] << 10 )
+                      | ( ( unsigned ) c[ 2 ] << 20 );
+    * reinterpret_cast< double2 * >( t )     = make_double2( x[ 0 ], x[ 1 ] );
+    * reinterpret_cast< int4 * >( t + 16 )   = make_int4( ( int ) x2, ( int ) ( x2 >> 32 ), b,
+                                                          ( int ) cp );
+    * reinterpret_cast< float4 * >( t + 32 ) = make_float4( w, I, Q, U );
+    * reinterpret_cast< int4 * >( t + 48 )   = make_int4( __float_as_int( V ), pix, cpix, 0 );
+}
+
+// The ray's start: position, block, cell.
+__device__ __forceinline__ void load_task_ray( const peel_task_t * q, long long k, double x[ 3 ],
+                                               int & b, int c[ 3 ] )
+{
+    const char * t = reinterpret_cast< const char * >( q + k );
+    const double2 a = * reinterpret_cast< const double2 * >( t );
+    const int4    v = * reinterpret_cast< const int4 * >( t + 16 );
+    x[ 0 ] = a.x;
+    x[ 1 ] = a.y;
+    x[ 2 ] = __hiloint2double( v.y, v.x );
+    b = v.z;
+    const unsigned cp = ( unsigned ) v.w;
+    c[ 0 ] = ( int ) ( cp & 1023u );
+    c[ 1 ] = ( int ) ( ( cp >> 10 ) & 1023u );
+    c[ 2 ] = ( int ) ( cp >> 20 );
+}
+
+// The ray's pending contribution: weight, Stokes vector toward the observer,
+// its pixel and coarse per-batch pixel.
+struct task_dep_t
+{
+    float w, I, Q, U, V;
+    int   pix, cpix;
+};
+__device__ __forceinline__ task_dep_t load_task_deposit( const peel_task_t * q, long long k )
+{
+    const char * t = reinterpret_cast< const char * >( q + k );
+    const float4 f = * reinterpret_cast< const float4 * >( t + 32 );
+    const int4   g = * reinterpret_cast< const int4 * >( t + 48 );
+    return task_dep_t { f.x, f.y, f.z, f.w, __int_as_float( g.x ), g.y, g.z };
+}
 
 // A packet's walk crossing into a block of another rank (it has entered the
 // block: position snapped to the face, cell and block set).  The inverse

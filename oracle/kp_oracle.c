@@ -491,7 +491,7 @@ static int temit( const tctx * t, const kpo_cfg_t * c, long long pid, tpk * p, f
         return 1;
     }
     const kpo_source_t * s = c->sources + pid % c->n_sources;
-    * peel_I = s->kind == 0 && s->emit == 0 ? 0x1.45f306p-4f : 0.0f;
+    * peel_I = s->kind == 0 && s->emit == 0 ? OM_INV4PI : 0.0f;
     if( s->kind == 0 )
     {
         for( int a = 0; a < 3; ++ a ) { p->x[ a ] = s->pos[ a ]; p->c[ a ] = s->cell[ a ]; }

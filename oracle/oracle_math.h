@@ -18,6 +18,15 @@
 #include <stdint.h>
 #include <string.h>
 
+/* Physical constants in the arithmetic type of the build (float here; the
+ * FP64 build of the restatement, kp_oracle64.c, gives double values). */
+#ifndef OM_INV4PI
+#define OM_INV4PI 0x1.45f306p-4f          /* 1 / (4 pi)  */
+#endif
+#ifndef OM_3_16PI
+#define OM_3_16PI 0x1.e8ec8ap-5f          /* 3 / (16 pi) */
+#endif
+
 typedef struct { uint32_t x, y, z, w; } om_u4;
 
 static inline uint32_t om_mulhi( uint32_t a, uint32_t b )
@@ -140,7 +149,7 @@ static inline om_smat om_scatter_matrix( om_phase ph, float mu )
     s.r33 = ( 2.0f * mu ) / a;
     if( ph.kind == 0 )
     {
-        s.f11 = a * 0x1.e8ec8ap-5f;               /* 3 / (16 pi) */
+        s.f11 = a * OM_3_16PI;
         s.r12 = ( mu2 - 1.0f ) / a;
     }
     else
@@ -148,7 +157,7 @@ static inline om_smat om_scatter_matrix( om_phase ph, float mu )
         const float g2 = ph.g * ph.g;
         const float den = ( 1.0f + g2 ) - ( 2.0f * ph.g ) * mu;
         const float sd = sqrtf( den );
-        s.f11 = ( ( 1.0f - g2 ) * 0x1.45f306p-4f ) / ( den * sd );   /* 1 / (4 pi) */
+        s.f11 = ( ( 1.0f - g2 ) * OM_INV4PI ) / ( den * sd );
         s.r12 = -ph.pmax * ( ( 1.0f - mu2 ) / a );
     }
     return s;

@@ -12,6 +12,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(_HERE, "_ref", "libkporacle.so")
+LIB64 = os.path.join(_HERE, "_ref", "libkporacle64.so")   # every float in double
 
 
 class _Mesh(ctypes.Structure):
@@ -24,6 +25,7 @@ class _Mesh(ctypes.Structure):
 
 
 _lib = None
+_lib64 = None
 
 
 def lib():
@@ -33,6 +35,16 @@ def lib():
             raise FileNotFoundError(f"{LIB} missing: run `make -C oracle`")
         _lib = ctypes.CDLL(LIB)
     return _lib
+
+
+def lib64():
+    """The FP64 build of the restatement (exports with a _f64 suffix)."""
+    global _lib64
+    if _lib64 is None:
+        if not os.path.exists(LIB64):
+            raise FileNotFoundError(f"{LIB64} missing: run `make -C oracle`")
+        _lib64 = ctypes.CDLL(LIB64)
+    return _lib64
 
 
 def available() -> bool:
@@ -219,10 +231,11 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, flux=Fal
 
 
 def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, grad_shift=24,
-            abs_sum=False):
+            abs_sum=False, fp64=False):
     """Restated path-replay adjoint; returns int64 (g_len, g_int), counters,
     and with ``abs_sum`` also the per-cell sum of |deposit| over both
-    tallies and the per-cell deposit count ([n_cells, 2] float64)."""
+    tallies and the per-cell deposit count ([n_cells, 2] float64).  With
+    ``fp64`` the FP64 build runs it (every float quantity in double)."""
     src = (_Source * max(1, len(cfg.sources)))()
     for k, s in enumerate(cfg.sources):
         src[k].kind, src[k].emit = int(s.kind), int(s.emit)
@@ -236,22 +249,25 @@ def adjoint(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, adj_img, g
     n_cells = tab.n_blocks * tab.cells_per_block
     g_len, g_int = np.zeros(n_cells, np.int64), np.zeros(n_cells, np.int64)
     cnt = np.zeros(10, np.uint64)
-    sigma2 = np.ascontiguousarray(sigma2, np.float32)
+    ftype = np.float64 if fp64 else np.float32
+    sigma2 = np.ascontiguousarray(sigma2, np.float32).astype(ftype)
     lookup = np.ascontiguousarray(lookup, np.int32)
     lk_n = np.ascontiguousarray(lookup_n, np.int32)
-    adj = np.ascontiguousarray(adj_img, np.float32)
+    adj = np.ascontiguousarray(adj_img, np.float32).astype(ftype)
     s = tab._struct()
-    L = lib()
-    L.kpo_adjoint.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int] + [ctypes.c_void_p] * 3
+    L = lib64() if fp64 else lib()
+    sfx = "_f64" if fp64 else ""
+    f_adj, f_sink = getattr(L, "kpo_adjoint" + sfx), getattr(L, "kpo_set_abs_sink" + sfx)
+    f_adj.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int] + [ctypes.c_void_p] * 3
     p = lambda a: ctypes.c_void_p(a.ctypes.data)
     sink = np.zeros((n_cells, 2), np.float64) if abs_sum else None
-    L.kpo_set_abs_sink.argtypes = [ctypes.c_void_p]
-    L.kpo_set_abs_sink(p(sink) if abs_sum else None)
+    f_sink.argtypes = [ctypes.c_void_p]
+    f_sink(p(sink) if abs_sum else None)
     try:
-        st = L.kpo_adjoint(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
-                           p(adj), grad_shift, p(g_len), p(g_int), p(cnt))
+        st = f_adj(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
+                   p(adj), grad_shift, p(g_len), p(g_int), p(cnt))
     finally:
-        L.kpo_set_abs_sink(None)
+        f_sink(None)
     if st != 0:
         raise RuntimeError(f"kpo_adjoint failed ({st})")
     return (g_len, g_int, cnt, sink) if abs_sum else (g_len, g_int, cnt)

@@ -63,10 +63,17 @@ def test_float_tally_mode_close_to_fixed():
     torch.cuda.synchronize()
     img_fx = fx.image.cpu().numpy() * 2.0 ** -t.fx_shift
     img_fl = fl.image.cpu().numpy().astype(np.float64)
-    # float atomics: reordering error <= n_terms * eps * sum|terms| per pixel;
-    # with int64 rounding 2^-32 per term the two agree to 1e-5 of the peak.
-    np.testing.assert_allclose(img_fl, img_fx, rtol=0, atol=1e-5 * np.abs(img_fx).max())
-    np.testing.assert_allclose(img_fl[..., 0].sum(), img_fx[..., 0].sum(), rtol=1e-6)
+    # Float atomics sum the same deposits in another order.  Pixel sums above
+    # a noise floor of 1e-3 of the image's peak agree within 1e-6 relative;
+    # below it a few deposits of either sign may cancel, and the bar is
+    # 1e-9 of the peak there (the int64 rounding is 2^-32 per deposit).
+    peak = np.abs(img_fx).max()
+    big = np.abs(img_fx) > 1e-3 * peak
+    assert big.sum() > 1000
+    rel = np.abs(img_fl - img_fx)[big] / np.abs(img_fx)[big]
+    assert rel.max() <= 1e-6, (rel.max(), np.percentile(rel, 99))
+    np.testing.assert_allclose(img_fl[~big], img_fx[~big], rtol=1e-6, atol=1e-9 * peak)
+    np.testing.assert_allclose(img_fl[..., 0].sum(), img_fx[..., 0].sum(), rtol=1e-7)
 
 
 @pytest.mark.parametrize("name", ["amr_point", "hg_multi", "table"])

@@ -128,6 +128,6 @@ def oracle_inputs(mesh, t):
     return tab, grid, n, cells
 
 
-def run_oracle_adjoint(mesh, sig, t, adj_img, grad_shift=24, abs_sum=False):
+def run_oracle_adjoint(mesh, sig, t, adj_img, grad_shift=24, abs_sum=False, fp64=False):
     tab, grid, n, cells = oracle_inputs(mesh, t)
-    return port.adjoint(tab, sig, grid, n, t, cells, adj_img, grad_shift, abs_sum)
+    return port.adjoint(tab, sig, grid, n, t, cells, adj_img, grad_shift, abs_sum, fp64)
