@@ -214,5 +214,6 @@ def load_solution(path: str) -> dict:
             out[name] = a.reshape(shp).copy()
         if "kp|config" in f:
             out["config"] = json.loads(f["kp|config"].decode())
+        if "kp|packets_done" in f:
             out["packets_done"] = int(f.read("kp|packets_done", np.int64)[0])
     return out
