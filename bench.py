@@ -372,77 +372,108 @@ def _timed(fn):
     return out, e0.elapsed_time(e1)
 
 
-def _gradient_check(mesh, sig, cfg, g_img, grad, rng, n_check=20_000_000, n_batch=10,
-                    n_dirs=8, n_cells=32):
+def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=200_000_000, n_batch=20, n_dirs=8,
+                    n_cells=16, n_cell_check=50_000_000):
     """Paired batch-means comparison of the path-replay gradient with
     common-random-number central differences of the same estimator.
 
     The functional is F = sum over packets of <a, image contribution> with
     a = g_img / max|g_img| (the loss linearised at the forward solution).
     Packets [0, n_check) are cut into n_batch ranges; on each range the
-    adjoint and the differences use the same packets, so their difference per
-    range has a small spread and z = mean / (std / sqrt(n_batch)) tests
-    agreement.  Directions: 8 Gaussian density blobs (radius 0.08 box, both
-    coefficients scaled by 1 +- 0.05 phi: albedo unchanged) and 32 single
-    cells drawn among the 2000 of largest |dL/dsigma_sca| (sigma_sca +- 10%)."""
+    adjoint and the differences use the same packets.
+
+    Blob directions (the 2% bar): Gaussian density blobs of radius 0.08 box
+    (both coefficients scaled by 1 +- 0.05 phi, albedo unchanged) centred on
+    the cells of largest |dF/dsigma_sca|, chosen from a gradient of other
+    packets (ids from 5e9) so that the choice does not favour the checked
+    estimate.  For each: the difference's mean, its batch-means standard
+    error, and the adjoint's relative difference from it; a direction passes
+    when that is within 2% and the standard error is within 1%.
+    Single cells (a z-score check, too noisy for a 2% bar): n_cells cells
+    among the 2000 of largest |dF/dsigma_sca| (sigma_sca +- 10%), on the
+    first n_cell_check packets."""
     import numpy as np
     import torch
     from kratos_polrad_b200 import scenes
     from kratos_polrad_b200.adjoint import gradients
     from kratos_polrad_b200.transport import Tallies, forward
-    nb = n_check // n_batch
     a = (g_img / g_img.abs().max()).float().contiguous()
     a64 = a.double()
-    cb = [dataclasses.replace(cfg, n_packets=nb, packet_offset=b * nb, n_record=0)
-          for b in range(n_batch)]
+    mesh.set_sigma(sig)
+    sel = dataclasses.replace(cfg, n_packets=20_000_000, packet_offset=5_000_000_000, n_record=0)
+    g_sel = gradients(mesh, sel, a, 24)[0].cpu().numpy()
     xc = scenes.cell_centers(mesh)
-    phis = [np.exp(-((xc - rng.uniform(0.2, 0.8, 3)) ** 2).sum(1) / (2 * 0.08 ** 2))
-            for _ in range(n_dirs)]
-    cells = rng.choice(np.argsort(-np.abs(grad))[:2000], n_cells, replace=False)
+    order = np.argsort(-np.abs(g_sel))
+    centres = []
+    for k in order:                       # blob centres at least 0.15 box apart
+        if all(np.linalg.norm(xc[k] - c) > 0.15 for c in centres):
+            centres.append(xc[k])
+        if len(centres) == n_dirs:
+            break
+    phis = [np.exp(-((xc - c) ** 2).sum(1) / (2 * 0.08 ** 2)) for c in centres]
+    cells = rng.choice(order[:2000], n_cells, replace=False)
     sig_d = torch.tensor(sig, device="cuda", dtype=torch.float64)
     phi_d = torch.tensor(np.stack(phis, 1), device="cuda", dtype=torch.float64)
     cells_d = torch.tensor(cells, device="cuda")
-    adj = np.zeros((n_batch, n_dirs + n_cells))
-    mesh.set_sigma(sig)
-    for b, c in enumerate(cb):
-        gs, ga = gradients(mesh, c, a, 24)
-        adj[b, :n_dirs] = ((gs * sig_d[:, 0])[:, None] * phi_d
-                           + (ga * sig_d[:, 1])[:, None] * phi_d).sum(0).cpu().numpy()
-        adj[b, n_dirs:] = gs[cells_d].cpu().numpy()
 
-    def scores(s2):
+    def ranges(n_total):
+        nb = n_total // n_batch
+        return [dataclasses.replace(cfg, n_packets=nb, packet_offset=b * nb, n_record=0)
+                for b in range(n_batch)]
+
+    cb, cc = ranges(n_check), ranges(n_cell_check)
+    adj_b = np.zeros((n_batch, n_dirs))
+    adj_c = np.zeros((n_batch, n_cells))
+    for b in range(n_batch):
+        gs, ga = gradients(mesh, cb[b], a, 24)
+        adj_b[b] = ((gs * sig_d[:, 0])[:, None] * phi_d
+                    + (ga * sig_d[:, 1])[:, None] * phi_d).sum(0).cpu().numpy()
+        adj_c[b] = gradients(mesh, cc[b], a, 24)[0][cells_d].cpu().numpy()
+
+    def scores(s2, ranges_):
         mesh.set_sigma(s2)
         out = []
-        for c in cb:
+        for c in ranges_:
             tal = forward(mesh, c, Tallies(c))
             out.append(float((tal.image.double() * a64).sum()) * tal.scale())
         return np.array(out)
 
-    fd = np.zeros_like(adj)
+    fd_b = np.zeros_like(adj_b)
+    fd_c = np.zeros_like(adj_c)
+    h = 0.05
     for k, phi in enumerate(phis):
-        h = 0.05
         sp = (sig * (1 + h * phi)[:, None]).astype(np.float32)
         sm = (sig * (1 - h * phi)[:, None]).astype(np.float32)
-        fd[:, k] = (scores(sp) - scores(sm)) / (2 * h)
+        fd_b[:, k] = (scores(sp, cb) - scores(sm, cb)) / (2 * h)
     for j, cell in enumerate(cells):
         sp, sm = sig.copy(), sig.copy()
         sp[cell, 0] *= 1.1
         sm[cell, 0] *= 0.9
-        fd[:, n_dirs + j] = (scores(sp) - scores(sm)) / (float(sp[cell, 0]) - float(sm[cell, 0]))
+        fd_c[:, j] = (scores(sp, cc) - scores(sm, cc)) / (float(sp[cell, 0]) - float(sm[cell, 0]))
     mesh.set_sigma(sig)
-    d = adj - fd
-    z = d.mean(0) / (d.std(0, ddof=1) / np.sqrt(n_batch))
-    rel = np.abs(d.mean(0)) / np.abs(fd.mean(0))
-    zd, zc, rd, rc = z[:n_dirs], z[n_dirs:], rel[:n_dirs], rel[n_dirs:]
+    sq = np.sqrt(n_batch)
+    fd_mean, fd_se = fd_b.mean(0), fd_b.std(0, ddof=1) / sq
+    adj_mean = adj_b.mean(0)
+    rel = np.abs(adj_mean - fd_mean) / np.abs(fd_mean)
+    rel_se = fd_se / np.abs(fd_mean)
+    d = adj_b - fd_b
+    zb = d.mean(0) / (d.std(0, ddof=1) / sq)
+    dc = adj_c - fd_c
+    zc = dc.mean(0) / (dc.std(0, ddof=1) / sq)
+    ok = (rel <= 0.02) & (rel_se <= 0.01)
     return {"packets": n_check, "batches": n_batch,
-            "blob_directions": {"n": n_dirs, "rel_diff": [round(float(v), 5) for v in rd],
-                                "z": [round(float(v), 2) for v in zd],
-                                "max_abs_z": float(np.abs(zd).max())},
-            "cells": {"n": n_cells, "median_rel_diff": float(np.median(rc)),
+            "blob_directions": {"n": n_dirs, "fd": [float(v) for v in fd_mean],
+                                "fd_rel_std_err": [round(float(v), 5) for v in rel_se],
+                                "adjoint": [float(v) for v in adj_mean],
+                                "rel_diff": [round(float(v), 5) for v in rel],
+                                "max_rel_diff": float(rel.max()),
+                                "within_2pct_with_se_below_1pct": int(ok.sum()),
+                                "paired_z": [round(float(v), 2) for v in zb]},
+            "cells": {"n": n_cells, "packets": n_cell_check,
                       "frac_abs_z_below_3": float(np.mean(np.abs(zc) < 3)),
                       "mean_z2": float(np.mean(zc ** 2)), "max_abs_z": float(np.abs(zc).max())},
-            "note": "adjoint vs CRN central differences on the same packets; "
-                    "z from 10 paired packet ranges"}
+            "note": "adjoint vs common-random-number central differences on the same packets "
+                    "(paired batch means); blob centres chosen from other packets"}
 
 
 def run_diff(args):
@@ -481,7 +512,7 @@ def run_diff(args):
     g = x.grad[:, 0].detach().cpu().numpy()
     g_img = torch.zeros_like(img)
     g_img[..., 1:3] = 2 * (img.detach() - target)[..., 1:3]
-    check = None if args.no_cpu_baseline else _gradient_check(mesh, sig, cfg, g_img, g, rng)
+    check = None if args.no_cpu_baseline else _gradient_check(mesh, sig, cfg, g_img, rng)
     line = {"metric": "path-replay gradient, 96^3 lognormal, Q/U image loss", "unit": "ms",
             "value": t_bwd, "higher_is_better": False, "n_gpus": 1,
             "config": {"workload": "lognormal_96_diff", "packets": n_pk, "cells": mesh.n_cells},
@@ -773,6 +804,7 @@ def run_large(args):
     rho 1.5, seed 5; ~2e7 cells, 166 MB of coefficients: beyond L2), HG g=0.6
     with polarization, 64 random point sources, 256^2 IQUV image; one forward
     solve and one path-replay gradient of `--packets` packets (default 1e9)."""
+    import numpy as np
     import torch
     from kratos_polrad_b200 import scenes
     from kratos_polrad_b200.adjoint import adjoint
@@ -787,7 +819,18 @@ def run_large(args):
     with ClockSampler(0) as clk:
         _, t_fwd = _timed(lambda: forward(mesh, cfg, tal))
     c = tal.counts()
-    p_tan, rel = scenes.batch_rel_error(tal.image_batch.cpu().numpy() * tal.scale())
+    bimg = tal.image_batch.cpu().numpy() * tal.scale()
+    p_tan, rel = scenes.batch_rel_error(bimg)
+    # the image-integrated linear polarization fraction sqrt(Q^2+U^2)/I, and
+    # the intensity-weighted mean degree of the coarse pixels, with their
+    # batch-means relative std-errors
+    from kratos_polrad_b200.transport import batch_std_error
+    p_int, rel_int = batch_std_error(bimg.sum((1, 2)))
+    deg = np.array([np.sqrt(b[..., 1] ** 2 + b[..., 2] ** 2).sum() / b[..., 0].sum()
+                    for b in bimg])
+    p_deg = float(np.sqrt(bimg.sum(0)[..., 1] ** 2 + bimg.sum(0)[..., 2] ** 2).sum()
+                  / bimg.sum(0)[..., 0].sum())
+    rel_deg = float(deg.std(ddof=1) / np.sqrt(len(deg)) / p_deg)
     g_img = torch.randn((cfg.image_n, cfg.image_n, 4), device="cuda",
                         generator=torch.Generator(device="cuda").manual_seed(5))
     acnt = torch.zeros(10, dtype=torch.int64, device="cuda")
@@ -799,6 +842,8 @@ def run_large(args):
                                     "blocks": mesh.n_blocks, "cells": mesh.n_cells,
                                     "sigma_MB": sig.nbytes / 1e6, "image": cfg.image_n},
             "forward_ms": t_fwd, "counts": c, "pol_tangential": p_tan, "pol_rel_std_err": rel,
+            "pol_integrated": p_int, "pol_integrated_rel_std_err": rel_int,
+            "pol_mean_degree_coarse": p_deg, "pol_mean_degree_rel_std_err": rel_deg,
             "adjoint_ms": t_adj, "adjoint_cost_vs_forward": t_adj / t_fwd,
             "adjoint_packet_steps_per_s": float(ac[0] + ac[1]) / (t_adj / 1e3),
             "clocks": clk.summary()}
