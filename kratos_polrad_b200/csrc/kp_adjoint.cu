@@ -57,7 +57,8 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
     double fx[ 3 ];                               // face cache of the active ray
     int   phase = PH_EMIT, ray = RAY_WALK, pass = 0;
     float ptau = 0.f, pG = 0.f, G0 = 0.f;
-    int   pk = 0, pend = 0, nv = 0;
+    double ptc = 0.0;             // a peel-off ray: distance travelled from its start
+    int   pk = 0, pend = 0, nv = 0;   // (p.x), fx its face distances (oray_faces)
     bool  remeasure = false;
     double R = 0.0;
     float gk[ ADJ_KMAX ];
@@ -83,10 +84,12 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         {
             park_walk( sp, p );
             park_dir( sd, p, P.o, P.inv_o );
-            pG = G0; ptau = 0.f; pk = 0; pend = 0;
+            pG = G0; ptau = 0.f; pk = 0; pend = 0; ptc = 0.0;
             ray = RAY_DEPOSIT;
+            oray_faces( P, p.b, p.c, p.x, fx );
         }
-        faces_all( P.m, p.b, p.c, p.d, fx );
+        else
+            faces_all( P.m, p.b, p.c, p.d, fx );
     };
     // The lane's packet has ended (in the current pass).
     auto end_packet = [ & ](  )
@@ -126,9 +129,9 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                     unpark_walk( sp, p );
                     if( G != 0.0f )
                     {
-                        pG = G; ptau = 0.f; pk = 0;
+                        pG = G; ptau = 0.f; pk = 0; ptc = 0.0;
                         ray = RAY_DEPOSIT;          // the walk position stays parked
-                        faces_all( P.m, p.b, p.c, p.d, fx );   // p.d is still o
+                        oray_faces( P, p.b, p.c, p.x, fx );    // p.d is still o
                         return;
                     }
                 }
@@ -189,12 +192,15 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         {   // batched block hand-offs (see k_forward)
             if( phase != PH_HOP ) continue;
             const int b_old = p.b;
-            bool lost;
-            const bool left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax,
-                                            comp( p.d, hop_ax ) > 0.0f, lost );
+            bool lost, left;
+            if( ray != RAY_WALK )   // a peel-off ray: rebased at its crossing point
+                left = ! oray_rebase( P, p.b, p.c, p.x, ptc, fx, hop_ax, lost );
+            else
+                left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax, comp( p.d, hop_ax ) > 0.0f, lost );
             if( ! left )
             {
-                faces_all( P.m, p.b, p.c, p.d, fx );
+                if( ray == RAY_WALK )
+                    faces_all( P.m, p.b, p.c, p.d, fx );
                 if( p.b != b_old && counting(  ) ) count( sp, KP_CNT_HOPS );
             }
             phase = PH_SEGMENT;
@@ -239,13 +245,16 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                     sp.w[ th ] = p.w; sp.I[ th ] = peel_I;
                     sp.Q[ th ] = sp.U[ th ] = sp.V[ th ] = 0.0f;
                     sp.pix[ th ] = pix;
-                    pend = 0; ptau = 0.0f; pk = 0;
+                    pend = 0; ptau = 0.0f; pk = 0; ptc = 0.0;
                     park_walk( sp, p );
                     park_dir( sd, p, P.o, P.inv_o );
                     ray = RAY_MEASURE;
                 }
             }
-            faces_all( P.m, p.b, p.c, p.d, fx );
+            if( ray != RAY_WALK )
+                oray_faces( P, p.b, p.c, p.x, fx );
+            else
+                faces_all( P.m, p.b, p.c, p.d, fx );
             continue;
         }
 
@@ -301,12 +310,12 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
             if( do_peel )
             {
                 pend = end;
-                ptau = 0.f; pk = 0;
+                ptau = 0.f; pk = 0; ptc = 0.0;
                 if( pass == 0 || nv > ADJ_KMAX )
                 {
                     park_walk( sp, p );
                     park_dir( sd, p, P.o, P.inv_o );
-                    faces_all( P.m, p.b, p.c, p.d, fx );
+                    oray_faces( P, p.b, p.c, p.x, fx );
                     ray = RAY_MEASURE;
                     remeasure = pass == 1;
                     continue;
@@ -316,7 +325,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                 {
                     park_walk( sp, p );
                     park_dir( sd, p, P.o, P.inv_o );
-                    faces_all( P.m, p.b, p.c, p.d, fx );
+                    oray_faces( P, p.b, p.c, p.x, fx );
                     ray = RAY_DEPOSIT;
                     continue;
                 }
@@ -335,7 +344,11 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         const float2 sg = P.m.sigma[ ci ];
         const float ext = __fadd_rn( sg.x, sg.y );
         int ax;                                   // p.d / p.inv: the active ray's
-        const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
+        double t;
+        if( peel )
+            t = oray_segment( fx, ptc, ax );
+        else
+            t = exit_cached( p.x, fx, p.d, p.inv, ax );
         const float et = __fmul_rn( ext, ( float ) t );
         bool interact = false, peel_cut = false;
         if( peel )
@@ -367,16 +380,20 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         }
         if( ! peel_cut )
         {
-            if( ! peel )
+            bool in_block;
+            if( peel )
+                in_block = oray_step_in_block( P, p.b, p.c, p.x, fx, ax );
+            else
             {
                 p.tau = __fsub_rn( p.tau, et );
                 if( pass == 1 && R != 0.0 )
                     add_grad< TALLY >( P.g_len, ci, __dmul_rn( -R, t ), P.g_scale );
+                #pragma unroll
+                for( int a = 0; a < 3; ++ a )
+                    if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
+                in_block = step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d );
             }
-            #pragma unroll
-            for( int a = 0; a < 3; ++ a )
-                if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
-            if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
+            if( ! in_block )
             {   // leaves the block: wait for a batched hand-off
                 hop_ax = ax;
                 phase = PH_HOP;

@@ -83,8 +83,9 @@ k_forward( const __grid_constant__ fwd_params_t P )
     packet_t p;
     double fx[ 3 ];                               // face cache of the active ray
     int  phase = PH_EMIT;
-    bool peel = false;
-    float ptau = 0;
+    bool peel = false;            // the lane runs a peel-off ray: p.x holds its start,
+    float ptau = 0;               // fx the distances to its cell's faces (oray_faces)
+    double ptc = 0.0;             // ... and ptc the distance it has travelled
     int pk = 0, pend = 0;
     int si = 0;                                   // scene of a batched launch
     int hop_ax = 0;                               // face axis of a pending hand-off
@@ -126,6 +127,29 @@ k_forward( const __grid_constant__ fwd_params_t P )
             tlink = ( int ) k;
         }
         return true;
+    };
+
+    // A peel-off ray marched by this lane at once from the packet's position
+    // (its contribution is in sp / sd): every ray of the single-kernel walk,
+    // and the rays that find the queue full in the deferred one.  Only the
+    // decomposed rounds schedule their rays segment by segment with the walk
+    // (a ray may cross into another rank's block mid-way).
+    auto peel_now = [ & ](  )
+    {
+        unsigned segs = 0, hops = 0;
+        const float tau = oray_march( P, p.b, p.c, p.x, segs, hops );
+        cnt.peel += segs;
+        if( hops )
+            atomicAdd( sp.cnt + KP_CNT_HOPS, ( unsigned long long ) hops );
+        if( tau <= P.tau_cut )
+        {
+            const int th = threadIdx.x;
+            const float att = __fmul_rn( sp.w[ th ], ( float ) phys::kp_exp_neg( -( double ) tau ) );
+            deposit_pixel< TALLY >( P, sp.pix[ th ], sd.cpix[ th ], __fmul_rn( att, sp.I[ th ] ),
+                                    __fmul_rn( att, sp.Q[ th ] ), __fmul_rn( att, sp.U[ th ] ),
+                                    __fmul_rn( att, sp.V[ th ] ) );
+            count( sp, KP_CNT_DEPOSITS );
+        }
     };
 
     // coefficients of cell c of block b (DD: owned blocks stored compactly)
@@ -267,9 +291,11 @@ k_forward( const __grid_constant__ fwd_params_t P )
             // neighbour lookup and the new block's geometry in one batch
             if( phase != PH_HOP ) continue;
             const int b_old = p.b;
-            bool lost;
-            const bool left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax,
-                                            comp( p.d, hop_ax ) > 0.0f, lost );
+            bool lost, left;
+            if( peel )      // a peel-off ray: rebased at its crossing point
+                left = ! oray_rebase( P, p.b, p.c, p.x, ptc, fx, hop_ax, lost );
+            else
+                left = ! cross_face( P.m, p.b, p.c, p.x, hop_ax, comp( p.d, hop_ax ) > 0.0f, lost );
             if( ! left )
             {
                 if( p.b != b_old ) count( sp, KP_CNT_HOPS );
@@ -290,7 +316,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                                 P.dd_out_peel_rank[ k ] = r;
                                 dd_peel_t & o = P.dd_out_peel[ k ];
                                 for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
-                                o.b = p.b; o.ptau = ptau; o.pk = pk;
+                                o.b = p.b; o.ptau = ptau; o.pk = pk; o.tc = ptc;
                                 o.w = sp.w[ t ]; o.I = sp.I[ t ]; o.Q = sp.Q[ t ]; o.U = sp.U[ t ];
                                 o.V = sp.V[ t ]; o.pix = sp.pix[ t ]; o.cpix = sd.cpix[ t ];
                             }
@@ -335,8 +361,11 @@ k_forward( const __grid_constant__ fwd_params_t P )
                         continue;
                     }
                 }
-                if( ! peel && p.b != b_old ) set_wv( sc.w[ threadIdx.x ], p.b );
-                faces_all( P.m, p.b, p.c, p.d, fx );
+                if( ! peel )
+                {
+                    if( p.b != b_old ) set_wv( sc.w[ threadIdx.x ], p.b );
+                    faces_all( P.m, p.b, p.c, p.d, fx );
+                }
             }
             phase = PH_SEGMENT;
             after_crossing( false, left, lost );
@@ -389,10 +418,10 @@ k_forward( const __grid_constant__ fwd_params_t P )
                         p.x[ a ] = o.x[ a ]; p.c[ a ] = o.c[ a ]; p.inv[ a ] = P.inv_o[ a ];
                     }
                     p.b = o.b; p.d = P.o;
-                    ptau = o.ptau; pk = o.pk;
+                    ptau = o.ptau; pk = o.pk; ptc = o.tc;
                     sp.w[ t ] = o.w; sp.I[ t ] = o.I; sp.Q[ t ] = o.Q; sp.U[ t ] = o.U;
                     sp.V[ t ] = o.V; sp.pix[ t ] = o.pix; sd.cpix[ t ] = o.cpix;
-                    faces_all( P.m, p.b, p.c, p.d, fx );
+                    oray_faces( P, p.b, p.c, p.x, fx );
                     peel = true; solo = true; pend = 0;
                     phase = PH_SEGMENT;
                     continue;
@@ -477,19 +506,26 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     sp.Q[ t ] = sp.U[ t ] = sp.V[ t ] = 0.0f;
                     sp.pix[ t ] = pix;
                     sd.cpix[ t ] = coarse_pixel( P, pix, sc.batch[ t ] );
-                    bool queued = false;
                     if constexpr( DEFER )
-                        queued = defer_peel( 0 );
-                    if( ! queued )
                     {
-                        pend = 0; ptau = 0.0f; pk = 0;
+                        if( ! defer_peel( 0 ) )
+                            peel_now(  );
+                    }
+                    else if constexpr( ! DD )
+                        peel_now(  );
+                    else
+                    {
+                        pend = 0; ptau = 0.0f; pk = 0; ptc = 0.0;
                         park_walk( sp, p );
                         park_dir( sd, p, P.o, P.inv_o );
                         peel = true;
                     }
                 }
             }
-            faces_all( P.m, p.b, p.c, p.d, fx );
+            if( peel )
+                oray_faces( P, p.b, p.c, p.x, fx );
+            else
+                faces_all( P.m, p.b, p.c, p.d, fx );
             store_cold( sc, p );
             set_wv( p.w, p.b );
             continue;
@@ -541,14 +577,18 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             if( ! end && p.n_steps >= P.max_steps )
                 end = PK_STEP_CAP;
-            if constexpr( DEFER )
-                if( do_peel && defer_peel( p.n_scat ) )
-                    do_peel = false;             // queued: the walk goes on (or ends) now
+            if constexpr( ! DD )
+                if( do_peel )
+                {   // queued, or marched here: the walk goes on (or ends) now
+                    if( ! DEFER || ! defer_peel( p.n_scat ) )
+                        peel_now(  );
+                    do_peel = false;
+                }
             if( do_peel )
             {
                 park_walk( sp, p );
                 park_dir( sd, p, P.o, P.inv_o );
-                ptau = 0.0f; pk = 0; pend = end;
+                ptau = 0.0f; pk = 0; pend = end; ptc = 0.0;
                 peel = true;
                 phase = PH_SEGMENT;
             }
@@ -562,7 +602,10 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 phase = PH_SEGMENT;
             if( phase == PH_SEGMENT )
             {
-                faces_all( P.m, p.b, p.c, p.d, fx );
+                if( peel )
+                    oray_faces( P, p.b, p.c, p.x, fx );
+                else
+                    faces_all( P.m, p.b, p.c, p.d, fx );
                 store_cold( sc, p );
                 set_wv( p.w, p.b );
             }
@@ -570,18 +613,22 @@ k_forward( const __grid_constant__ fwd_params_t P )
         }
 
         // ---- PH_SEGMENT: segments of the active ray, up to KP_WALK_INNER
-        // before the next scheduling round where no peel-off ray runs here
-        // (DEFER, or no image) ----
+        // before the next scheduling round where no peel-off ray is
+        // scheduled here (all but the decomposed rounds) ----
         if( phase != PH_SEGMENT ) continue;
         #pragma unroll 1
-        for( int it = 0; it < ( DEFER || ( ! DD && P.img_n == 0 ) ? KP_WALK_INNER : 1 ); ++ it )
+        for( int it = 0; it < ( ! DD ? KP_WALK_INNER : 1 ); ++ it )
         {
             // the active ray's direction is in p.d / p.inv (a peel-off ray
             // holds them while the walk's are parked)
             const float2 sg = sigma_at( p.b, p.c );
             const float ext = __fadd_rn( sg.x, sg.y );
             int ax;
-            const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
+            double t;
+            if( peel )
+                t = oray_segment( fx, ptc, ax );
+            else
+                t = exit_cached( p.x, fx, p.d, p.inv, ax );
             const float et = __fmul_rn( ext, ( float ) t );
             bool interact = false, peel_cut = false;
             if( peel )
@@ -609,16 +656,20 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 break;
             }
             if( ! peel_cut )
-            {   // advance to the exit face and into the next cell (shared code)
-                if( ! peel )
-                {
+            {   // into the next cell
+                bool in_block;
+                if( peel )
+                    in_block = oray_step_in_block( P, p.b, p.c, p.x, fx, ax );
+                else
+                {   // the walk advances to the exit face
                     p.tau = __fsub_rn( p.tau, et );
                     add_flux( t );
+                    #pragma unroll
+                    for( int a = 0; a < 3; ++ a )
+                        if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
+                    in_block = step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d );
                 }
-                #pragma unroll
-                for( int a = 0; a < 3; ++ a )
-                    if( a != ax ) p.x[ a ] = __fma_rn( t, ( double ) comp( p.d, a ), p.x[ a ] );
-                if( ! step_in_block( P.m, p.b, p.c, p.x, fx, ax, p.d ) )
+                if( ! in_block )
                 {   // leaves the block: wait for a batched hand-off
                     hop_ax = ax;
                     phase = PH_HOP;
@@ -669,7 +720,8 @@ k_peel( const __grid_constant__ fwd_params_t P )
     const unsigned long long n_tasks =
         min( * P.pq_count, ( unsigned long long ) P.pq_cap );
     const int nc0 = P.m.nc[ 0 ], nc1 = P.m.nc[ 1 ];
-    double x[ 3 ], fx[ 3 ], g0[ 3 ], gd[ 3 ];
+    double x0[ 3 ], tm[ 3 ], g0[ 3 ], gd[ 3 ];    // ray start, distances to the next faces
+    double tc = 0.0;                              // distance travelled from x0
     int    c[ 3 ] = { 0, 0, 0 }, b = 0, hop_ax = 0, pk = 0, ci = 0;
     const float2 * sb = P.m.sigma;                // this block's coefficients
     float  ptau = 0.0f;
@@ -686,7 +738,8 @@ k_peel( const __grid_constant__ fwd_params_t P )
     long long task = -1;
     unsigned n_seg_done = 0;
     int phase = PH_EMIT;
-    // geometry of block b, its face cache and the cell's index in the block
+    // geometry of block b, the distances to the cell's faces (oray_faces's
+    // expression) and the cell's index in the block
     auto enter = [ & ](  )
     {
         const double * g = P.m.geo_d + 16 * ( size_t ) b;
@@ -695,8 +748,10 @@ k_peel( const __grid_constant__ fwd_params_t P )
         {
             g0[ a ] = g[ a ];
             gd[ a ] = g[ 3 + a ];
-            fx[ a ] = __fma_rn( ( double ) ( c[ a ] + ( comp( P.o, a ) > 0.0f ? 1 : 0 ) ), gd[ a ],
-                                g0[ a ] );
+            const float oa = comp( P.o, a );
+            tm[ a ] = oa == 0.0f ? 1e300
+                    : __dmul_rn( __dsub_rn( __fma_rn( ( double ) ( c[ a ] + ( oa > 0.0f ? 1 : 0 ) ),
+                                                      gd[ a ], g0[ a ] ), x0[ a ] ), P.inv_o[ a ] );
         }
         sb = P.m.sigma + ( size_t ) b * P.m.cpb;
         ci = c[ 0 ] + nc0 * ( c[ 1 ] + nc1 * c[ 2 ] );
@@ -782,9 +837,9 @@ k_peel( const __grid_constant__ fwd_params_t P )
                         continue;
                 }
             }
-            load_task_ray( P.pq, ( long long ) idx, x, b, c );
+            load_task_ray( P.pq, ( long long ) idx, x0, b, c );
             task = ( long long ) idx;
-            ptau = 0.0f; pk = 0;
+            ptau = 0.0f; pk = 0; tc = 0.0;
             enter(  );
             phase = PH_SEGMENT;
             continue;
@@ -795,6 +850,8 @@ k_peel( const __grid_constant__ fwd_params_t P )
             if( phase != PH_HOP ) continue;
             const int b_old = b;
             bool lost;
+            double x[ 3 ];                            // the crossing point: the new x0
+            oray_point( P, x0, tc, x );
             const bool left = ! cross_face( P.m, b, c, x, hop_ax, comp( P.o, hop_ax ) > 0.0f, lost );
             const unsigned m_moved = __ballot_sync( m_hop, ! left && b != b_old );
             if( lane == ( unsigned ) ( __ffs( m_hop ) - 1 ) && m_moved )
@@ -804,6 +861,9 @@ k_peel( const __grid_constant__ fwd_params_t P )
                 phase = PH_EMIT;
                 continue;
             }
+            #pragma unroll
+            for( int a = 0; a < 3; ++ a ) x0[ a ] = x[ a ];
+            tc = 0.0;
             enter(  );
             phase = pk >= ( 1 << 20 ) ? PH_EMIT : PH_SEGMENT;
             continue;
@@ -814,7 +874,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
         for( int it = 0; it < KP_PEEL_INNER; ++ it )
         {
             int ax;
-            const double t = exit_cached( x, fx, P.o, P.inv_o, ax );
+            const double t = oray_segment( tm, tc, ax );
             ++ n_seg_done;
             ++ pk;
             if constexpr( MODE == 2 )
@@ -839,10 +899,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
                     break;
                 }
             }
-            #pragma unroll
-            for( int a = 0; a < 3; ++ a )
-                if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
-            // step_in_block with the block geometry in registers
+            // into the next cell of the block, with its geometry in registers
             const bool pos = comp( P.o, ax ) > 0.0f;
             const int cax = ax == 0 ? c[ 0 ] : ( ax == 1 ? c[ 1 ] : c[ 2 ] );
             const int cn = cax + ( pos ? 1 : -1 );
@@ -855,9 +912,11 @@ k_peel( const __grid_constant__ fwd_params_t P )
             const double nf = __fma_rn( ( double ) ( cn + ( pos ? 1 : 0 ) ),
                                         ax == 0 ? gd[ 0 ] : ( ax == 1 ? gd[ 1 ] : gd[ 2 ] ),
                                         ax == 0 ? g0[ 0 ] : ( ax == 1 ? g0[ 1 ] : g0[ 2 ] ) );
+            const double ntm = __dmul_rn( __dsub_rn( nf, ax == 0 ? x0[ 0 ] : ( ax == 1 ? x0[ 1 ] : x0[ 2 ] ) ),
+                                          P.inv_o[ ax ] );
             #pragma unroll
             for( int a = 0; a < 3; ++ a )
-                if( a == ax ) { c[ a ] = cn; x[ a ] = fx[ a ]; fx[ a ] = nf; }
+                if( a == ax ) { c[ a ] = cn; tm[ a ] = ntm; }
             const int st = ax == 0 ? 1 : ( ax == 1 ? nc0 : nc0 * nc1 );
             ci += pos ? st : -st;
             if( pk >= ( 1 << 20 ) )

@@ -220,13 +220,14 @@ struct __align__( 16 ) dd_walk_t
 // contribution (the deposit happens where the ray ends).
 struct __align__( 16 ) dd_peel_t
 {
-    double x[ 3 ];
-    int    b, c[ 3 ];
+    double x[ 3 ];                 // the ray's start
+    int    b, c[ 3 ];              // the block entered, its cell
     float  ptau;
     int    pk;
     float  w, I, Q, U, V;
     int    pix, cpix;
-    int    pad[ 3 ];
+    int    pad;
+    double tc;                     // distance travelled from the start
 };
 
 enum pk_status { PK_ESCAPED = 1, PK_ABSORBED = 2, PK_SCATTER_CAP = 3, PK_STEP_CAP = 4,
@@ -524,33 +525,129 @@ __device__ __forceinline__ long long cold_pid( const SC & sc )
     return ( long long ) ( ( ( unsigned long long ) sc.pid_hi[ t ] << 32 ) | sc.pid_lo[ t ] );
 }
 
-// Optical depth from x to the domain boundary along the observer direction;
-// stops early (returns > tau_cut) once tau_cut is exceeded.
-__device__ __forceinline__ float peel_tau( const fwd_params_t & P, int b, const int c0[ 3 ],
-                                           const double x0[ 3 ], unsigned long long & steps,
-                                           unsigned long long & hops )
+// Peel-off rays toward the observer are marched as a fixed-direction cell
+// walk, block by block, measured from the point x0 where the ray entered its
+// block (or started): tm[a] is the distance from x0 to the next face of the
+// current cell on axis a ((face - x0[a]) times the inverse observer
+// direction; 1e300 on an axis the direction does not move along), a segment
+// ends at the nearest (the first axis wins ties), and its length is that
+// distance less the distance tc already travelled from x0 (never negative).
+// A block hand-off goes through the crossing point x0 + tc o (oray_point),
+// which cross_face snaps to the new block's face (wrapping a periodic
+// boundary), and that point becomes the new x0 with tc = 0 (oray_rebase).
+// The position is not advanced segment by segment, so a segment costs one
+// comparison chain and, inside a block, one new face.
+
+// tm for every axis of cell c of block b.
+__device__ __forceinline__ void oray_faces( const fwd_params_t & P, int b, const int c[ 3 ],
+                                            const double x0[ 3 ], double tm[ 3 ] )
+{
+    const double * g = P.m.geo_d + 16 * ( size_t ) b;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+    {
+        const float oa = comp( P.o, a );
+        tm[ a ] = oa == 0.0f ? 1e300
+                : __dmul_rn( __dsub_rn( __fma_rn( ( double ) ( c[ a ] + ( oa > 0.0f ? 1 : 0 ) ),
+                                                  g[ 3 + a ], g[ a ] ), x0[ a ] ), P.inv_o[ a ] );
+    }
+}
+
+// Length of the ray's next segment; ax receives its exit face's axis and tc
+// moves to the face.
+__device__ __forceinline__ double oray_segment( const double tm[ 3 ], double & tc, int & ax )
+{
+    int a0 = 0;
+    double tn = tm[ 0 ];
+    if( tm[ 1 ] < tn ) { tn = tm[ 1 ]; a0 = 1; }
+    if( tm[ 2 ] < tn ) { tn = tm[ 2 ]; a0 = 2; }
+    double dt = __dsub_rn( tn, tc );
+    dt = dt < 0.0 ? 0.0 : dt;
+    tc = tn > tc ? tn : tc;
+    ax = a0;
+    return dt;
+}
+
+// Into the next cell across face ax when it lies in the same block (the cell
+// and that axis's face distance move) and true; false, changing nothing,
+// when the step leaves the block.
+__device__ __forceinline__ bool oray_step_in_block( const fwd_params_t & P, int b, int c[ 3 ],
+                                                    const double x0[ 3 ], double tm[ 3 ], int ax )
+{
+    const bool pos = comp( P.o, ax ) > 0.0f;
+    // selects, not c[ ax ] / x0[ ax ]: a runtime index would move the arrays
+    // to local memory
+    const int cax = ax == 0 ? c[ 0 ] : ( ax == 1 ? c[ 1 ] : c[ 2 ] );
+    const int cn = cax + ( pos ? 1 : -1 );
+    if( cn < 0 || cn >= P.m.nc[ ax ] )
+        return false;
+    const double * g = P.m.geo_d + 16 * ( size_t ) b;
+    const double xa = ax == 0 ? x0[ 0 ] : ( ax == 1 ? x0[ 1 ] : x0[ 2 ] );
+    const double nt = __dmul_rn( __dsub_rn( __fma_rn( ( double ) ( cn + ( pos ? 1 : 0 ) ),
+                                                      g[ 3 + ax ], g[ ax ] ), xa ), P.inv_o[ ax ] );
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a )
+        if( a == ax ) { c[ a ] = cn; tm[ a ] = nt; }
+    return true;
+}
+
+// The ray's point at distance tc from x0.
+__device__ __forceinline__ void oray_point( const fwd_params_t & P, const double x0[ 3 ], double tc,
+                                            double x[ 3 ] )
+{
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) x[ a ] = __fma_rn( tc, P.o_d[ a ], x0[ a ] );
+}
+
+// Block hand-off of a ray across face ax: through its crossing point into the
+// neighbour (b, c move), which becomes its new x0 (tc = 0, tm refreshed).
+// False when the ray leaves the domain or finds no neighbour.
+__device__ __forceinline__ bool oray_rebase( const fwd_params_t & P, int & b, int c[ 3 ],
+                                             double x0[ 3 ], double & tc, double tm[ 3 ], int ax,
+                                             bool & lost )
+{
+    double x[ 3 ];
+    oray_point( P, x0, tc, x );
+    if( ! cross_face( P.m, b, c, x, ax, comp( P.o, ax ) > 0.0f, lost ) )
+        return false;
+    #pragma unroll
+    for( int a = 0; a < 3; ++ a ) x0[ a ] = x[ a ];
+    tc = 0.0;
+    oray_faces( P, b, c, x0, tm );
+    return true;
+}
+
+// A whole peel-off ray marched by one lane: the optical depth from x0 (cell
+// c0 of block b) to the domain boundary, or the first value beyond tau_cut;
+// segs and hops receive its segments and block hand-offs.  The segments are
+// those of the scheduled march (k_peel, the inline rays), one by one.
+__device__ __forceinline__ float oray_march( const fwd_params_t & P, int b, const int c0[ 3 ],
+                                                 const double x0[ 3 ], unsigned & segs,
+                                                 unsigned & hops )
 {
     int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
-    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
+    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };    // where the ray entered its block
+    double tm[ 3 ], tc = 0.0;
+    oray_faces( P, b, c, x, tm );
     float tau = 0.0f;
     for( int k = 0; k < ( 1 << 20 ); ++ k )
     {
         const float2 sg = P.m.sigma[ cell_index( P.m, b, c ) ];
         const float ext = __fadd_rn( sg.x, sg.y );
         int ax;
-        const double t = exit_dist( P.m, b, c, x, P.o, P.inv_o, ax );
-        tau = __fadd_rn( tau, __fmul_rn( ext, ( float ) t ) );
-        ++ steps;
+        const double dt = oray_segment( tm, tc, ax );
+        tau = __fadd_rn( tau, __fmul_rn( ext, ( float ) dt ) );
+        ++ segs;
         if( tau > P.tau_cut )
             return tau;
-        #pragma unroll
-        for( int a = 0; a < 3; ++ a )
-            if( a != ax ) x[ a ] = __fma_rn( t, P.o_d[ a ], x[ a ] );
-        bool lost;
-        const int b_old = b;
-        if( ! cross_face( P.m, b, c, x, ax, comp( P.o, ax ) > 0.0f, lost ) )
-            return tau;
-        hops += b != b_old;
+        if( ! oray_step_in_block( P, b, c, x, tm, ax ) )
+        {
+            bool lost;
+            const int b_old = b;
+            if( ! oray_rebase( P, b, c, x, tc, tm, ax, lost ) )
+                return tau;
+            hops += b != b_old;
+        }
     }
     return tau;
 }

@@ -309,27 +309,102 @@ static int tcross( const tctx * t, int * b, int * c, double * x, int ax, int pos
     return 1;
 }
 
+/* Peel-off ray toward the observer: a fixed-direction cell march, block by
+ * block, measured from the point x0 where the ray entered its current block
+ * (or started).  tm[a] is the distance from x0 to the next face of the
+ * current cell on axis a ((face - x0[a]) times the inverse direction; 1e300
+ * on an axis the observer direction does not move along); a segment ends at
+ * the nearest (the first axis wins ties) and its length is that distance
+ * less the distance already travelled from x0 (tc; never negative).  A block
+ * hand-off goes through the crossing point x0 + tc o, snapped to the new
+ * block's face (which also wraps a periodic boundary), and makes it the new
+ * x0.  The kernels march every peel-off ray this way (k_peel, and the rays of
+ * k_forward and k_adjoint marched where they start). */
+typedef struct
+{
+    int    b, c[ 3 ];
+    double x0[ 3 ], tm[ 3 ], tc;
+} tray;
+
+static void tray_faces( const tctx * t, tray * r )
+{
+    const kpo_mesh_t * m = t->m;
+    for( int a = 0; a < 3; ++ a )
+    {
+        const float oa = om_comp( t->o, a );
+        if( oa == 0.0f ) { r->tm[ a ] = 1e300; continue; }
+        const double face = fma( ( double ) ( r->c[ a ] + ( oa > 0.0f ? 1 : 0 ) ),
+                                 m->dx0[ 3 * r->b + a ], m->xf0[ 3 * r->b + a ] );
+        r->tm[ a ] = ( face - r->x0[ a ] ) * t->inv_o[ a ];
+    }
+}
+
+static void tray_start( const tctx * t, tray * r, int b, const int * c0, const double * x0 )
+{
+    r->b = b;
+    for( int a = 0; a < 3; ++ a ) { r->c[ a ] = c0[ a ]; r->x0[ a ] = x0[ a ]; }
+    r->tc = 0.0;
+    tray_faces( t, r );
+}
+
+/* Length of the ray's next segment; *ax receives the axis of its exit face. */
+static double tray_segment( tray * r, int * ax )
+{
+    int a0 = 0;
+    double tn = r->tm[ 0 ];
+    if( r->tm[ 1 ] < tn ) { tn = r->tm[ 1 ]; a0 = 1; }
+    if( r->tm[ 2 ] < tn ) { tn = r->tm[ 2 ]; a0 = 2; }
+    double dt = tn - r->tc;
+    dt = dt < 0.0 ? 0.0 : dt;
+    if( tn > r->tc ) r->tc = tn;
+    * ax = a0;
+    return dt;
+}
+
+/* Into the next cell across face ax; 0 when the ray leaves the domain. */
+static int tray_cross( const tctx * t, tray * r, int ax, unsigned long long * hops )
+{
+    const kpo_mesh_t * m = t->m;
+    const int pos = om_comp( t->o, ax ) > 0.0f;
+    const int cn = r->c[ ax ] + ( pos ? 1 : -1 );
+    if( cn >= 0 && cn < m->nc[ ax ] )
+    {
+        r->c[ ax ] = cn;
+        const double face = fma( ( double ) ( cn + pos ), m->dx0[ 3 * r->b + ax ],
+                                 m->xf0[ 3 * r->b + ax ] );
+        r->tm[ ax ] = ( face - r->x0[ ax ] ) * t->inv_o[ ax ];
+        return 1;
+    }
+    double x[ 3 ];
+    for( int a = 0; a < 3; ++ a ) x[ a ] = fma( r->tc, t->o_d[ a ], r->x0[ a ] );
+    int lost;
+    const int b_old = r->b;
+    if( ! tcross( t, & r->b, r->c, x, ax, pos, & lost ) ) return 0;
+    * hops += r->b != b_old;
+    for( int a = 0; a < 3; ++ a ) r->x0[ a ] = x[ a ];
+    r->tc = 0.0;
+    tray_faces( t, r );
+    return 1;
+}
+
+/* Optical depth from x0 to the domain boundary along the observer direction;
+ * stops early (returns > tau_cut) once tau_cut is exceeded. */
 static float tpeel_tau( const tctx * t, int b, const int * c0, const double * x0,
                         unsigned long long * steps, unsigned long long * hops )
 {
-    int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
-    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
+    tray r;
+    tray_start( t, & r, b, c0, x0 );
     float tau = 0.0f;
     for( int k = 0; k < ( 1 << 20 ); ++ k )
     {
-        const long ci = tcell( t, b, c );
+        const long ci = tcell( t, r.b, r.c );
         const float ext = t->sig[ 2 * ci ] + t->sig[ 2 * ci + 1 ];
         int ax;
-        const double tt = texit( t, b, c, x, t->o, t->inv_o, & ax );
-        tau = tau + ext * ( float ) tt;
+        const double dt = tray_segment( & r, & ax );
+        tau = tau + ext * ( float ) dt;
         ++ * steps;
         if( tau > t->tau_cut ) return tau;
-        for( int a = 0; a < 3; ++ a )
-            if( a != ax ) x[ a ] = fma( tt, t->o_d[ a ], x[ a ] );
-        int lost;
-        const int b_old = b;
-        if( ! tcross( t, & b, c, x, ax, om_comp( t->o, ax ) > 0.0f, & lost ) ) return tau;
-        * hops += b != b_old;
+        if( ! tray_cross( t, & r, ax, hops ) ) return tau;
     }
     return tau;
 }
@@ -767,23 +842,21 @@ static float tscore( const float * g, int pix, float I, float Q, float U, float 
 static void tpeel_deposit( const tctx * t, int b, const int * c0, const double * x0, float G,
                            long long * g_len, double gsc, unsigned long long * steps )
 {
-    int c[ 3 ] = { c0[ 0 ], c0[ 1 ], c0[ 2 ] };
-    double x[ 3 ] = { x0[ 0 ], x0[ 1 ], x0[ 2 ] };
+    tray r;
+    tray_start( t, & r, b, c0, x0 );
     float tau = 0.0f;
+    unsigned long long hops = 0;
     for( int k = 0; k < ( 1 << 20 ); ++ k )
     {
-        const long ci = tcell( t, b, c );
+        const long ci = tcell( t, r.b, r.c );
         const float ext = t->sig[ 2 * ci ] + t->sig[ 2 * ci + 1 ];
         int ax;
-        const double tt = texit( t, b, c, x, t->o, t->inv_o, & ax );
-        tau = tau + ext * ( float ) tt;
+        const double dt = tray_segment( & r, & ax );
+        tau = tau + ext * ( float ) dt;
         ++ * steps;
         if( tau > t->tau_cut ) return;
-        tgadd( g_len, ci, -( double ) G * tt, gsc );
-        for( int a = 0; a < 3; ++ a )
-            if( a != ax ) x[ a ] = fma( tt, t->o_d[ a ], x[ a ] );
-        int lost;
-        if( ! tcross( t, & b, c, x, ax, om_comp( t->o, ax ) > 0.0f, & lost ) ) return;
+        tgadd( g_len, ci, -( double ) G * dt, gsc );
+        if( ! tray_cross( t, & r, ax, & hops ) ) return;
     }
 }
 
