@@ -475,7 +475,28 @@ k_forward( const __grid_constant__ fwd_params_t P )
             {
                 const int r = P.dd_owner[ p.b ];
                 if( r != P.dd_rank )
-                {   // emitted into a block of rank r (plane sources): hand it over
+                {   // emitted into a block of rank r (plane sources, caller-made
+                    // packets): hand it over, with the direct light of the
+                    // emission as a peel-off ray that starts there
+                    if( P.img_n > 0 && peel_I > 0.0f )
+                    {
+                        const int pix = image_pixel( P, p.x );
+                        if( pix >= 0 )
+                        {
+                            const unsigned long long k = atomicAdd( P.dd_out_count + 1, 1ull );
+                            if( k < ( unsigned long long ) P.dd_cap_peel )
+                            {
+                                P.dd_out_peel_rank[ k ] = r;
+                                dd_peel_t & o = P.dd_out_peel[ k ];
+                                for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+                                o.b = p.b; o.ptau = 0.0f; o.pk = 0; o.tc = 0.0;
+                                o.w = p.w; o.I = peel_I; o.Q = o.U = o.V = 0.0f;
+                                o.pix = pix; o.cpix = coarse_pixel( P, pix, sc.batch[ threadIdx.x ] );
+                            }
+                            else
+                                atomicOr( P.m.status, ST_QUEUE_FULL );
+                        }
+                    }
                     const unsigned long long k = atomicAdd( P.dd_out_count, 1ull );
                     if( k < ( unsigned long long ) P.dd_cap_walk )
                     {
