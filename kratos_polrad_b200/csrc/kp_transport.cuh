@@ -268,7 +268,8 @@ __device__ __forceinline__ void set_inv( packet_t & p )
     for( int a = 0; a < 3; ++ a )
     {
         const float da = comp( p.d, a );
-        p.inv[ a ] = da != 0.0f ? __ddiv_rn( 1.0, ( double ) da ) : 0.0;
+        // the correctly rounded reciprocal: 1.0 / da, bit for bit
+        p.inv[ a ] = da != 0.0f ? __drcp_rn( ( double ) da ) : 0.0;
     }
 }
 

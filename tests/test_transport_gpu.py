@@ -63,14 +63,18 @@ def test_float_tally_mode_close_to_fixed():
     torch.cuda.synchronize()
     img_fx = fx.image.cpu().numpy() * 2.0 ** -t.fx_shift
     img_fl = fl.image.cpu().numpy().astype(np.float64)
-    # Float atomics sum the same deposits in another order.  Pixel sums above
-    # a noise floor of 1e-3 of the image's peak agree within 1e-6 relative;
-    # below it a few deposits of either sign may cancel, and the bar is
-    # 1e-9 of the peak there (the int64 rounding is 2^-32 per deposit).
-    peak = np.abs(img_fx).max()
-    big = np.abs(img_fx) > 1e-3 * peak
-    assert big.sum() > 400
-    rel = np.abs(img_fl - img_fx)[big] / np.abs(img_fx)[big]
+    # Float atomics sum the same deposits in another order.  On every pixel
+    # whose intensity is above a noise floor of 1e-3 of the peak, each Stokes
+    # component agrees within 1e-6 of the pixel's I: a deposit's |Q|, |U|,
+    # |V| never exceed its I, so the summation error of every component is
+    # bounded relative to I, while Q, U and V themselves may cancel to near
+    # zero.  Below the floor the bar is 1e-9 of the peak (the int64 rounding
+    # is 2^-32 per deposit).
+    I_fx = img_fx[..., 0]
+    peak = I_fx.max()
+    big = I_fx > 1e-3 * peak
+    assert big.sum() > 100
+    rel = (np.abs(img_fl - img_fx)[big] / I_fx[big][:, None]).max(1)
     assert rel.max() <= 1e-6, (rel.max(), np.percentile(rel, 99))
     np.testing.assert_allclose(img_fl[~big], img_fx[~big], rtol=1e-6, atol=1e-9 * peak)
     np.testing.assert_allclose(img_fl[..., 0].sum(), img_fx[..., 0].sum(), rtol=1e-7)
