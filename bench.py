@@ -372,7 +372,7 @@ def _timed(fn):
     return out, e0.elapsed_time(e1)
 
 
-def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=200_000_000, n_batch=20, n_dirs=8,
+def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=600_000_000, n_batch=20, n_dirs=8,
                     n_cells=16, n_cell_check=50_000_000):
     """Paired batch-means comparison of the path-replay gradient with
     common-random-number central differences of the same estimator.
@@ -383,10 +383,12 @@ def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=200_000_000, n_batch=20,
     adjoint and the differences use the same packets.
 
     Blob directions (the 2% bar): Gaussian density blobs of radius 0.08 box
-    (both coefficients scaled by 1 +- 0.05 phi, albedo unchanged) centred on
-    the cells of largest |dF/dsigma_sca|, chosen from a gradient of other
-    packets (ids from 5e9) so that the choice does not favour the checked
-    estimate.  For each: the difference's mean, its batch-means standard
+    (both coefficients scaled by 1 +- 0.05 phi, albedo unchanged).  Their
+    centres are the points of a 16^3 grid over the box with the largest
+    |dF/d blob| (at least 0.15 box apart), that derivative taken from a
+    gradient of other packets (ids from 5e9), so that the choice does not
+    favour the checked estimate; large derivatives keep the differences'
+    relative noise low.  For each: the difference's mean, its batch-means standard
     error, and the adjoint's relative difference from it; a direction passes
     when that is within 2% and the standard error is within 1%.
     Single cells (a z-score check, too noisy for a 2% bar): n_cells cells
@@ -401,15 +403,24 @@ def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=200_000_000, n_batch=20,
     a64 = a.double()
     mesh.set_sigma(sig)
     sel = dataclasses.replace(cfg, n_packets=20_000_000, packet_offset=5_000_000_000, n_record=0)
-    g_sel = gradients(mesh, sel, a, 24)[0].cpu().numpy()
+    gs_sel, ga_sel = gradients(mesh, sel, a, 24)
+    g_sel = gs_sel.cpu().numpy()
     xc = scenes.cell_centers(mesh)
-    order = np.argsort(-np.abs(g_sel))
+    xc_d = torch.tensor(xc, device="cuda", dtype=torch.float64)
+    w_sel = (gs_sel.double() * torch.tensor(sig[:, 0], device="cuda", dtype=torch.float64)
+             + ga_sel.double() * torch.tensor(sig[:, 1], device="cuda", dtype=torch.float64))
+    lo, hi = xc.min(0), xc.max(0)
+    grid = np.stack(np.meshgrid(*[np.linspace(lo[k], hi[k], 16) for k in range(3)],
+                                indexing="ij"), -1).reshape(-1, 3)
+    blob = np.array([float((w_sel * torch.exp(-((xc_d - torch.tensor(c, device="cuda")) ** 2)
+                                              .sum(1) / (2 * 0.08 ** 2))).sum()) for c in grid])
     centres = []
-    for k in order:                       # blob centres at least 0.15 box apart
-        if all(np.linalg.norm(xc[k] - c) > 0.15 for c in centres):
-            centres.append(xc[k])
+    for k in np.argsort(-np.abs(blob)):   # blob centres at least 0.15 box apart
+        if all(np.linalg.norm(grid[k] - c) > 0.15 for c in centres):
+            centres.append(grid[k])
         if len(centres) == n_dirs:
             break
+    order = np.argsort(-np.abs(g_sel))
     phis = [np.exp(-((xc - c) ** 2).sum(1) / (2 * 0.08 ** 2)) for c in centres]
     cells = rng.choice(order[:2000], n_cells, replace=False)
     sig_d = torch.tensor(sig, device="cuda", dtype=torch.float64)
@@ -821,6 +832,10 @@ def run_large(args):
     c = tal.counts()
     bimg = tal.image_batch.cpu().numpy() * tal.scale()
     p_tan, rel = scenes.batch_rel_error(bimg)
+    # tangential polarization about the nearest source's image position:
+    # linear in Q, U (unbiased batch means), positive for the scattered
+    # light's pattern around each source
+    p_loc, rel_loc = scenes.batch_rel_error(bimg, scenes.source_pixels(cfg, bimg.shape[1]))
     # the image-integrated linear polarization fraction sqrt(Q^2+U^2)/I, and
     # the intensity-weighted mean degree of the coarse pixels, with their
     # batch-means relative std-errors
@@ -842,6 +857,7 @@ def run_large(args):
                                     "blocks": mesh.n_blocks, "cells": mesh.n_cells,
                                     "sigma_MB": sig.nbytes / 1e6, "image": cfg.image_n},
             "forward_ms": t_fwd, "counts": c, "pol_tangential": p_tan, "pol_rel_std_err": rel,
+            "pol_tangential_about_sources": p_loc, "pol_tangential_about_sources_rel_std_err": rel_loc,
             "pol_integrated": p_int, "pol_integrated_rel_std_err": rel_int,
             "pol_mean_degree_coarse": p_deg, "pol_mean_degree_rel_std_err": rel_deg,
             "adjoint_ms": t_adj, "adjoint_cost_vs_forward": t_adj / t_fwd,

@@ -126,6 +126,16 @@ public:
         if( gen_ && n_par_ > 0 )
             table_ = static_cast< kp_packet_init_t * >(
                 alloc( sizeof( kp_packet_init_t ) * ( size_t ) n_par_, s ) );
+        if( cfg_.tally_mode == KP_TALLY_FLOAT )
+        {   // the float atomics' rounding errors (kp_tallies_t::carry)
+            size_t n = ( size_t ) n_cells_;
+            if( cfg_.n_mu_bins > 0 )
+                n += ( size_t ) cfg_.n_batches * cfg_.n_mu_bins * 4;
+            if( cfg_.image_n > 0 )
+                n += ( size_t ) cfg_.image_n * cfg_.image_n * 4
+                     + ( size_t ) cfg_.n_batches * cfg_.image_batch_n * cfg_.image_batch_n * 4;
+            carry_ = static_cast< float * >( alloc( sizeof( float ) * n, s ) );
+        }
         done_ = 0;
     }
 
@@ -153,6 +163,8 @@ public:
         t.image_batch = image_batch_;
         t.counters = counters_;
         t.flux = flux_;
+        t.carry = carry_;
+        t.flux_n = n_cells_;
         transport::forward( * mesh_, c, t, s );
         done_ += n_par_;
     }
@@ -253,10 +265,10 @@ public:
     virtual void finalize(  ) noexcept
     {
         for( void * p : { flux_, ( void * ) counters_, mu_, image_, image_batch_,
-                          ( void * ) table_ } )
+                          ( void * ) table_, ( void * ) carry_ } )
             if( p ) kp_free( p );
         flux_ = nullptr; counters_ = nullptr; mu_ = image_ = image_batch_ = nullptr;
-        table_ = nullptr;
+        table_ = nullptr; carry_ = nullptr;
         mesh_ = nullptr;
     }
 
@@ -296,6 +308,7 @@ private:
     void *                     image_batch_ = nullptr;
     unsigned long long *       counters_ = nullptr;
     kp_packet_init_t *         table_ = nullptr;
+    float *                    carry_ = nullptr;
 };
 
 }   // namespace kp::particle::radiation

@@ -362,6 +362,19 @@ typedef struct kp_tallies
     unsigned long long * counters;
     kp_packet_record_t * records;
     void * flux;
+    float * carry;       /* KP_TALLY_FLOAT only, optional (NULL: plain float
+                            atomics): device floats, zeroed before the first
+                            call, that collect the rounding error of every
+                            float atomic, laid out as the float tallies in
+                            use one after another: image, image_batch (both
+                            with an image), mu (n_mu_bins > 0), flux (flux
+                            set; flux_n entries).  Each solve adds them into
+                            the tallies at its end and zeroes them, so a
+                            tally is the exact sum of its float deposits up
+                            to about 2^-24 of its own value instead of 2^-24
+                            of every partial sum.  The batched solve does not
+                            take it. */
+    long long flux_n;    /* entries of flux (needed with carry and flux)     */
 } kp_tallies_t;
 
 /* Asynchronous on `stream`.  Calls that share a mesh handle must not
@@ -503,7 +516,8 @@ int kp_mesh_tape_id( const kp_mesh_t * mesh, long long * tape_id );
  * are marched inside the walk kernel, where they start (kp_transport_forward
  * queues them for a second kernel, and the queue is an allocation): the
  * int64 tallies are the same bit for bit, float tallies agree within float
- * rounding (another summation order), and the solve is slower.  A
+ * rounding (another summation order; kp_tallies_t::carry, the caller's
+ * memory, folds in their rounding errors), and the solve is slower.  A
  * kp_transport_split_event event is recorded after the walk.  Inputs and outputs are the
  * caller's: the mesh must already be on the current device (kp_mesh_upload,
  * or an earlier kp_mesh_set_sigma, at set-up time), else KP_ERR_CONFIG; a

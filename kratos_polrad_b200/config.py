@@ -83,7 +83,8 @@ class CTransportCfg(ctypes.Structure):
 
 class CTallies(ctypes.Structure):
     _fields_ = [("mu", c_void_p), ("image", c_void_p), ("image_batch", c_void_p),
-                ("counters", c_void_p), ("records", c_void_p), ("flux", c_void_p)]
+                ("counters", c_void_p), ("records", c_void_p), ("flux", c_void_p),
+                ("carry", c_void_p), ("flux_n", c_ll)]
 
 
 # numpy view of kp_packet_record_t (88 bytes)

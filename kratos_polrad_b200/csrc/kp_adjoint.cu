@@ -224,7 +224,9 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
                 continue;
             }
             const long long pid = P.pid0 + ( P.adj_list ? ( long long ) P.adj_list[ idx ]
-                                                        : ( long long ) idx );
+                                                        : source_major( ( long long ) idx,
+                                                                        ( long long ) n_items,
+                                                                        P.n_src ) );
             float peel_I;
             if( ! emit_any( P, pid, p, peel_I ) )
             {
@@ -525,11 +527,11 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
                 phase = PH_DONE;
                 continue;
             }
-            lp = ( int ) idx;
+            lp = ( int ) source_major( ( long long ) idx, P.n_packets, P.n_src );
             if constexpr( PASS == 1 )
                 if( P.adj_flag[ lp ] )
                     continue;                     // replayed by k_adjoint
-            const long long pid = P.pid0 + ( long long ) idx;
+            const long long pid = P.pid0 + ( long long ) lp;
             float peel_I;
             if( ! emit_any( P, pid, p, peel_I ) )
             {
@@ -954,6 +956,7 @@ extern "C" int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_c
         {   // more packets than one chunk of the queue: an untaped solve
             P.work = mesh->workspace(  );
             kp::launch_deferred_solve( mesh, P, cfg->tally_mode, ( cudaStream_t ) stream );
+            kp::fold_carry( * cfg, * tallies, ( cudaStream_t ) stream );
             return;
         }
         kp::adjoint_buffers( mesh, P, P.n_packets );
@@ -965,6 +968,7 @@ extern "C" int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_c
             kp::launch_deferred_chunk< KP_TALLY_FIXED, true >( P, s );
         else
             kp::launch_deferred_chunk< KP_TALLY_FLOAT, true >( P, s );
+        kp::fold_carry( * cfg, * tallies, s );
         mesh->tape_cfg = * cfg;
         mesh->tape_cfg.sources = nullptr;
         for( int k = 0; k < cfg->n_sources; ++ k ) mesh->tape_src[ k ] = cfg->sources[ k ];

@@ -191,7 +191,8 @@ k_forward( const __grid_constant__ fwd_params_t P )
             }
             else
                 i = cell_index( P.m, p.b, p.c );
-            add_grad< TALLY >( P.flux, i, __dmul_rn( dl, sc.wv[ threadIdx.x ] ), P.flux_scale );
+            add_grad< TALLY >( P.flux, P.c_flux, i, __dmul_rn( dl, sc.wv[ threadIdx.x ] ),
+                               P.flux_scale );
         }
     };
 
@@ -247,7 +248,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
             {
                 end = PK_ESCAPED;
                 if( tally_escape< TALLY >( P, ( char * ) P.mu_tally + ( size_t ) si * P.mu_scene_stride
-                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), p,
+                                             * ( TALLY == KP_TALLY_FIXED ? 8 : 4 ), P.c_mu, p,
                                              sc.batch[ threadIdx.x ] ) )
                     count( sp, KP_CNT_DEPOSITS );
             }
@@ -459,8 +460,11 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 peel_I = s.kind == KP_SOURCE_POINT && s.emit == KP_EMIT_ISOTROPIC ? 0x1.45f306p-4f
                                                                                   : 0.0f;
             }
-            else
+            else if constexpr( DD )
                 ok = emit_any( P, P.pid0 + ( long long ) idx, p, peel_I );
+            else
+                ok = emit_any( P, P.pid0 + source_major( ( long long ) idx, P.n_packets, P.n_src ),
+                               p, peel_I );
             if( ! ok )
             {
                 atomicOr( P.m.status, ST_BAD_SOURCE );
@@ -1044,6 +1048,72 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     P.n_record = c.n_record;
     P.flux = t.flux;
     P.flux_scale = std::ldexp( 1.0, c.flux_fx_shift > 0 ? c.flux_fx_shift : c.fx_shift );
+    const carry_fold_t f = carry_layout( c, t );
+    for( int k = 0; k < f.n_seg; ++ k )
+    {
+        if( f.seg[ k ].hi == t.image )       P.c_image = f.seg[ k ].c;
+        if( f.seg[ k ].hi == t.image_batch ) P.c_img_batch = f.seg[ k ].c;
+        if( f.seg[ k ].hi == t.mu )          P.c_mu = f.seg[ k ].c;
+        if( f.seg[ k ].hi == t.flux )        P.c_flux = f.seg[ k ].c;
+    }
+}
+
+// The float tallies' carries (kp_tallies_t::carry): image, image_batch, mu,
+// flux, one after another, each as long as its tally.
+carry_fold_t carry_layout( const kp_transport_cfg_t & c, const kp_tallies_t & t )
+{
+    carry_fold_t f {  };
+    if( c.tally_mode != KP_TALLY_FLOAT || t.carry == nullptr )
+        return f;
+    float * q = t.carry;
+    auto add = [ & ]( void * hi, long long n )
+    {
+        f.seg[ f.n_seg ++ ] = carry_seg_t { static_cast< float * >( hi ), q, n };
+        q += n;
+    };
+    if( c.image_n > 0 )
+    {
+        const long long bn = c.image_batch_n;
+        add( t.image, 4ll * c.image_n * c.image_n );
+        add( t.image_batch, 4ll * c.n_batches * bn * bn );
+    }
+    if( c.n_mu_bins > 0 )
+        add( t.mu, 4ll * c.n_batches * c.n_mu_bins );
+    if( t.flux )
+    {
+        require( t.flux_n > 0, "a flux tally with a carry needs flux_n", KP_ERR_CONFIG );
+        add( t.flux, t.flux_n );
+    }
+    return f;
+}
+
+__global__ void k_fold_carry( const carry_fold_t f )
+{
+    const long long stride = ( long long ) gridDim.x * blockDim.x;
+    for( int k = 0; k < f.n_seg; ++ k )
+        for( long long i = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; i < f.seg[ k ].n;
+             i += stride )
+        {
+            const float e = f.seg[ k ].c[ i ];
+            if( e != 0.0f )
+            {
+                f.seg[ k ].hi[ i ] = __fadd_rn( f.seg[ k ].hi[ i ], e );
+                f.seg[ k ].c[ i ] = 0.0f;
+            }
+        }
+}
+
+// Adds the carries into their tallies and zeroes them (after a solve's
+// kernels, on its stream); nothing without a carry.
+void fold_carry( const kp_transport_cfg_t & c, const kp_tallies_t & t, cudaStream_t s )
+{
+    const carry_fold_t f = carry_layout( c, t );
+    long long n = 0;
+    for( int k = 0; k < f.n_seg; ++ k ) n += f.seg[ k ].n;
+    if( n == 0 ) return;
+    const long long grid = std::min< long long >( ( n + 255 ) / 256, 4 * 148 );
+    k_fold_carry<<< ( unsigned ) grid, 256, 0, s >>>( f );
+    KP_CUDA( cudaGetLastError(  ) );
 }
 
 // Converts one C source to its device form; point sources are located in
@@ -1258,10 +1328,14 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
                 kp::launch_deferred< KP_TALLY_FIXED >( mesh, P, ( cudaStream_t ) stream );
             else
                 kp::launch_deferred< KP_TALLY_FLOAT >( mesh, P, ( cudaStream_t ) stream );
-            return;
         }
-        kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
-        if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
+        else
+        {
+            kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
+            if( kp::split_event )
+                KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
+        }
+        kp::fold_carry( * cfg, * tallies, ( cudaStream_t ) stream );
     } );
 }
 
@@ -1356,6 +1430,7 @@ extern "C" int kp_transport_forward_dd( kp_mesh_t * mesh, const kp_transport_cfg
         else
             fx ? kp::launch_dd< KP_TALLY_FIXED, false >( P, items, s )
                : kp::launch_dd< KP_TALLY_FLOAT, false >( P, items, s );
+        kp::fold_carry( * cfg, * tallies, s );
     } );
 }
 
@@ -1421,5 +1496,6 @@ extern "C" int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transpor
         P.work = static_cast< unsigned long long * >( kp::noalloc_scratch(  ) );
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
         if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
+        kp::fold_carry( * cfg, * tallies, ( cudaStream_t ) stream );
     } );
 }

@@ -82,6 +82,8 @@ struct fwd_params_t
     long long   n_record;
     void      * flux;              // path-length flux tally [n_cells] (null: off)
     double      flux_scale;        // its fixed point scale
+    // float tallies' rounding-error carries (kp_tallies_t::carry; null: none)
+    float     * c_image, * c_img_batch, * c_mu, * c_flux;
     unsigned long long * work;     // scratch: next packet index
     // adjoint only
     const float4 * adj_img;        // dL/d(image) [img_n * img_n] (I, Q, U, V)
@@ -653,14 +655,55 @@ __device__ __forceinline__ float oray_march( const fwd_params_t & P, int b, cons
     return tau;
 }
 
+// Carries of the float tallies and the fold that adds them in after a solve
+// (kp_tallies_t::carry).
+struct carry_seg_t
+{
+    float   * hi;                  // the tally
+    float   * c;                   // its carry
+    long long n;
+};
+struct carry_fold_t
+{
+    carry_seg_t seg[ 4 ];
+    int         n_seg;
+};
+carry_fold_t carry_layout( const kp_transport_cfg_t & c, const kp_tallies_t & t );
+void fold_carry( const kp_transport_cfg_t & c, const kp_tallies_t & t, cudaStream_t s );
+
+// FP32 atomic add of v to base[i].  With a carry array, the rounding error
+// of the sum that the atomic stored goes to carry[i]: atom.add.f32 rounds to
+// nearest even, so the value it read (old) and v give that error exactly by
+// the error-free transformation TwoSum (Knuth, TAOCP vol. 2, 4.2.2; Moller
+// 1965): s = old + v, bv = s - old, e = (old - (s - bv)) + (v - bv), and
+// old + v = s + e exactly.  base[i] + carry[i], folded after the solve, is
+// then the float deposits' sum up to the carry's own rounding (of order
+// 2^-24 of the sum of the errors, themselves 2^-24 of the partial sums).
+// Subnormal operands, which the atomic flushes to zero, lose at most 2^-126.
+__device__ __forceinline__ void atomic_add_carry( float * base, float * carry, size_t i, float v )
+{
+    if( carry == nullptr )
+    {
+        atomicAdd( base + i, v );
+        return;
+    }
+    const float old = atomicAdd( base + i, v );
+    const float s   = __fadd_rn( old, v );
+    const float bv  = __fsub_rn( s, old );
+    const float e   = __fadd_rn( __fsub_rn( old, __fsub_rn( s, bv ) ), __fsub_rn( v, bv ) );
+    if( e != 0.0f )
+        atomicAdd( carry + i, e );
+}
+
 template< int TALLY >
-__device__ __forceinline__ void add_tally( void * base, size_t i, float v, double sc )
+__device__ __forceinline__ void add_tally( void * base, float * carry, size_t i, float v,
+                                           double sc )
 {
     if( TALLY == KP_TALLY_FIXED )
         atomicAdd( ( unsigned long long * ) base + i,
                    ( unsigned long long ) __double2ll_rn( __dmul_rn( ( double ) v, sc ) ) );
     else
-        atomicAdd( ( float * ) base + i, v );
+        atomic_add_carry( ( float * ) base, carry, i, v );
 }
 
 // Image pixel (iy * n + ix) under position x, or -1 outside the image.
@@ -700,26 +743,35 @@ __device__ __forceinline__ void deposit_pixel( const fwd_params_t & P, int pixel
                                                float I, float Q, float U, float V )
 {
     const size_t pix = ( size_t ) pixel * 4;
-    add_tally< TALLY >( P.image, pix + 0, I, P.fx_scale );
-    add_tally< TALLY >( P.image, pix + 1, Q, P.fx_scale );
-    add_tally< TALLY >( P.image, pix + 2, U, P.fx_scale );
-    add_tally< TALLY >( P.image, pix + 3, V, P.fx_scale );
+    add_tally< TALLY >( P.image, P.c_image, pix + 0, I, P.fx_scale );
+    add_tally< TALLY >( P.image, P.c_image, pix + 1, Q, P.fx_scale );
+    add_tally< TALLY >( P.image, P.c_image, pix + 2, U, P.fx_scale );
+    add_tally< TALLY >( P.image, P.c_image, pix + 3, V, P.fx_scale );
     const size_t bp = ( size_t ) cpix * 4;
-    add_tally< TALLY >( P.img_batch, bp + 0, I, P.fx_scale );
-    add_tally< TALLY >( P.img_batch, bp + 1, Q, P.fx_scale );
-    add_tally< TALLY >( P.img_batch, bp + 2, U, P.fx_scale );
-    add_tally< TALLY >( P.img_batch, bp + 3, V, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, P.c_img_batch, bp + 0, I, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, P.c_img_batch, bp + 1, Q, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, P.c_img_batch, bp + 2, U, P.fx_scale );
+    add_tally< TALLY >( P.img_batch, P.c_img_batch, bp + 3, V, P.fx_scale );
 }
 
-// Adjoint gradient deposit (int64 fixed point or float atomics).
+// Double-valued deposit (adjoint gradients, flux): int64 fixed point, or the
+// value rounded to float and added by float atomics (with a carry array,
+// carrying their rounding error as atomic_add_carry does).
 template< int TALLY >
-__device__ __forceinline__ void add_grad( void * base, size_t i, double v, double sc )
+__device__ __forceinline__ void add_grad( void * base, float * carry, size_t i, double v,
+                                          double sc )
 {
     if( TALLY == KP_TALLY_FIXED )
         atomicAdd( ( unsigned long long * ) base + i,
                    ( unsigned long long ) __double2ll_rn( __dmul_rn( v, sc ) ) );
     else
-        atomicAdd( ( float * ) base + i, ( float ) v );
+        atomic_add_carry( ( float * ) base, carry, i, ( float ) v );
+}
+
+template< int TALLY >
+__device__ __forceinline__ void add_grad( void * base, size_t i, double v, double sc )
+{
+    add_grad< TALLY >( base, nullptr, i, v, sc );
 }
 
 // Adjoint score of a peel-off contribution: <dL/dimage[pix], (I, Q, U, V)>.
@@ -735,7 +787,7 @@ __device__ __forceinline__ float score( const fwd_params_t & P, int pix, float I
 // plane of d and +z).
 template< int TALLY >
 __device__ __forceinline__ bool tally_escape( const fwd_params_t & P, void * mu_base,
-                                              const packet_t & p, int batch )
+                                              float * carry, const packet_t & p, int batch )
 {
     if( P.n_mu <= 0 ) return false;
     const float fb = floorf( __fmul_rn( __fsub_rn( p.d.z, P.mu_lo ), P.mu_inv_w ) );
@@ -747,10 +799,10 @@ __device__ __forceinline__ bool tally_escape( const fwd_params_t & P, void * mu_
     float q = p.S.q, u = p.S.u;
     phys::rotate( q, u, c2, s2 );
     const size_t i = ( ( size_t ) batch * P.n_mu + bin ) * 4;
-    add_tally< TALLY >( mu_base, i + 0, p.w, P.fx_scale );
-    add_tally< TALLY >( mu_base, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
-    add_tally< TALLY >( mu_base, i + 2, __fmul_rn( p.w, u ), P.fx_scale );
-    add_tally< TALLY >( mu_base, i + 3, __fmul_rn( p.w, p.S.v ), P.fx_scale );
+    add_tally< TALLY >( mu_base, carry, i + 0, p.w, P.fx_scale );
+    add_tally< TALLY >( mu_base, carry, i + 1, __fmul_rn( p.w, q ), P.fx_scale );
+    add_tally< TALLY >( mu_base, carry, i + 2, __fmul_rn( p.w, u ), P.fx_scale );
+    add_tally< TALLY >( mu_base, carry, i + 3, __fmul_rn( p.w, p.S.v ), P.fx_scale );
     return true;
 }
 
@@ -842,6 +894,34 @@ __device__ __forceinline__ bool emit_packet( const fwd_params_t & P, long long p
     p.n_steps = 0;
     set_inv( p );
     return true;
+}
+
+// Packet (pid - pid0) that work index w of a launch of n packets walks:
+// source-major order.  Packet pid starts from source pid % n_src, so the
+// launch takes the packets of one source after another (slot j = 0 ..
+// n_src - 1 holds k = j + m n_src, m = 0, 1, ...), and the packets in flight
+// at any time start from one or two sources and share their part of the
+// mesh in L2 instead of spreading over all of them.  The tallies (int64 sums)
+// and the records (indexed by pid) do not depend on the order.  The
+// identity for one source (and for a packet table, n_src = 1).
+__device__ __forceinline__ long long source_major( long long w, long long n, int n_src )
+{
+    if( n_src <= 1 )
+        return w;
+    const long long q = n / n_src, r = n % n_src;
+    long long j, m;
+    if( w < r * ( q + 1 ) )
+    {
+        j = w / ( q + 1 );
+        m = w % ( q + 1 );
+    }
+    else
+    {
+        const long long v = w - r * ( q + 1 );
+        j = r + v / q;
+        m = v % q;
+    }
+    return j + m * n_src;
 }
 
 // Creates packet `pid` of a single-mesh launch: from the caller's packet

@@ -53,25 +53,48 @@ def slab(n_packets=1_000_000, nx=128, ny=128, nz=64, block=16, tau=10.0, seed=1,
     return mesh, sigma2, cfg
 
 
-def tangential_polarization(img_iquv: np.ndarray) -> float:
+def tangential_polarization(img_iquv: np.ndarray, centres=None) -> float:
     """Intensity-weighted tangential polarization of an image about its centre:
     sum(-Q cos 2phi + U sin 2phi) / sum(I), phi the pixel's position angle
     from the vertical toward the horizontal image axis (positive for the
     centrosymmetric pattern of scattered light).  The image's Stokes frame is
-    e1 = vertical, e2 = -horizontal, hence the sign of the U term."""
+    e1 = vertical, e2 = -horizontal, hence the sign of the U term.  With
+    ``centres`` ([k, 2] (vertical, horizontal) offsets from the image centre
+    in pixels, source_pixels) phi is taken about the nearest of them: the
+    pattern around several sources."""
     n = img_iquv.shape[0]
     c = (np.arange(n) + 0.5) - n / 2
     Y, X = np.meshgrid(c, c, indexing="ij")
+    if centres is not None:
+        cen = np.asarray(centres, np.float64)
+        d2 = (Y[..., None] - cen[:, 0]) ** 2 + (X[..., None] - cen[:, 1]) ** 2
+        near = cen[d2.argmin(-1)]
+        Y, X = Y - near[..., 0], X - near[..., 1]
     phi = np.arctan2(X, Y)
     I, Q, U = (img_iquv[..., k].astype(np.float64) for k in range(3))
     return float((-Q * np.cos(2 * phi) + U * np.sin(2 * phi)).sum() / max(I.sum(), 1e-300))
 
 
-def batch_rel_error(batch_images: np.ndarray) -> tuple[float, float]:
-    """Tangential polarization and its batch-means relative std-error from
-    per-batch coarse images [n_batches, bn, bn, 4]."""
-    p = np.array([tangential_polarization(b) for b in batch_images])
-    tot = tangential_polarization(batch_images.sum(0))
+def source_pixels(cfg, n: int) -> np.ndarray:
+    """Image positions of cfg's point sources on an n x n image of the
+    observer cfg names: [k, 2] (vertical, horizontal) offsets from the image
+    centre in pixels, the projection the peel-off uses (image vertical = the
+    projection of +z, horizontal = vertical x observer direction)."""
+    inc, az = math.radians(cfg.inclination_deg), math.radians(cfg.azimuth_deg)
+    o = np.array([math.sin(inc) * math.cos(az), math.sin(inc) * math.sin(az), math.cos(inc)])
+    ev = np.array([-math.cos(inc) * math.cos(az), -math.cos(inc) * math.sin(az), math.sin(inc)])
+    eh = np.cross(ev, o)
+    r = np.array([s.pos for s in cfg.sources], np.float64) - np.asarray(cfg.image_center)
+    inv_pix = n / (2.0 * cfg.image_half_width)
+    return np.stack([r @ ev * inv_pix, r @ eh * inv_pix], 1)
+
+
+def batch_rel_error(batch_images: np.ndarray, centres=None) -> tuple[float, float]:
+    """Tangential polarization (about ``centres``, else the image centre) and
+    its batch-means relative std-error from per-batch coarse images
+    [n_batches, bn, bn, 4]."""
+    p = np.array([tangential_polarization(b, centres) for b in batch_images])
+    tot = tangential_polarization(batch_images.sum(0), centres)
     err = p.std(ddof=1) / math.sqrt(len(p))
     return tot, (err / abs(tot) if tot != 0 else float("inf"))
 
@@ -185,6 +208,6 @@ def large_amr(n_packets=1_000_000_000, n_root=256, block=16, sigma_ln=1.5, level
     srcs = [Source(SOURCE_POINT, EMIT_ISOTROPIC, tuple(p)) for p in rng.uniform(0.05, 0.95, (n_sources, 3))]
     cfg = TransportConfig(n_packets=n_packets, seed=seed, sources=srcs, phase=PHASE_HG_POL,
                           hg_g=0.6, pol_max=0.5, image_n=image_n, inclination_deg=60.0,
-                          image_center=(0.5, 0.5, 0.5), image_half_width=0.75, image_batch_n=8,
+                          image_center=(0.5, 0.5, 0.5), image_half_width=0.75, image_batch_n=64,
                           n_batches=32, w_min=0.01, fx_shift=30)
     return mesh, sigma2, cfg

@@ -29,10 +29,13 @@ class Tallies:
     """Device output buffers of a transport run (accumulated across calls).
 
     ``n_cells`` sizes the path-length flux tally when ``cfg.flux`` is set
-    (the mesh's cell count; a decomposed rank's own cells).
+    (the mesh's cell count; a decomposed rank's own cells).  In float mode
+    the tallies come with their rounding-error carry (kp_tallies_t::carry),
+    which each solve folds into them at its end; ``carry=False`` leaves plain
+    float atomics.
     """
 
-    def __init__(self, cfg: TransportConfig, device="cuda", n_cells: int = 0):
+    def __init__(self, cfg: TransportConfig, device="cuda", n_cells: int = 0, carry: bool = True):
         dt = torch.int64 if cfg.tally_mode == TALLY_FIXED else torch.float32
         self.cfg = cfg
         self.mu = torch.zeros((cfg.n_batches, max(cfg.n_mu_bins, 1), 4), dtype=dt, device=device)
@@ -46,12 +49,22 @@ class Tallies:
         if cfg.flux and n_cells <= 0:
             raise ValueError("the flux tally needs the mesh's cell count (n_cells)")
         self.flux = torch.zeros(n_cells, dtype=dt, device=device) if cfg.flux else None
+        n_carry = 0
+        if cfg.image_n:
+            n_carry += self.image.numel() + self.image_batch.numel()
+        if cfg.n_mu_bins:
+            n_carry += self.mu.numel()
+        if self.flux is not None:
+            n_carry += self.flux.numel()
+        self.carry = (torch.zeros(max(n_carry, 1), dtype=torch.float32, device=device)
+                      if carry and cfg.tally_mode == TALLY_FLOAT else None)
 
     def zero_(self):
         for t in (self.mu, self.image, self.image_batch, self.counters):
             t.zero_()
-        if self.flux is not None:
-            self.flux.zero_()
+        for t in (self.flux, self.carry):
+            if t is not None:
+                t.zero_()
         if self.records is not None:
             self.records.zero_()
         return self
@@ -64,6 +77,8 @@ class Tallies:
         t.counters = ptr(self.counters)
         t.records = ptr(self.records) if self.records is not None else None
         t.flux = ptr(self.flux) if self.flux is not None else None
+        t.flux_n = self.flux.numel() if self.flux is not None else 0
+        t.carry = ptr(self.carry) if self.carry is not None else None
         return t
 
     def scale(self) -> float:

@@ -441,9 +441,33 @@ static int timage_pixel( const tctx * t, const double * x )
     return ( int ) fy * t->img_n + ( int ) fx;
 }
 
+/* Optional record of every image deposit: its pixel and (I, Q, U, V), in
+ * deposit order, up to `cap` deposits (the count keeps growing past it).  Set
+ * by kpo_set_pixel_sink; process-global, for sequential test use: the exact
+ * sum of a pixel's float deposits bounds the rounding of both tally modes. */
+static int *       s_pix_sink_pix = NULL;
+static float *     s_pix_sink_val = NULL;
+static long long   s_pix_sink_cap = 0;
+static long long * s_pix_sink_n   = NULL;
+
+void kpo_set_pixel_sink( int * pix, float * val, long long cap, long long * n )
+{
+    s_pix_sink_pix = pix; s_pix_sink_val = val; s_pix_sink_cap = cap; s_pix_sink_n = n;
+}
+
 static void tdeposit_pixel( const tctx * t, int pixel, long long pid,
                             float I, float Q, float U, float V )
 {
+    if( s_pix_sink_n )
+    {
+        const long long k = ( * s_pix_sink_n ) ++;
+        if( k < s_pix_sink_cap )
+        {
+            s_pix_sink_pix[ k ] = pixel;
+            s_pix_sink_val[ 4 * k + 0 ] = I; s_pix_sink_val[ 4 * k + 1 ] = Q;
+            s_pix_sink_val[ 4 * k + 2 ] = U; s_pix_sink_val[ 4 * k + 3 ] = V;
+        }
+    }
     const int ix = pixel % t->img_n, iy = pixel / t->img_n;
     const long pix = ( long ) pixel * 4;
     tadd( t->image, pix + 0, I, t->fx_scale );

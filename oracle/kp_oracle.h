@@ -161,6 +161,10 @@ int kpo_adjoint( const kpo_mesh_t * m, const float * sigma2, const int * lookup,
  * |v| to sink[2 i] and 1 to sink[2 i + 1] (2 n_cells doubles); NULL switches
  * it off. */
 void kpo_set_abs_sink( double * sink );
+/* While n is non-null, every image deposit of kpo_transport is recorded:
+ * pix[k] = its pixel, val[4 k .. 4 k + 3] = its (I, Q, U, V), for the first
+ * `cap` deposits; *n counts all of them.  n = NULL switches it off. */
+void kpo_set_pixel_sink( int * pix, float * val, long long cap, long long * n );
 #ifdef __cplusplus
 }
 #endif

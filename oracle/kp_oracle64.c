@@ -31,6 +31,7 @@
 #define kpo_log_exp        kpo_log_exp_f64
 #define kpo_scatter_sample kpo_scatter_sample_f64
 #define kpo_set_abs_sink   kpo_set_abs_sink_f64
+#define kpo_set_pixel_sink kpo_set_pixel_sink_f64
 #define kpo_adjoint        kpo_adjoint_f64
 
 /* kpo_trace calls kpo_trace_ex before defining it */

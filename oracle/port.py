@@ -186,12 +186,16 @@ def lookup_grid(levels, regs, nc_root_blocks):
     return g, n
 
 
-def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, flux=False):
+def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, flux=False,
+              deposits=0):
     """Runs the restated transport for a TransportConfig-like ``cfg``.
 
     ``source_cells``: (ib, cell[3]) per source (point sources), located by
     the caller.  Returns dict of int64 tallies, counters and records; with
-    ``flux`` also the int64 path-length flux tally ([n_cells]).
+    ``flux`` also the int64 path-length flux tally ([n_cells]); with
+    ``deposits`` = cap > 0 also "deposits": (pixel [k] int32, (I, Q, U, V)
+    [k, 4] float32) of the first cap image deposits in deposit order, and
+    "n_deposits", the count of all of them.
     """
     src = (_Source * max(1, len(cfg.sources)))()
     for k, s in enumerate(cfg.sources):
@@ -221,11 +225,25 @@ def transport(tab: Tables, sigma2, lookup, lookup_n, cfg, source_cells, flux=Fal
         out["flux"] = np.zeros(tab.n_blocks * tab.cells_per_block, np.int64)
     L.kpo_transport.argtypes = [ctypes.c_void_p] * 11
     p = lambda a: ctypes.c_void_p(a.ctypes.data)
-    st = L.kpo_transport(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
-                         p(out["mu"]), p(out["image"]), p(out["image_batch"]), p(out["counters"]),
-                         p(rec), p(out["flux"]) if flux else None)
+    if deposits:
+        d_pix, d_val = np.zeros(deposits, np.int32), np.zeros((deposits, 4), np.float32)
+        d_n = np.zeros(1, np.int64)
+        L.kpo_set_pixel_sink.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
+                                         ctypes.c_void_p]
+        L.kpo_set_pixel_sink(p(d_pix), p(d_val), deposits, p(d_n))
+    try:
+        st = L.kpo_transport(ctypes.byref(s), p(sigma2), p(lookup), p(lk_n), ctypes.byref(c),
+                             p(out["mu"]), p(out["image"]), p(out["image_batch"]),
+                             p(out["counters"]), p(rec), p(out["flux"]) if flux else None)
+    finally:
+        if deposits:
+            L.kpo_set_pixel_sink(None, None, 0, None)
     if st != 0:
         raise RuntimeError(f"kpo_transport failed ({st})")
+    if deposits:
+        k = int(min(d_n[0], deposits))
+        out["deposits"] = (d_pix[:k], d_val[:k])
+        out["n_deposits"] = int(d_n[0])
     out["records"] = rec[:cfg.n_record]
     return out
 

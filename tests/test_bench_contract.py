@@ -69,3 +69,38 @@ def test_reference_arm_does_not_load_the_product():
     xf0, _, _, _ = mesh.geometry(8)
     want = np.concatenate([sig.ravel().astype(np.float64), xf0.ravel(), [ib[0]], cell[0]])
     np.testing.assert_array_equal(got, want)
+
+
+def test_tangential_polarization_about_sources():
+    """A centrosymmetric pattern drawn around two source positions reads its
+    own degree about them, and about the image centre much less."""
+    import numpy as np
+    from kratos_polrad_b200 import scenes
+    n, p = 64, 0.1
+    cen = np.array([[-10.0, 12.0], [9.0, -14.0]])
+    c = (np.arange(n) + 0.5) - n / 2
+    Y, X = np.meshgrid(c, c, indexing="ij")
+    d2 = (Y[..., None] - cen[:, 0]) ** 2 + (X[..., None] - cen[:, 1]) ** 2
+    near = cen[d2.argmin(-1)]
+    phi = np.arctan2(X - near[..., 1], Y - near[..., 0])
+    img = np.zeros((n, n, 4))
+    img[..., 0] = 1.0
+    img[..., 1] = -p * np.cos(2 * phi)
+    img[..., 2] = p * np.sin(2 * phi)
+    assert abs(scenes.tangential_polarization(img, cen) - p) < 1e-12
+    assert abs(scenes.tangential_polarization(img)) < 0.5 * p
+
+
+def test_source_pixels_match_the_peel_off_projection():
+    """A source at the image centre sits at offset 0; one displaced along the
+    image's vertical axis (+z at inclination 90) moves up by its offset over
+    the pixel size."""
+    import numpy as np
+    from kratos_polrad_b200 import scenes
+    from kratos_polrad_b200.config import SOURCE_POINT, Source, TransportConfig
+    cfg = TransportConfig(n_packets=1, sources=[Source(SOURCE_POINT, 0, (0.5, 0.5, 0.5)),
+                                               Source(SOURCE_POINT, 0, (0.5, 0.5, 0.75))],
+                          inclination_deg=90.0, image_center=(0.5, 0.5, 0.5), image_half_width=0.5)
+    px = scenes.source_pixels(cfg, 64)
+    np.testing.assert_allclose(px[0], [0, 0], atol=1e-12)
+    np.testing.assert_allclose(px[1], [0.25 * 64, 0], atol=1e-9)

@@ -59,7 +59,9 @@ def test_noalloc_matches_forward_on_two_calls(name):
 @pytest.mark.gpu
 def test_noalloc_float_tallies_within_rounding():
     """Float tallies: the inline peel-off rays add into the image in another
-    order than the queued ones, so the two agree within float rounding."""
+    order than the queued ones.  Both carry their rounding errors
+    (kp_tallies_t::carry, the caller's memory: the fold after the walk is
+    the only other launch), so each pixel agrees within 1e-6 of its I."""
     import dataclasses
     import torch
     from kratos_polrad_b200.transport import TALLY_FLOAT
@@ -71,9 +73,11 @@ def test_noalloc_float_tallies_within_rounding():
     _noalloc(mesh, cfg, tal, torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert mesh.status() == 0
-    a, b = tal.image.cpu().numpy(), ref.image.cpu().numpy()
-    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(b).max())
-    assert abs(a[..., 0].sum() - b[..., 0].sum()) <= 1e-6 * abs(b[..., 0].sum())
+    a, b = tal.image.cpu().numpy().astype(np.float64), ref.image.cpu().numpy().astype(np.float64)
+    lit = b[..., 0] > 0
+    assert (a[~lit] == 0).all()
+    assert (np.abs(a - b)[lit] / b[..., 0][lit][:, None]).max() <= 1e-6
+    assert abs(a[..., 0].sum() - b[..., 0].sum()) <= 1e-7 * abs(b[..., 0].sum())
     assert torch.equal(tal.counters, ref.counters)
 
 

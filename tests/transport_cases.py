@@ -94,7 +94,7 @@ def to_device(t):
     return dataclasses.replace(t, packets=packet_table(t.packets))
 
 
-def run_oracle(mesh, sig, t):
+def run_oracle(mesh, sig, t, deposits=0):
     tab = port.Tables.from_mesh(mesh, 8)
     lev, reg = mesh.blocks()
     root = [mesh.nc[a] and int(round((mesh.x_max[a] - mesh.x_min[a]) /
@@ -108,7 +108,7 @@ def run_oracle(mesh, sig, t):
             cells.append((ib[0], cell[0]))
         else:
             cells.append((0, (0, 0, 0)))
-    return port.transport(tab, sig, grid, n, t, cells)
+    return port.transport(tab, sig, grid, n, t, cells, deposits=deposits)
 
 
 def oracle_inputs(mesh, t):
