@@ -372,8 +372,8 @@ def _timed(fn):
     return out, e0.elapsed_time(e1)
 
 
-def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=600_000_000, n_batch=20, n_dirs=8,
-                    n_cells=16, n_cell_check=50_000_000):
+def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=1_200_000_000, n_batch=20, n_dirs=8,
+                    n_cells=16, n_cell_check=50_000_000, h=0.1):
     """Paired batch-means comparison of the path-replay gradient with
     common-random-number central differences of the same estimator.
 
@@ -383,7 +383,10 @@ def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=600_000_000, n_batch=20,
     adjoint and the differences use the same packets.
 
     Blob directions (the 2% bar): Gaussian density blobs of radius 0.08 box
-    (both coefficients scaled by 1 +- 0.05 phi, albedo unchanged).  Their
+    (both coefficients scaled by 1 +- h phi, albedo unchanged; h = 0.1: the
+    differences' noise comes from the packets whose paths the perturbation
+    changes, a fraction that grows like h, so their standard error falls
+    like h^-1/2 while the central difference's bias grows like h^2).  Their
     centres are the points of a 16^3 grid over the box with the largest
     |dF/d blob| (at least 0.15 box apart), that derivative taken from a
     gradient of other packets (ids from 5e9), so that the choice does not
@@ -451,7 +454,6 @@ def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=600_000_000, n_batch=20,
 
     fd_b = np.zeros_like(adj_b)
     fd_c = np.zeros_like(adj_c)
-    h = 0.05
     for k, phi in enumerate(phis):
         sp = (sig * (1 + h * phi)[:, None]).astype(np.float32)
         sm = (sig * (1 - h * phi)[:, None]).astype(np.float32)
@@ -472,7 +474,7 @@ def _gradient_check(mesh, sig, cfg, g_img, rng, n_check=600_000_000, n_batch=20,
     dc = adj_c - fd_c
     zc = dc.mean(0) / (dc.std(0, ddof=1) / sq)
     ok = (rel <= 0.02) & (rel_se <= 0.01)
-    return {"packets": n_check, "batches": n_batch,
+    return {"packets": n_check, "batches": n_batch, "h": h,
             "blob_directions": {"n": n_dirs, "fd": [float(v) for v in fd_mean],
                                 "fd_rel_std_err": [round(float(v), 5) for v in rel_se],
                                 "adjoint": [float(v) for v in adj_mean],
@@ -858,6 +860,10 @@ def run_large(args):
                                     "sigma_MB": sig.nbytes / 1e6, "image": cfg.image_n},
             "forward_ms": t_fwd, "counts": c, "pol_tangential": p_tan, "pol_rel_std_err": rel,
             "pol_tangential_about_sources": p_loc, "pol_tangential_about_sources_rel_std_err": rel_loc,
+            # the std-error falls like packets^-1/2: packets (and forward time at
+            # this rate) for 1% on the statistic about the sources
+            "pol_packets_for_1pct": n_pk * (rel_loc / 0.01) ** 2,
+            "pol_forward_s_for_1pct": t_fwd / 1e3 * (rel_loc / 0.01) ** 2,
             "pol_integrated": p_int, "pol_integrated_rel_std_err": rel_int,
             "pol_mean_degree_coarse": p_deg, "pol_mean_degree_rel_std_err": rel_deg,
             "adjoint_ms": t_adj, "adjoint_cost_vs_forward": t_adj / t_fwd,

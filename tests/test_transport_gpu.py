@@ -87,7 +87,7 @@ def test_float_tally_mode_within_1e6_of_exact():
     assert ref["n_deposits"] == len(ref["deposits"][0]) > 10000
     ex, cnt = _exact_image(t, ref["deposits"])
     I = ex[..., 0]
-    assert (I > 0).sum() > 500 and cnt.max() > 1000
+    assert (I > 0).sum() > 200 and cnt.max() > 1000
 
     img_fx = fx.image.cpu().numpy() * 2.0 ** -t.fx_shift
     assert (np.abs(img_fx - ex) <= cnt[..., None] * 2.0 ** -(t.fx_shift + 1) + 1e-15).all()
