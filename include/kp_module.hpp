@@ -26,6 +26,12 @@
 // path-length flux (rad_t::flx; the walk deposits into field 0 of the n_hv
 // fields, as photon.h:81 does).
 //
+// A packet that uses up its step_max segments in a cycle ends there, as in
+// the reference (photon.h:122-123), unless the module's comm_mode() is
+// keep_pool: then it waits in the module's pool and the next cycle resumes
+// it before the cycle's new packets (kp_transport_forward_resume); drain()
+// runs cycles without new packets until the pool is empty.
+//
 // Host C++17; the generator header needs nvcc.  Every failure throws
 // std::runtime_error (kp::api), as the reference's cuda_api does.
 #ifndef KP_MODULE_HPP
@@ -33,12 +39,20 @@
 
 #include "kp_transport.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <functional>
 #include <string>
 #include <vector>
+
+namespace kp::particle
+{
+// Whether a cycle's unfinished packets stay in the pool (particle::
+// comm_mode_t, modules/particle/types/driver_base.h:12).
+enum comm_mode_t : int { refresh_pool, keep_pool };
+}   // namespace kp::particle
 
 namespace kp::particle::radiation
 {
@@ -100,6 +114,19 @@ public:
     // keeps the default set (the sources()).
     virtual void enroll( generator_t gen = nullptr ) { gen_ = std::move( gen ); }
 
+    // particle::base_t::comm_mode (modules/particle/driver.cpp:67-69):
+    // refresh_pool, the reference's default, ends a packet that uses up its
+    // step_max segments in a cycle (photon.h:122-123).  A module that returns
+    // keep_pool keeps such packets in its pool instead, as the reference's
+    // pool keeps its to_keep particles (types/particle_pool.h:191-248): the
+    // next cycle resumes them (kp_transport_forward_resume) before its new
+    // packets, each cycle gives every packet step_max more segments, and a
+    // packet ends for good after pool_max_steps() segments in all.
+    virtual comm_mode_t comm_mode(  ) const { return refresh_pool; }
+    long long & pool_max_steps(  ) { return pool_max_; }
+    // Packets waiting in the pool for the next cycle (keep_pool).
+    long long pool_size(  ) const { return n_pool_; }
+
     // particle::base_t::init: binds the mesh and allocates the packet table
     // (with a generator) and the tallies on the current device, zeroed.
     virtual void init( mesh_t & mesh, stream_t s = nullptr )
@@ -157,16 +184,34 @@ public:
             gen_( table_, n_par_, c.packet_offset, s );
             c.packets = table_;
         }
-        kp_tallies_t t {  };
-        t.mu = mu_;
-        t.image = image_;
-        t.image_batch = image_batch_;
-        t.counters = counters_;
-        t.flux = flux_;
-        t.carry = carry_;
-        t.flux_n = n_cells_;
-        transport::forward( * mesh_, c, t, s );
+        const kp_tallies_t t = tallies(  );
+        if( comm_mode(  ) == keep_pool )
+            integrate_pool( c, t, s );
+        else
+            transport::forward( * mesh_, c, t, s );
         done_ += n_par_;
+    }
+
+    // keep_pool: cycles without new packets until the pool is empty, so that
+    // every packet of the run has ended (at most pool_max_steps() / step_max
+    // + 1 cycles).  Nothing to do in refresh_pool mode.
+    virtual void drain( stream_t s = nullptr )
+    {
+        if( ! mesh_ || comm_mode(  ) != keep_pool )
+            return;
+        const long long max_cycles = pool_max_ / std::max( par_.step_max, 1 ) + 2;
+        for( long long k = 0; n_pool_ > 0; ++ k )
+        {
+            if( k >= max_cycles )
+                throw std::runtime_error( "kratos_polrad_b200: the packet pool does not drain" );
+            kp_transport_cfg_t c = cfg_;
+            c.n_packets = 0;
+            c.packet_offset = cfg_.packet_offset + done_;
+            c.n_sources = 0;
+            c.sources = nullptr;
+            c.packets = nullptr;
+            integrate_pool( c, tallies(  ), s );
+        }
     }
 
     // particle::base_t::step: n_cycle_stp cycles, then the stream is synced.
@@ -265,10 +310,13 @@ public:
     virtual void finalize(  ) noexcept
     {
         for( void * p : { flux_, ( void * ) counters_, mu_, image_, image_batch_,
-                          ( void * ) table_, ( void * ) carry_ } )
+                          ( void * ) table_, ( void * ) carry_, ( void * ) pool_in_,
+                          ( void * ) pool_out_, ( void * ) pool_count_ } )
             if( p ) kp_free( p );
         flux_ = nullptr; counters_ = nullptr; mu_ = image_ = image_batch_ = nullptr;
         table_ = nullptr; carry_ = nullptr;
+        pool_in_ = pool_out_ = nullptr; pool_count_ = nullptr;
+        cap_in_ = cap_out_ = n_pool_ = 0;
         mesh_ = nullptr;
     }
 
@@ -287,6 +335,58 @@ public:
     long long n_cells(  ) const { return n_cells_; }
 
 private:
+    kp_tallies_t tallies(  ) const
+    {
+        kp_tallies_t t {  };
+        t.mu = mu_;
+        t.image = image_;
+        t.image_batch = image_batch_;
+        t.counters = counters_;
+        t.flux = flux_;
+        t.carry = carry_;
+        t.flux_n = n_cells_;
+        return t;
+    }
+
+    // One keep_pool cycle: resumes the pool, emits c's packets, and keeps the
+    // packets that used up step_max for the next cycle.  Reads the pool's new
+    // size back (a sync, as the reference's pool_t::regulate reads n_mv).
+    void integrate_pool( kp_transport_cfg_t c, const kp_tallies_t & t, stream_t s )
+    {
+        const long long need = std::max< long long >( n_pool_ + c.n_packets, 1 );
+        if( cap_out_ < need )
+        {   // the out queue holds every packet of the cycle
+            if( pool_out_ ) api( kp_free( pool_out_ ) );
+            pool_out_ = nullptr;
+            cap_out_ = 0;
+            void * p = nullptr;
+            api( kp_malloc( & p, sizeof( kp_packet_state_t ) * ( size_t ) need ) );
+            pool_out_ = static_cast< kp_packet_state_t * >( p );
+            cap_out_ = need;
+        }
+        if( ! pool_count_ )
+            pool_count_ = static_cast< unsigned long long * >(
+                alloc( sizeof( unsigned long long ), s ) );
+        api( kp_memset_async( pool_count_, 0, sizeof( unsigned long long ), s ) );
+        c.max_steps = pool_max_;
+        kp_resume_t r {  };
+        r.in = pool_in_;
+        r.n_in = n_pool_;
+        r.out = pool_out_;
+        r.cap_out = cap_out_;
+        r.out_count = pool_count_;
+        r.step_budget = std::max( par_.step_max, 1 );
+        transport::forward_resume( * mesh_, c, r, t, s );
+        unsigned long long n = 0;
+        api( kp_stream_sync( s ) );
+        api( kp_memcpy( & n, pool_count_, sizeof( n ) ) );
+        if( ( long long ) n > cap_out_ )
+            throw std::runtime_error( "kratos_polrad_b200: packet pool overflow" );
+        std::swap( pool_in_, pool_out_ );
+        std::swap( cap_in_, cap_out_ );
+        n_pool_ = ( long long ) n;
+    }
+
     static void * alloc( size_t bytes, stream_t s )
     {
         void * p = nullptr;
@@ -309,6 +409,13 @@ private:
     unsigned long long *       counters_ = nullptr;
     kp_packet_init_t *         table_ = nullptr;
     float *                    carry_ = nullptr;
+    // keep_pool: the packets carried to the next cycle (in), the queue this
+    // cycle suspends into (out), their capacities and the device count
+    kp_packet_state_t *        pool_in_ = nullptr;
+    kp_packet_state_t *        pool_out_ = nullptr;
+    unsigned long long *       pool_count_ = nullptr;
+    long long                  cap_in_ = 0, cap_out_ = 0, n_pool_ = 0;
+    long long                  pool_max_ = 1ll << 24;
 };
 
 }   // namespace kp::particle::radiation

@@ -386,6 +386,63 @@ typedef struct kp_tallies
 int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
                           const kp_tallies_t * tallies, void * stream );
 
+/* Packet state carried between calls, 128 bytes in device memory: a walk
+ * that a step budget suspended (kp_transport_forward_resume), or one handed
+ * to another rank (kp_transport_forward_dd's walk records have this
+ * layout).  Everything the walk needs to go on bit for bit. */
+typedef struct kp_packet_state
+{
+    double   x[ 3 ];
+    float    d[ 3 ];
+    float    e1[ 3 ];        /* Stokes reference vector                       */
+    float    stokes[ 3 ];    /* q, u, v relative to I                         */
+    float    w;              /* weight                                        */
+    float    tau;            /* optical depth left to the next interaction    */
+    int      ib, cell[ 3 ];
+    int      n_scatter, n_steps;
+    uint32_t stream_id;      /* RNG key word 2 (kp_transport_cfg_t::stream_id) */
+    uint32_t pid_lo, pid_hi; /* global packet id                              */
+    uint32_t rng_draws;      /* Philox blocks consumed                        */
+    int      batch;          /* batch-means index (pid % n_batches)           */
+    int      pad[ 4 ];
+} kp_packet_state_t;
+
+/* Step budget and packet queues of a resumable call. */
+typedef struct kp_resume
+{
+    const kp_packet_state_t * in;   /* device [n_in]: packets an earlier call
+                                       suspended, resumed before cfg's new ones */
+    long long n_in;
+    kp_packet_state_t * out;        /* device [cap_out]: packets this call
+                                       suspends (must not overlap `in`)         */
+    long long cap_out;
+    unsigned long long * out_count; /* device: packets written to out, added to
+                                       (zero it first); a count above cap_out
+                                       means lost packets (kp_mesh_status:
+                                       queue overflow)                          */
+    int step_budget;                /* walk segments a packet may take in this
+                                       call (>= 1)                              */
+} kp_resume_t;
+
+/* kp_transport_forward with a per-call step budget, as the reference walks
+ * each packet for at most `step` segments per cycle (photon::cart_t::proc,
+ * modules/particle/radiation/photon.h:104-125).  The reference then removes
+ * a packet whose budget ran out (todo = to_rm, photon.h:122-123); here it is
+ * kept, as the pool keeps unfinished particles across cycles (types/
+ * particle_pool.h:191-248, evolve/integrator.h:80-106): its whole state goes
+ * to rs->out, and a later call that passes it in rs->in continues its walk.
+ * A call first resumes rs->in, then emits cfg's n_packets new packets (none
+ * needed: n_packets may be 0 without sources).  cfg->max_steps still ends a
+ * packet for good.  In fixed point, calls that carry every packet to its
+ * end give the tallies, counters and records of one kp_transport_forward
+ * with the same cfg, bit for bit (records: packet_offset and n_record as in
+ * that solve).  The reference's behaviour, a budget that ends packets, is
+ * kp_transport_forward with max_steps = the budget.  Out-of-place queues
+ * (swap in and out between calls); worst case cap_out = n_in + n_packets. */
+int kp_transport_forward_resume( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                 const kp_resume_t * rs, const kp_tallies_t * tallies,
+                                 void * stream );
+
 /* Upper bound on the mesh's peel-off queue (device memory, 64 B per ray;
  * default 2^27 rays = 8.6 GB).  With an image, kp_transport_forward queues
  * the peel-off rays of its packets and marches them in a second kernel; the

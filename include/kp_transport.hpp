@@ -291,6 +291,13 @@ struct transport
         api( kp_trace_sph( m.get(  ), precision, n, x, x_car, dir, cell, ib, proper, step, todo,
                            flux_mode, fx_shift, flux, s ) );
     }
+    // A call with a step budget (see kp_resume_t): resumes r.in, emits c's
+    // packets, suspends into r.out the packets that use up the budget.
+    static void forward_resume( mesh_t & m, const kp_transport_cfg_t & c, const kp_resume_t & r,
+                                const kp_tallies_t & t, stream_t s = nullptr )
+    {
+        api( kp_transport_forward_resume( m.get(  ), & c, & r, & t, s ) );
+    }
     // One round of a decomposed solve on this rank (see kp_dd_round_t).
     static void forward_dd( mesh_t & m, const kp_transport_cfg_t & c, const kp_dd_round_t & r,
                             const kp_tallies_t & t, stream_t s = nullptr )

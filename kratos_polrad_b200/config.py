@@ -99,6 +99,16 @@ PACKET_INIT_DTYPE = np.dtype([("x", "<f8", 3), ("d", "<f4", 3), ("w", "<f4"),
                               ("pad", "<i4")])
 assert PACKET_INIT_DTYPE.itemsize == 64
 
+# numpy view of kp_packet_state_t (128 bytes): a packet carried between calls
+# (suspended by a step budget, or a decomposed round's migrating walk)
+PACKET_STATE_DTYPE = np.dtype([("x", "<f8", 3), ("d", "<f4", 3), ("e1", "<f4", 3),
+                               ("stokes", "<f4", 3), ("w", "<f4"), ("tau", "<f4"),
+                               ("ib", "<i4"), ("cell", "<i4", 3), ("n_scatter", "<i4"),
+                               ("n_steps", "<i4"), ("stream_id", "<u4"), ("pid_lo", "<u4"),
+                               ("pid_hi", "<u4"), ("rng_draws", "<u4"), ("batch", "<i4"),
+                               ("pad", "<i4", 4)])
+assert PACKET_STATE_DTYPE.itemsize == 128
+
 
 @dataclass
 class Source:

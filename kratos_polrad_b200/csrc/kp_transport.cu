@@ -67,14 +67,24 @@ namespace cg = cooperative_groups;
 // its `proper`; w / volume of the walk's block waits in shared memory (set
 // at emission, interactions and block hand-offs), so a segment adds one
 // multiply and one atomic.
+// RESUME (not with DD or TAPE): work items are first the packets an earlier
+// call suspended (P.rs_in), then the call's new packets; a packet that has
+// walked P.rs_budget segments in this launch (and is below max_steps) is
+// written whole to P.rs_out and left for a later call instead of ending.
+// Its arithmetic is that of an uninterrupted walk: the face cache and the
+// inverse direction are rebuilt bit for bit from the stored state.
 template< int TALLY, int NT, bool DD = false, bool DEFER = false, bool TAPE = false,
-          bool FLUX = false >
+          bool FLUX = false, bool RESUME = false >
 __global__ void __launch_bounds__( NT, KP_FWD_RESIDENT / NT )
 k_forward( const __grid_constant__ fwd_params_t P )
 {
+    static_assert( ! ( RESUME && ( DD || TAPE ) ), "RESUME runs without DD and TAPE" );
     __shared__ park_t< NT > sp;
     __shared__ dir_park_t< NT > sd;
     __shared__ cold_park_t< NT > sc;
+    // RESUME: the lane's packet stops (suspends or, at max_steps, ends) when
+    // its n_steps reaches this
+    __shared__ int s_stop[ RESUME ? NT : 1 ];
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     if( threadIdx.x < KP_NCOUNTERS ) sp.cnt[ threadIdx.x ] = 0;
@@ -196,8 +206,50 @@ k_forward( const __grid_constant__ fwd_params_t P )
         }
     };
 
+    // A whole walk (dd_walk_t) becomes the lane's packet: one arriving from
+    // another rank (DD), or one an earlier call suspended (RESUME).
+    auto load_walk = [ & ]( const dd_walk_t & o )
+    {
+        const int t = threadIdx.x;
+        for( int a = 0; a < 3; ++ a ) { p.x[ a ] = o.x[ a ]; p.c[ a ] = o.c[ a ]; }
+        p.d = phys::v3 { o.d[ 0 ], o.d[ 1 ], o.d[ 2 ] };
+        p.e1 = phys::v3 { o.e1[ 0 ], o.e1[ 1 ], o.e1[ 2 ] };
+        p.S = phys::stokes_t { o.S[ 0 ], o.S[ 1 ], o.S[ 2 ] };
+        p.w = o.w; p.tau = o.tau; p.b = o.b;
+        p.n_scat = o.n_scat; p.n_steps = o.n_steps;
+        p.rng = phys::rng_t { P.seed, o.k1, o.pid_lo, o.pid_hi, o.draw };
+        sc.batch[ t ] = o.batch;
+        set_inv( p );
+        store_cold( sc, p );
+        set_wv( p.w, p.b );
+        faces_all( P.m, p.b, p.c, p.d, fx );
+    };
+    // The lane's whole packet (its cold state loaded) into a walk record.
+    auto store_walk = [ & ]( dd_walk_t & o )
+    {
+        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
+        o.d[ 0 ] = p.d.x; o.d[ 1 ] = p.d.y; o.d[ 2 ] = p.d.z;
+        o.e1[ 0 ] = p.e1.x; o.e1[ 1 ] = p.e1.y; o.e1[ 2 ] = p.e1.z;
+        o.S[ 0 ] = p.S.q; o.S[ 1 ] = p.S.u; o.S[ 2 ] = p.S.v;
+        o.w = p.w; o.tau = p.tau; o.b = p.b;
+        o.n_scat = p.n_scat; o.n_steps = p.n_steps;
+        o.k1 = p.rng.k1; o.pid_lo = p.rng.pid_lo; o.pid_hi = p.rng.pid_hi;
+        o.draw = p.rng.draw; o.batch = sc.batch[ threadIdx.x ];
+    };
+    // RESUME: the packet (cold state loaded) leaves this launch unfinished.
+    auto suspend = [ & ](  )
+    {
+        const unsigned long long k = atomicAdd( P.rs_count, 1ull );
+        if( k < ( unsigned long long ) P.rs_cap )
+            store_walk( P.rs_out[ k ] );
+        else
+            atomicOr( P.m.status, ST_QUEUE_FULL );
+        phase = PH_EMIT;
+    };
+
     // After the active ray crossed a face (or stopped): the end of a peel-off
-    // ray (deposit, walk resumes) or of the packet's walk (escape, step cap).
+    // ray (deposit, walk resumes) or of the packet's walk (escape, step cap,
+    // or, RESUME, the end of this launch's step budget).
     // Shared by the segment phase and the hand-off phase.
     auto after_crossing = [ & ]( bool peel_cut, bool left, bool lost )
     {
@@ -253,9 +305,14 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     count( sp, KP_CNT_DEPOSITS );
             }
         }
-        else if( p.n_steps >= P.max_steps )
+        else if( p.n_steps >= ( RESUME ? ( long long ) s_stop[ threadIdx.x ] : P.max_steps ) )
         {
             load_cold( sc, p, P.seed );
+            if( RESUME && p.n_steps < P.max_steps )
+            {
+                suspend(  );
+                return;
+            }
             end = PK_STEP_CAP;
         }
         if( end )
@@ -346,15 +403,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                         {
                             load_cold( sc, p, P.seed );
                             P.dd_out_walk_rank[ k ] = r;
-                            dd_walk_t & o = P.dd_out_walk[ k ];
-                            for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
-                            o.d[ 0 ] = p.d.x; o.d[ 1 ] = p.d.y; o.d[ 2 ] = p.d.z;
-                            o.e1[ 0 ] = p.e1.x; o.e1[ 1 ] = p.e1.y; o.e1[ 2 ] = p.e1.z;
-                            o.S[ 0 ] = p.S.q; o.S[ 1 ] = p.S.u; o.S[ 2 ] = p.S.v;
-                            o.w = p.w; o.tau = p.tau; o.b = p.b;
-                            o.n_scat = p.n_scat; o.n_steps = p.n_steps;
-                            o.k1 = p.rng.k1; o.pid_lo = p.rng.pid_lo; o.pid_hi = p.rng.pid_hi;
-                            o.draw = p.rng.draw; o.batch = sc.batch[ t ];
+                            store_walk( P.dd_out_walk[ k ] );
                         }
                         else
                             atomicOr( P.m.status, ST_QUEUE_FULL );
@@ -394,19 +443,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 const int t = threadIdx.x;
                 if( idx < nw )
                 {   // a walk arriving from another rank
-                    const dd_walk_t & o = P.dd_in_walk[ idx ];
-                    for( int a = 0; a < 3; ++ a ) { p.x[ a ] = o.x[ a ]; p.c[ a ] = o.c[ a ]; }
-                    p.d = phys::v3 { o.d[ 0 ], o.d[ 1 ], o.d[ 2 ] };
-                    p.e1 = phys::v3 { o.e1[ 0 ], o.e1[ 1 ], o.e1[ 2 ] };
-                    p.S = phys::stokes_t { o.S[ 0 ], o.S[ 1 ], o.S[ 2 ] };
-                    p.w = o.w; p.tau = o.tau; p.b = o.b;
-                    p.n_scat = o.n_scat; p.n_steps = o.n_steps;
-                    p.rng = phys::rng_t { P.seed, o.k1, o.pid_lo, o.pid_hi, o.draw };
-                    sc.batch[ t ] = o.batch;
-                    set_inv( p );
-                    store_cold( sc, p );
-                    set_wv( p.w, p.b );
-                    faces_all( P.m, p.b, p.c, p.d, fx );
+                    load_walk( P.dd_in_walk[ idx ] );
                     peel = false; solo = false;
                     phase = PH_SEGMENT;
                     continue;
@@ -438,10 +475,25 @@ k_forward( const __grid_constant__ fwd_params_t P )
                           : ( int ) ( pid % P.dd_ranks ) != P.dd_rank )
                     continue;
             }
-            else if( idx >= ( unsigned long long ) P.n_packets )
+            else
             {
-                phase = PH_DONE;
-                continue;
+                if constexpr( RESUME )
+                {
+                    if( idx < ( unsigned long long ) P.rs_n_in )
+                    {   // a packet suspended by an earlier call goes on
+                        load_walk( P.rs_in[ idx ] );
+                        s_stop[ threadIdx.x ] = ( int ) min( P.max_steps,
+                                                             ( long long ) p.n_steps + P.rs_budget );
+                        phase = PH_SEGMENT;
+                        continue;
+                    }
+                    idx -= ( unsigned long long ) P.rs_n_in;
+                }
+                if( idx >= ( unsigned long long ) P.n_packets )
+                {
+                    phase = PH_DONE;
+                    continue;
+                }
             }
             bool ok;
             float peel_I = 0.0f;          // emission's intensity toward the observer
@@ -505,15 +557,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
                     if( k < ( unsigned long long ) P.dd_cap_walk )
                     {
                         P.dd_out_walk_rank[ k ] = r;
-                        dd_walk_t & o = P.dd_out_walk[ k ];
-                        for( int a = 0; a < 3; ++ a ) { o.x[ a ] = p.x[ a ]; o.c[ a ] = p.c[ a ]; }
-                        o.d[ 0 ] = p.d.x; o.d[ 1 ] = p.d.y; o.d[ 2 ] = p.d.z;
-                        o.e1[ 0 ] = p.e1.x; o.e1[ 1 ] = p.e1.y; o.e1[ 2 ] = p.e1.z;
-                        o.S[ 0 ] = p.S.q; o.S[ 1 ] = p.S.u; o.S[ 2 ] = p.S.v;
-                        o.w = p.w; o.tau = p.tau; o.b = p.b;
-                        o.n_scat = p.n_scat; o.n_steps = p.n_steps;
-                        o.k1 = p.rng.k1; o.pid_lo = p.rng.pid_lo; o.pid_hi = p.rng.pid_hi;
-                        o.draw = p.rng.draw; o.batch = sc.batch[ threadIdx.x ];
+                        store_walk( P.dd_out_walk[ k ] );
                     }
                     else
                         atomicOr( P.m.status, ST_QUEUE_FULL );
@@ -553,6 +597,8 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 faces_all( P.m, p.b, p.c, p.d, fx );
             store_cold( sc, p );
             set_wv( p.w, p.b );
+            if constexpr( RESUME )
+                s_stop[ threadIdx.x ] = ( int ) min( P.max_steps, ( long long ) P.rs_budget );
             continue;
         }
 
@@ -623,6 +669,8 @@ k_forward( const __grid_constant__ fwd_params_t P )
                 count( sp, end == PK_ABSORBED ? KP_CNT_ABSORBED : KP_CNT_CAPPED );
                 phase = PH_EMIT;
             }
+            else if( RESUME && p.n_steps >= s_stop[ threadIdx.x ] )
+                suspend(  );             // the budget ran out with this segment
             else
                 phase = PH_SEGMENT;
             if( phase == PH_SEGMENT )
@@ -1046,6 +1094,7 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     P.counters = t.counters;
     P.records = t.records;
     P.n_record = c.n_record;
+    P.rec_pid0 = c.packet_offset;
     P.flux = t.flux;
     P.flux_scale = std::ldexp( 1.0, c.flux_fx_shift > 0 ? c.flux_fx_shift : c.fx_shift );
     const carry_fold_t f = carry_layout( c, t );
@@ -1136,7 +1185,8 @@ void make_source( kp_mesh_t * mesh, const kp_source_t & s, src_dev_t & d )
 void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
                       const kp_tallies_t & t, fwd_params_t & P )
 {
-    if( c.packets == nullptr )
+    const bool emits = c.packets == nullptr && c.n_packets > 0;
+    if( emits )
         require( c.n_sources >= 1 && c.n_sources <= MAX_SOURCES && c.sources,
                  "need 1..KP_MAX_SOURCES sources", KP_ERR_CAPACITY );
     fill_common_params( c, t, P );
@@ -1144,8 +1194,9 @@ void make_fwd_params( kp_mesh_t * mesh, const kp_transport_cfg_t & c,
     P.m = mesh->view(  );
     P.pk_table = c.packets;
     P.pk_pid0 = c.packet_offset;
-    P.n_src = c.packets ? 1 : c.n_sources;        // P.src[ 0 ] unused with a table
-    if( c.packets == nullptr )
+    // P.src[ 0 ] is unused with a table or without new packets
+    P.n_src = emits ? c.n_sources : 1;
+    if( emits )
         for( int k = 0; k < c.n_sources; ++ k )
             make_source( mesh, c.sources[ k ], P.src[ k ] );
     for( int a = 0; a < 3; ++ a )
@@ -1161,16 +1212,16 @@ int persistent_grid( const void * kernel, int threads )
     return n_sm * std::max( per_sm, 1 );
 }
 
-template< int TALLY, int NT, bool FLUX >
+template< int TALLY, int NT, bool FLUX, bool RESUME = false >
 void launch_forward_k( const fwd_params_t & P, cudaStream_t s, int grid_pct )
 {
-    const void * k = ( const void * ) k_forward< TALLY, NT, false, false, false, FLUX >;
+    const void * k = ( const void * ) k_forward< TALLY, NT, false, false, false, FLUX, RESUME >;
     long long grid = persistent_grid( k, NT );
     grid = std::max< long long >( 1, grid * grid_pct / 100 );
-    grid = std::min< long long >( grid, ( P.n_packets + NT - 1 ) / NT );
+    grid = std::min< long long >( grid, ( P.n_packets + P.rs_n_in + NT - 1 ) / NT );
     KP_CUDA( cudaMemsetAsync( P.work, 0, sizeof( unsigned long long ), s ) );
     // whole warps only: the scheduler ballots over full warps
-    k_forward< TALLY, NT, false, false, false, FLUX ><<< ( unsigned ) grid, NT, 0, s >>>( P );
+    k_forward< TALLY, NT, false, false, false, FLUX, RESUME ><<< ( unsigned ) grid, NT, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
 }
 
@@ -1231,32 +1282,32 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets )
     }
 }
 
-template< int TALLY, bool TAPE, bool FLUX >
+template< int TALLY, bool TAPE, bool FLUX, bool RESUME >
 void launch_deferred_walk( const fwd_params_t & P, cudaStream_t s )
 {
-    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true, TAPE, FLUX >;
+    const void * kf = ( const void * ) k_forward< TALLY, 256, false, true, TAPE, FLUX, RESUME >;
     long long grid = persistent_grid( kf, 256 );
-    grid = std::min< long long >( grid, ( P.n_packets + 255 ) / 256 );
-    k_forward< TALLY, 256, false, true, TAPE, FLUX ><<< ( unsigned ) grid, 256, 0, s >>>( P );
+    grid = std::min< long long >( grid, ( P.n_packets + P.rs_n_in + 255 ) / 256 );
+    k_forward< TALLY, 256, false, true, TAPE, FLUX, RESUME ><<< ( unsigned ) grid, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
 }
 
-template< int TALLY, bool TAPE >
+template< int TALLY, bool TAPE, bool RESUME >
 void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s )
 {
     P.pq_count = P.work + 1;
     P.pq_next = P.work + 2;
     KP_CUDA( cudaMemsetAsync( P.work, 0, 3 * sizeof( unsigned long long ), s ) );
-    if( P.flux ) launch_deferred_walk< TALLY, TAPE, true  >( P, s );
-    else         launch_deferred_walk< TALLY, TAPE, false >( P, s );
+    if( P.flux ) launch_deferred_walk< TALLY, TAPE, true,  RESUME >( P, s );
+    else         launch_deferred_walk< TALLY, TAPE, false, RESUME >( P, s );
     if( split_event ) KP_CUDA( cudaEventRecord( split_event, s ) );
     constexpr int MODE = TAPE ? 3 : 0;
     const long long gp = persistent_grid( ( const void * ) k_peel< TALLY, MODE >, 256 );
     k_peel< TALLY, MODE ><<< ( unsigned ) gp, 256, 0, s >>>( P );
     KP_CUDA( cudaGetLastError(  ) );
 }
-template void launch_deferred_chunk< KP_TALLY_FIXED, true >( fwd_params_t &, cudaStream_t );
-template void launch_deferred_chunk< KP_TALLY_FLOAT, true >( fwd_params_t &, cudaStream_t );
+template void launch_deferred_chunk< KP_TALLY_FIXED, true, false >( fwd_params_t &, cudaStream_t );
+template void launch_deferred_chunk< KP_TALLY_FLOAT, true, false >( fwd_params_t &, cudaStream_t );
 
 // The deferred adjoint's marches of the queued vertex rays: mode 1 measures
 // their scores, mode 2 deposits along them (k_peel).
@@ -1296,9 +1347,7 @@ void launch_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
         C.pq_cap = mesh->pq_cap;
         C.pid0 = P.pid0 + done;
         C.n_packets = std::min( chunk, P.n_packets - done );
-        C.n_record = std::max< long long >( P.n_record - done, 0 );
-        C.records = C.n_record > 0 ? P.records + done : nullptr;
-        launch_deferred_chunk< TALLY, false >( C, s );
+        launch_deferred_chunk< TALLY, false, false >( C, s );
     }
 }
 
@@ -1364,6 +1413,96 @@ extern "C" int kp_transport_split_event( void * event )
 {
     kp::split_event = static_cast< cudaEvent_t >( event );
     return KP_OK;
+}
+
+////////////////////////////////////////////////////////////
+// Resumable solve: the step budget of one call (k_forward<..., RESUME>).
+
+static_assert( sizeof( kp_packet_state_t ) == sizeof( kp::dd_walk_t ), "packet state size" );
+static_assert( offsetof( kp_packet_state_t, n_steps ) == offsetof( kp::dd_walk_t, n_steps )
+               && offsetof( kp_packet_state_t, rng_draws ) == offsetof( kp::dd_walk_t, draw )
+               && offsetof( kp_packet_state_t, batch ) == offsetof( kp::dd_walk_t, batch ),
+               "packet state layout" );
+
+namespace kp
+{
+// With an image: work items (the resumed packets, then the new ones) in
+// chunks of the queue's capacity / 12, each walked and then marched, as
+// launch_deferred does for new packets alone.
+template< int TALLY >
+void launch_resume_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s )
+{
+    const long long n_in = P.rs_n_in, items = n_in + P.n_packets;
+    mesh->tape_id = 0;                      // the queue is overwritten
+    ensure_peel_queue( mesh, items );
+    const long long chunk = std::max< long long >( mesh->pq_cap / PQ_PER_PACKET, 1 );
+    static thread_local fwd_params_t C;
+    for( long long lo = 0; lo < items; lo += chunk )
+    {
+        const long long hi = std::min( items, lo + chunk );
+        C = P;
+        C.pq = static_cast< peel_task_t * >( mesh->d_pq );
+        C.pq_cap = mesh->pq_cap;
+        C.rs_in = P.rs_in + std::min( lo, n_in );
+        C.rs_n_in = std::max< long long >( std::min( hi, n_in ) - lo, 0 );
+        const long long first = std::max( lo, n_in );   // first new packet's item
+        C.pid0 = P.pid0 + ( first - n_in );
+        C.n_packets = std::max< long long >( hi - first, 0 );
+        launch_deferred_chunk< TALLY, false, true >( C, s );
+    }
+}
+}   // namespace kp
+
+extern "C" int kp_transport_forward_resume( kp_mesh_t * mesh, const kp_transport_cfg_t * cfg,
+                                            const kp_resume_t * rs, const kp_tallies_t * tallies,
+                                            void * stream )
+{
+    return kp::guarded( "kp_transport_forward_resume", [ & ]
+    {
+        kp::require( mesh && cfg && rs && tallies, "null argument" );
+        kp::require( rs->step_budget >= 1, "step_budget must be at least 1" );
+        kp::require( rs->n_in >= 0 && rs->cap_out >= 0, "negative queue size" );
+        kp::require( ( rs->n_in == 0 || rs->in ) && ( rs->cap_out == 0 || rs->out ) && rs->out_count,
+                     "null queue" );
+        {   // the kernel reads `in` while it writes `out`
+            const auto a0 = reinterpret_cast< uintptr_t >( rs->in );
+            const auto b0 = reinterpret_cast< uintptr_t >( rs->out );
+            const auto a1 = a0 + ( uintptr_t ) rs->n_in * sizeof( kp_packet_state_t );
+            const auto b1 = b0 + ( uintptr_t ) rs->cap_out * sizeof( kp_packet_state_t );
+            kp::require( rs->n_in == 0 || rs->cap_out == 0 || a1 <= b0 || b1 <= a0,
+                         "the in and out packet queues overlap" );
+        }
+        mesh->upload(  );
+        static thread_local kp::fwd_params_t P;
+        kp::make_fwd_params( mesh, * cfg, * tallies, P );
+        P.work = mesh->workspace(  );
+        P.rs_in = reinterpret_cast< const kp::dd_walk_t * >( rs->in );
+        P.rs_n_in = rs->n_in;
+        P.rs_out = reinterpret_cast< kp::dd_walk_t * >( rs->out );
+        P.rs_cap = rs->cap_out;
+        P.rs_count = rs->out_count;
+        P.rs_budget = rs->step_budget;
+        cudaStream_t s = ( cudaStream_t ) stream;
+        if( P.n_packets + P.rs_n_in > 0 )
+        {
+            const bool fx = cfg->tally_mode == KP_TALLY_FIXED, fl = P.flux != nullptr;
+            if( cfg->image_n > 0 )
+            {   // the deferred walk's interaction batch, as kp_transport_forward
+                if( cfg->lane_batch == 0 ) P.ev_batch = 12;
+                fx ? kp::launch_resume_deferred< KP_TALLY_FIXED >( mesh, P, s )
+                   : kp::launch_resume_deferred< KP_TALLY_FLOAT >( mesh, P, s );
+            }
+            else
+            {
+                if( fx ) fl ? kp::launch_forward_k< KP_TALLY_FIXED, 256, true,  true >( P, s, 100 )
+                            : kp::launch_forward_k< KP_TALLY_FIXED, 256, false, true >( P, s, 100 );
+                else     fl ? kp::launch_forward_k< KP_TALLY_FLOAT, 256, true,  true >( P, s, 100 )
+                            : kp::launch_forward_k< KP_TALLY_FLOAT, 256, false, true >( P, s, 100 );
+                if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, s ) );
+            }
+        }
+        kp::fold_carry( * cfg, * tallies, s );
+    } );
 }
 
 ////////////////////////////////////////////////////////////

@@ -80,6 +80,7 @@ struct fwd_params_t
     unsigned long long * counters;
     kp_packet_record_t * records;
     long long   n_record;
+    long long   rec_pid0;          // global id of the packet that records[0] holds
     void      * flux;              // path-length flux tally [n_cells] (null: off)
     double      flux_scale;        // its fixed point scale
     // float tallies' rounding-error carries (kp_tallies_t::carry; null: none)
@@ -109,6 +110,14 @@ struct fwd_params_t
     int       * dd_out_peel_rank;
     long long   dd_cap_walk, dd_cap_peel;
     unsigned long long * dd_out_count;  // [2]: walks, peel-off rays
+    // resumable solves only (kp_transport_forward_resume): packets carried
+    // across calls as whole walks
+    const struct dd_walk_t * rs_in;     // [rs_n_in] suspended earlier, resumed first
+    long long   rs_n_in;
+    struct dd_walk_t * rs_out;          // [rs_cap] suspended by this launch
+    long long   rs_cap;
+    unsigned long long * rs_count;      // records written to rs_out (may exceed rs_cap)
+    int         rs_budget;              // walk segments of a packet per launch
     // peel-off rays deferred to k_peel (plain forward solves)
     struct peel_task_t * pq;            // [pq_cap] tasks
     struct peel_link_t * pq_link;       // [pq_cap] per-packet links (tape, adjoint)
@@ -966,7 +975,7 @@ __device__ __forceinline__ bool emit_any( const fwd_params_t & P, long long pid,
 
 __device__ __forceinline__ void write_record( const fwd_params_t & P, const packet_t & p, int status )
 {
-    const long long k = p.pid(  ) - P.pid0;
+    const long long k = p.pid(  ) - P.rec_pid0;
     if( P.records == nullptr || k < 0 || k >= P.n_record ) return;
     kp_packet_record_t * r = P.records + k;       // field by field: no local copy
     #pragma unroll
@@ -1057,7 +1066,8 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets );
 // for chunks of n_pk packets), with their own counters: P.work is set to
 // them, so launches that use the mesh's workspace do not touch a tape.
 void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk );
-template< int TALLY, bool TAPE > void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s );
+template< int TALLY, bool TAPE, bool RESUME = false >
+void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s );
 // A forward solve with its peel-off rays queued for k_peel, in chunks (no tape).
 void launch_deferred_solve( kp_mesh_t * mesh, const fwd_params_t & P, int tally_mode,
                             cudaStream_t s );

@@ -17,12 +17,24 @@ import torch
 from . import _lib
 from ._lib import call, ptr
 from .config import (COUNTERS, EMIT_ISOTROPIC, EMIT_UP_UNIFORM, MAX_BATCHES,  # noqa: F401
-                     MAX_SOURCES, PACKET_INIT_DTYPE, PHASE_HG_POL, PHASE_RAYLEIGH, RECORD_DTYPE,
-                     SOURCE_PLANE_BASE, SOURCE_POINT, TALLY_FIXED, TALLY_FLOAT, CSource, CTallies,
-                     CTransportCfg, Source, TransportConfig)
+                     MAX_SOURCES, PACKET_INIT_DTYPE, PACKET_STATE_DTYPE, PHASE_HG_POL,
+                     PHASE_RAYLEIGH, RECORD_DTYPE, SOURCE_PLANE_BASE, SOURCE_POINT, TALLY_FIXED,
+                     TALLY_FLOAT, CSource, CTallies, CTransportCfg, Source, TransportConfig)
 
 _lib.register("kp_transport_forward", [ctypes.c_void_p, ctypes.POINTER(CTransportCfg),
                                        ctypes.POINTER(CTallies), ctypes.c_void_p])
+
+
+class CResume(ctypes.Structure):
+    """ctypes mirror of kp_resume_t."""
+    _fields_ = [("in_", ctypes.c_void_p), ("n_in", ctypes.c_longlong),
+                ("out", ctypes.c_void_p), ("cap_out", ctypes.c_longlong),
+                ("out_count", ctypes.c_void_p), ("step_budget", ctypes.c_int)]
+
+
+_lib.register("kp_transport_forward_resume", [ctypes.c_void_p, ctypes.POINTER(CTransportCfg),
+                                              ctypes.POINTER(CResume), ctypes.POINTER(CTallies),
+                                              ctypes.c_void_p])
 
 
 class Tallies:
@@ -123,6 +135,48 @@ def forward(mesh, cfg: TransportConfig, tallies: Tallies | None = None,
     else:
         call("kp_transport_forward", mesh.handle, ctypes.byref(c), ctypes.byref(t), s)
     return tallies
+
+
+def forward_resume(mesh, cfg: TransportConfig, step_budget: int, resumed=None,
+                   tallies: Tallies | None = None, capacity: int | None = None,
+                   stream: int | None = None):
+    """One call with a per-call step budget (``kp_transport_forward_resume``).
+
+    Resumes the packets in ``resumed`` (a device uint8 tensor [n, 128] of
+    kp_packet_state_t, as returned by an earlier call), then emits
+    ``cfg.n_packets`` new ones; every packet walks at most ``step_budget``
+    segments in this call.  Returns ``(tallies, suspended)``: the packets
+    that used up their budget, for the next call (``PACKET_STATE_DTYPE``
+    views them).  ``capacity`` bounds the suspended queue (default: every
+    packet of the call); an overflow raises.
+    """
+    if tallies is None:
+        tallies = Tallies(cfg, n_cells=mesh.n_cells if cfg.flux else 0)
+    dev = tallies.counters.device
+    n_in = 0 if resumed is None else int(resumed.shape[0])
+    cap = n_in + cfg.n_packets if capacity is None else int(capacity)
+    out = torch.empty((max(cap, 1), PACKET_STATE_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    r = CResume()
+    r.in_ = ptr(resumed) if n_in else None
+    r.n_in = n_in
+    r.out = ptr(out)
+    r.cap_out = cap
+    r.out_count = ptr(count)
+    r.step_budget = int(step_budget)
+    c, t = cfg.to_c(), tallies.to_c()
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    call("kp_transport_forward_resume", mesh.handle, ctypes.byref(c), ctypes.byref(r),
+         ctypes.byref(t), s)
+    n_out = int(count.item())
+    if n_out > cap:
+        raise RuntimeError(f"{n_out} packets suspended, the queue holds {cap}")
+    return tallies, out[:n_out]
+
+
+def packet_states(suspended: torch.Tensor) -> np.ndarray:
+    """Host view (PACKET_STATE_DTYPE) of a queue of suspended packets."""
+    return suspended.cpu().numpy().view(PACKET_STATE_DTYPE).reshape(-1)
 
 
 def packet_array(x, d, w=1.0, stokes=None, ib=-1, peel_I=0.0) -> np.ndarray:

@@ -9,6 +9,11 @@
 //                                      generated packets to <dir>/tables.bin
 //                                      and the module's container to
 //                                      <dir>/run.bin
+//   module_check pool <ini> <dir>      the same with a module that keeps its
+//                                      unfinished packets (keep_pool, at most
+//                                      100000 segments a packet), drained
+//                                      after the cycles; writes <dir>/
+//                                      tables_pool.bin and <dir>/run_pool.bin
 #include "kp_generate.cuh"
 #include "kp_module.hpp"
 
@@ -58,6 +63,12 @@ struct ring_gen_t
     }
 };
 
+// A module whose pool keeps the packets a cycle leaves unfinished.
+struct pool_rad_t : kp::particle::radiation::base_t
+{
+    kp::particle::comm_mode_t comm_mode(  ) const override { return kp::particle::keep_pool; }
+};
+
 void configure( kp::particle::radiation::base_t & rad )
 {
     auto & c = rad.transport_cfg(  );
@@ -81,13 +92,16 @@ int main( int argc, char ** argv )
 {
     if( argc < 3 )
     {
-        std::fprintf( stderr, "usage: module_check host|gpu <ini> [dir]\n" );
+        std::fprintf( stderr, "usage: module_check host|gpu|pool <ini> [dir]\n" );
         return 2;
     }
     const std::string mode = argv[ 1 ], ini = argv[ 2 ];
     try
     {
-        kp::particle::radiation::base_t rad;
+        const bool pool = mode == "pool";
+        pool_rad_t pool_rad;
+        kp::particle::radiation::base_t plain_rad;
+        kp::particle::radiation::base_t & rad = pool ? pool_rad : plain_rad;
         rad.read( ini );
         const auto & p = rad.particle_cfg(  );
         std::printf( "OK keys n_par=%g step_max=%d n_hv=%d n_cycle_stp=%d n_th=%d f_par=%g "
@@ -112,7 +126,10 @@ int main( int argc, char ** argv )
             throw std::runtime_error( "cannot read sigma.bin" );
         mesh.set_sigma( sig.data(  ), ( long long ) sig.size(  ) );
         rad.init( mesh );
-        std::ofstream ft( dir + "/tables.bin", std::ios::binary );
+        if( pool )
+            rad.pool_max_steps(  ) = 100000;
+        const std::string sfx = pool ? "_pool" : "";
+        std::ofstream ft( dir + "/tables" + sfx + ".bin", std::ios::binary );
         std::vector< kp_packet_init_t > table( ( size_t ) rad.packets_per_cycle(  ) );
         for( int c = 0; c < p.n_cycle_stp; ++ c )
         {
@@ -120,11 +137,15 @@ int main( int argc, char ** argv )
             dev.cp( table.data(  ), rad.packet_table(  ), table.size(  ) );
             ft.write( reinterpret_cast< const char * >( table.data(  ) ),
                       table.size(  ) * sizeof( kp_packet_init_t ) );
+            if( pool )
+                std::printf( "OK pool after cycle %d: %lld packets\n", c, rad.pool_size(  ) );
         }
+        rad.drain(  );
         dev.sync_all_streams(  );
         mesh.status(  );
-        rad.save( dir + "/run.bin" );
-        std::printf( "OK module packets_done=%lld\n", rad.packets_done(  ) );
+        rad.save( dir + "/run" + sfx + ".bin" );
+        std::printf( "OK module packets_done=%lld pool=%lld\n", rad.packets_done(  ),
+                     rad.pool_size(  ) );
         return 0;
     }
     catch( const std::exception & e )

@@ -46,3 +46,39 @@ def test_tape_entry_points_refuse_without_a_taped_solve():
                                                 None, None, None, None)
         assert st == _lib.KP_ERR_CONFIG
         assert b"no taped solve" in _lib.lib.kp_last_error()
+
+
+def test_resume_arguments_are_checked_before_device_work():
+    """kp_transport_forward_resume refuses a budget below 1, missing queues
+    and overlapping in/out queues (KP_ERR_ARG), before touching a GPU."""
+    from meshcases import AMR_BOX
+    from kratos_polrad_b200 import Mesh
+    from kratos_polrad_b200.transport import (CResume, EMIT_ISOTROPIC, SOURCE_POINT, Source,
+                                              TransportConfig)
+    from kratos_polrad_b200.config import CTallies
+    m = Mesh(AMR_BOX)
+    c = TransportConfig(n_packets=10, sources=[Source(SOURCE_POINT, EMIT_ISOTROPIC,
+                                                      (0.5, 0.5, 0.5))]).to_c()
+    t = CTallies()
+    buf = (ctypes.c_ubyte * (128 * 8))()
+    cnt = ctypes.c_ulonglong(0)
+    base = ctypes.addressof(buf)
+
+    def run(**kw):
+        r = CResume()
+        r.in_, r.n_in, r.out, r.cap_out = None, 0, base, 4
+        r.out_count, r.step_budget = ctypes.addressof(cnt), 10
+        for k, v in kw.items():
+            setattr(r, k, v)
+        st = _lib.lib.kp_transport_forward_resume(m.handle, ctypes.byref(c), ctypes.byref(r),
+                                                  ctypes.byref(t), None)
+        return st, _lib.lib.kp_last_error()
+
+    st, msg = run(step_budget=0)
+    assert st == _lib.KP_ERR_ARG and b"step_budget" in msg
+    st, msg = run(out_count=None)
+    assert st == _lib.KP_ERR_ARG and b"null queue" in msg
+    st, msg = run(n_in=3)                       # in is null
+    assert st == _lib.KP_ERR_ARG and b"null queue" in msg
+    st, msg = run(in_=base + 128 * 2, n_in=3)   # overlaps out[2:4]
+    assert st == _lib.KP_ERR_ARG and b"overlap" in msg

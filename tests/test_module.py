@@ -91,7 +91,7 @@ def test_module_run_matches_restatement(program):
     sig.tofile(d / "sigma.bin")
     r = subprocess.run([exe, "gpu", ini, str(d)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "OK module packets_done=3000" in r.stdout, r.stdout
+    assert "OK module packets_done=3000 pool=0" in r.stdout, r.stdout
     tables = np.fromfile(d / "tables.bin", PACKET_INIT_DTYPE).reshape(2, 1500)
     assert (tables["w"] >= 0.5).all()
     assert np.allclose(np.linalg.norm(tables["d"], axis=-1), 1, atol=1e-6)
@@ -122,3 +122,49 @@ def test_module_run_matches_restatement(program):
             np.testing.assert_array_equal(
                 fld[:, 0], (want["flux"][b * cpb:(b + 1) * cpb] * 2.0 ** -24).astype(np.float32))
             assert (fld[:, 1] == 0).all()
+
+
+@pytest.mark.gpu
+def test_module_keep_pool_matches_restatement(program):
+    """comm_mode() keep_pool: with step_max = 25 most packets outlive their
+    cycle, wait in the pool and go on in the next; drained after the cycles,
+    the run equals the restatement of the same packets walked to the end
+    (at most 100000 segments), bit for bit."""
+    from kratos_polrad_b200 import Mesh, bio
+    from kratos_polrad_b200.transport import PACKET_INIT_DTYPE, TransportConfig
+    from oracle import port
+    from transport_cases import cell_centers, oracle_inputs
+    exe, _, d = program
+    ini = d / "pool.ini"
+    ini.write_text(AMR_BOX.to_ini() + PARTICLE.replace("step_max = 100000", "step_max = 25"))
+    mesh = Mesh(AMR_BOX)
+    c = cell_centers(mesh)
+    rng = np.random.default_rng(12)
+    ext = 1.5 + 5.0 * np.exp(-((c - 0.5) ** 2).sum(1) / (2 * 0.1 ** 2))
+    alb = rng.uniform(0.6, 0.97, mesh.n_cells)
+    sig = np.stack([ext * alb, ext * (1 - alb)], 1).astype(np.float32)
+    sig.tofile(d / "sigma.bin")
+    r = subprocess.run([exe, "pool", str(ini), str(d)], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK module packets_done=3000 pool=0" in r.stdout, r.stdout
+    kept = [int(line.split()[-2]) for line in r.stdout.splitlines()
+            if line.startswith("OK pool after cycle")]
+    assert len(kept) == 2 and min(kept) > 100, r.stdout
+    tables = np.fromfile(d / "tables_pool.bin", PACKET_INIT_DTYPE).reshape(2, 1500)
+    cfg = TransportConfig(n_packets=1500, sources=[], seed=11, max_steps=100000, image_n=32,
+                          inclination_deg=60.0, image_center=(0.5, 0.5, 0.5),
+                          image_half_width=0.87, image_batch_n=4, n_mu_bins=8, mu_lo=-1.0,
+                          mu_hi=1.0, w_min=0.05, fx_shift=32, flux_fx_shift=24, flux=True)
+    tab, grid, gn, cells = oracle_inputs(mesh, cfg)
+    want = None
+    for cyc in range(2):
+        cc = dataclasses.replace(cfg, packet_offset=1500 * cyc, packets=tables[cyc])
+        o = port.transport(tab, sig, grid, gn, cc, cells, flux=True)
+        want = o if want is None else {k: want[k] + o[k] for k in
+                                       ("mu", "image", "image_batch", "counters", "flux")}
+    got = bio.load_solution(str(d / "run_pool.bin"))
+    for k in ("mu", "image", "image_batch", "flux"):
+        np.testing.assert_array_equal(got[k].astype(np.int64), want[k], err_msg=k)
+    np.testing.assert_array_equal(got["counters"].astype(np.int64),
+                                  want["counters"].astype(np.int64))
