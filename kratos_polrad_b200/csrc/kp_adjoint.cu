@@ -343,8 +343,7 @@ k_adjoint( const __grid_constant__ fwd_params_t P )
         if( phase != PH_SEGMENT ) continue;
         const bool peel = ray != RAY_WALK;
         const size_t ci = cell_index( P.m, p.b, p.c );
-        const float2 sg = P.m.sigma[ ci ];
-        const float ext = __fadd_rn( sg.x, sg.y );
+        const float ext = P.m.ext[ ci ];
         int ax;                                   // p.d / p.inv: the active ray's
         double t;
         if( peel )
@@ -640,8 +639,7 @@ k_adj_walk( const __grid_constant__ fwd_params_t P )
         for( int it = 0; it < KP_WALK_INNER; ++ it )
         {
             const size_t ci = cell_index( P.m, p.b, p.c );
-            const float2 sg = P.m.sigma[ ci ];
-            const float ext = __fadd_rn( sg.x, sg.y );
+            const float ext = P.m.ext[ ci ];
             int ax;
             const double t = exit_cached( p.x, fx, p.d, p.inv, ax );
             const float et = __fmul_rn( ext, ( float ) t );
@@ -904,6 +902,7 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
         adjoint_params( mesh, cfg, adj_image, grad_fx_shift, grad_len, grad_int, counters, P );
         if( P.n_packets == 0 ) return;
         auto s = ( cudaStream_t ) stream;
+        mesh->refresh_ext( s );
         const bool fx = cfg->tally_mode == KP_TALLY_FIXED;
         const int threads = kp::FWD_THREADS;
         mesh->tape_id = 0;                  // the queue is overwritten
@@ -950,6 +949,7 @@ extern "C" int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_c
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         if( P.n_packets == 0 ) return;
+        mesh->refresh_ext( ( cudaStream_t ) stream );
         if( cfg->lane_batch == 0 ) P.ev_batch = 12;
         kp::ensure_peel_queue( mesh, P.n_packets );
         if( P.n_packets > std::max< long long >( mesh->pq_cap / kp::PQ_PER_PACKET, 1 ) )
@@ -995,6 +995,7 @@ extern "C" int kp_transport_adjoint_tape( kp_mesh_t * mesh, long long tape_id,
         adjoint_params( mesh, cfg, adj_image, grad_fx_shift, grad_len, grad_int, counters, P );
         kp::adjoint_buffers( mesh, P, mesh->tape_n );      // the taped solve's layout
         auto s = ( cudaStream_t ) stream;
+        mesh->refresh_ext( s );
         const unsigned gs = 4 * 148;
         kp::k_adj_score<<< gs, 256, 0, s >>>( P );                        // G from the tape
         KP_CUDA( cudaGetLastError(  ) );

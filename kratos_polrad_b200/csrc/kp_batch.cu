@@ -28,12 +28,14 @@ struct kp_batch
     std::vector< kp_mesh_t * > meshes;
     std::vector< long long >   cell_off;       // first cell of each scene
     std::vector< long long >   prefix;         // packet index prefix [n + 1]
+    long long                  n_cells = 0;    // of the concatenated mesh
     std::vector< kp::scene_dev_t > scenes;
     kp::mesh_view_t view {  };
     int        * d_nb = nullptr;
     kp::blk_meta_t * d_meta = nullptr;
     double     * d_geo = nullptr;
     float2     * d_sigma = nullptr;
+    float      * d_ext = nullptr;              // sca + abs per cell, from d_sigma
     unsigned   * d_status = nullptr;
     unsigned long long * d_work = nullptr;
     long long  * d_prefix = nullptr;
@@ -50,6 +52,7 @@ struct kp_batch
     {
         if( gexec ) cudaGraphExecDestroy( gexec );
         cudaFree( d_nb ); cudaFree( d_meta ); cudaFree( d_geo ); cudaFree( d_sigma );
+        cudaFree( d_ext );
         cudaFree( d_status ); cudaFree( d_work ); cudaFree( d_prefix );
         cudaFree( d_prefix_trial ); cudaFree( d_scenes );
     }
@@ -68,6 +71,7 @@ void copy_sigma( kp_batch_t * b, cudaStream_t s )
         KP_CUDA( cudaMemcpyAsync( b->d_sigma + b->cell_off[ k ], m->d_sigma, n * sizeof( float2 ),
                                   cudaMemcpyDeviceToDevice, s ) );
     }
+    kp::extinction( b->d_sigma, b->d_ext, b->n_cells, s );
 }
 
 // Launch parameters of a batched solve.
@@ -172,6 +176,8 @@ int kp_batch_create( int n_scenes, const kp_scene_t * sc, kp_batch_t ** out )
         KP_CUDA( cudaMalloc( & b->d_meta, meta.size(  ) * sizeof( kp::blk_meta_t ) ) );
         KP_CUDA( cudaMalloc( & b->d_geo, geo.size(  ) * sizeof( double ) ) );
         KP_CUDA( cudaMalloc( & b->d_sigma, n_cells * sizeof( float2 ) ) );
+        KP_CUDA( cudaMalloc( & b->d_ext, n_cells * sizeof( float ) ) );
+        b->n_cells = ( long long ) n_cells;
         KP_CUDA( cudaMalloc( & b->d_status, 4 * sizeof( unsigned ) ) );
         KP_CUDA( cudaMalloc( & b->d_work, 4 * sizeof( unsigned long long ) ) );
         KP_CUDA( cudaMalloc( & b->d_prefix, b->prefix.size(  ) * sizeof( long long ) ) );
@@ -197,6 +203,7 @@ int kp_batch_create( int n_scenes, const kp_scene_t * sc, kp_batch_t ** out )
         v.meta = b->d_meta;
         v.geo_d = b->d_geo;
         v.sigma = b->d_sigma;
+        v.ext = b->d_ext;
         v.status = b->d_status;
         * out = b.release(  );
     } );

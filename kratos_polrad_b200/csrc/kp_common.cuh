@@ -103,6 +103,9 @@ struct mesh_view_t
                                           //   inv_dx[3] - ...
     const float      * __restrict__ geo_f;// [n_blocks][8]
     const float2     * __restrict__ sigma;// [n_blocks * cpb] (sca, abs)
+    // [n_blocks * cpb] extinction sca + abs (one float add, the value each
+    // walk and peel-off segment needs), derived from sigma before each solve
+    const float      * __restrict__ ext;
     const int        * __restrict__ lookup;// finest-level block grid
     int lookup_n[ 3 ];
     int max_level;
@@ -131,6 +134,7 @@ struct kp_mesh
     double     * d_geo_d  = nullptr;
     float      * d_geo_f  = nullptr;
     float2     * d_sigma  = nullptr;
+    float      * d_ext    = nullptr;     // sca + abs per cell (refresh_ext)
     int        * d_lookup = nullptr;
     unsigned   * d_status = nullptr;
     void       * d_pq    = nullptr;  long long pq_cap = 0;        // deferred peel-off rays
@@ -151,5 +155,14 @@ struct kp_mesh
     // Copies the tables to the current device; with_sigma also allocates the
     // (zeroed) coefficient array, which a decomposed rank does not hold.
     void upload( bool with_sigma = true );
+    // Recomputes d_ext from d_sigma on stream s: every solve does this first,
+    // since callers may write the coefficients through kp_mesh_sigma_ptr.
+    void refresh_ext( cudaStream_t s );
     void release(  );
 };
+
+namespace kp
+{
+// ext[i] = sigma[i].x + sigma[i].y (IEEE float add) for n cells, on stream s.
+void extinction( const float2 * sigma, float * ext, long long n, cudaStream_t s );
+}

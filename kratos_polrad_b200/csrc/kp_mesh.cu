@@ -2,6 +2,7 @@
 #include "kp_common.cuh"
 #include "host/ini.h"
 
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -20,6 +21,7 @@ kp::mesh_view_t kp_mesh::view(  ) const
     v.geo_d = d_geo_d;
     v.geo_f = d_geo_f;
     v.sigma = d_sigma;
+    v.ext   = d_ext;
     v.lookup = d_lookup;
     for( int a = 0; a < 3; ++ a ) v.lookup_n[ a ] = t.lookup_n[ a ];
     v.max_level = t.max_level;
@@ -40,6 +42,39 @@ kp::mesh_view_t kp_mesh::view(  ) const
     return v;
 }
 
+namespace
+{
+__global__ void k_extinction( const float2 * __restrict__ sigma, float * __restrict__ ext,
+                              long long n )
+{
+    const long long stride = ( long long ) gridDim.x * blockDim.x;
+    for( long long i = ( long long ) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride )
+    {
+        const float2 s = sigma[ i ];
+        ext[ i ] = __fadd_rn( s.x, s.y );
+    }
+}
+}   // namespace
+
+void kp::extinction( const float2 * sigma, float * ext, long long n, cudaStream_t s )
+{
+    if( n <= 0 ) return;
+    int dev = 0, n_sm = 0;
+    KP_CUDA( cudaGetDevice( & dev ) );
+    KP_CUDA( cudaDeviceGetAttribute( & n_sm, cudaDevAttrMultiProcessorCount, dev ) );
+    const long long grid = std::min< long long >( ( n + 255 ) / 256, 8ll * n_sm );
+    k_extinction<<< ( unsigned ) grid, 256, 0, s >>>( sigma, ext, n );
+    KP_CUDA( cudaGetLastError(  ) );
+}
+
+void kp_mesh::refresh_ext( cudaStream_t s )
+{
+    kp::require( d_sigma != nullptr && d_ext != nullptr, "mesh coefficients not on the device",
+                 KP_ERR_CONFIG );
+    const auto & t = tree->tables(  );
+    kp::extinction( d_sigma, d_ext, ( long long ) t.n_blocks * t.cells_per_block, s );
+}
+
 void kp_mesh::upload( bool with_sigma )
 {
     int dev = 0;
@@ -54,6 +89,8 @@ void kp_mesh::upload( bool with_sigma )
             const size_t n = ( size_t ) t.n_blocks * t.cells_per_block;
             KP_CUDA( cudaMalloc( & d_sigma, n * sizeof( float2 ) ) );
             KP_CUDA( cudaMemset( d_sigma, 0, n * sizeof( float2 ) ) );
+            KP_CUDA( cudaMalloc( & d_ext, n * sizeof( float ) ) );
+            KP_CUDA( cudaMemset( d_ext, 0, n * sizeof( float ) ) );
         }
         return;
     }
@@ -94,7 +131,10 @@ void kp_mesh::upload( bool with_sigma )
                              cudaMemcpyHostToDevice ) );
         KP_CUDA( cudaMalloc( & d_geo_f,  nb * 8 * sizeof( float ) ) );
         if( with_sigma )
+        {
             KP_CUDA( cudaMalloc( & d_sigma,  n_cells * sizeof( float2 ) ) );
+            KP_CUDA( cudaMalloc( & d_ext,    n_cells * sizeof( float ) ) );
+        }
         KP_CUDA( cudaMalloc( & d_status, 4 * sizeof( unsigned ) ) );
         KP_CUDA( cudaMalloc( & d_work, 32 * sizeof( unsigned long long ) ) );
         if( t.coord == 1 )
@@ -122,7 +162,10 @@ void kp_mesh::upload( bool with_sigma )
         KP_CUDA( cudaMemcpy( d_geo_f, gf.data(  ), gf.size(  ) * sizeof( float ),
                              cudaMemcpyHostToDevice ) );
         if( with_sigma )
+        {
             KP_CUDA( cudaMemset( d_sigma, 0, n_cells * sizeof( float2 ) ) );
+            KP_CUDA( cudaMemset( d_ext, 0, n_cells * sizeof( float ) ) );
+        }
         KP_CUDA( cudaMemset( d_status, 0, 4 * sizeof( unsigned ) ) );
     }
     catch( ... )
@@ -141,6 +184,7 @@ void kp_mesh::release(  )
     cudaFree( d_geo_d );  d_geo_d  = nullptr;
     cudaFree( d_geo_f );  d_geo_f  = nullptr;
     cudaFree( d_sigma );  d_sigma  = nullptr;
+    cudaFree( d_ext );    d_ext    = nullptr;
     cudaFree( d_lookup ); d_lookup = nullptr;
     cudaFree( d_status ); d_status = nullptr;
     cudaFree( d_work );   d_work   = nullptr;

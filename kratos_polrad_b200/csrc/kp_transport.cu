@@ -41,6 +41,9 @@ namespace cg = cooperative_groups;
 #ifndef KP_HOP_BATCH
 #define KP_HOP_BATCH 6               // lanes that wait for a batched block hand-off
 #endif
+#ifndef KP_EMIT_BATCH
+#define KP_EMIT_BATCH 0              // lanes that wait for an emission batch (0: the event batch)
+#endif
 #ifndef KP_PEEL_INNER
 #define KP_PEEL_INNER 8              // k_peel: segments per scheduling round
 #endif
@@ -178,6 +181,17 @@ k_forward( const __grid_constant__ fwd_params_t P )
         }
         else
             return P.m.sigma[ cell_index( P.m, b, c ) ];
+    };
+    // extinction of cell c of block b (the float sum of its coefficients)
+    auto ext_at = [ & ]( int b, const int c[ 3 ] ) -> float
+    {
+        if constexpr( DD )
+        {
+            const float2 sg = sigma_at( b, c );
+            return __fadd_rn( sg.x, sg.y );
+        }
+        else
+            return P.m.ext[ cell_index( P.m, b, c ) ];
     };
 
     // FLUX: w / volume of block b for the walk's later segments
@@ -337,7 +351,8 @@ k_forward( const __grid_constant__ fwd_params_t P )
         int run;
         if( n_ev > 0 && ( n_ev >= P.ev_batch || n_seg == 0 ) )
             run = PH_EVENT;
-        else if( n_emit > 0 && ( n_emit >= P.ev_batch || n_seg == 0 ) )
+        else if( n_emit > 0 && ( n_emit >= ( P.emit_batch > 0 ? P.emit_batch : P.ev_batch )
+                                 || n_seg == 0 ) )
             run = PH_EMIT;
         else if( n_hop > 0 && ( n_hop >= P.hop_batch || n_seg == 0 ) )
             run = PH_HOP;
@@ -694,8 +709,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
         {
             // the active ray's direction is in p.d / p.inv (a peel-off ray
             // holds them while the walk's are parked)
-            const float2 sg = sigma_at( p.b, p.c );
-            const float ext = __fadd_rn( sg.x, sg.y );
+            const float ext = ext_at( p.b, p.c );
             int ax;
             double t;
             if( peel )
@@ -796,7 +810,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
     double x0[ 3 ], tm[ 3 ], g0[ 3 ], gd[ 3 ];    // ray start, distances to the next faces
     double tc = 0.0;                              // distance travelled from x0
     int    c[ 3 ] = { 0, 0, 0 }, b = 0, hop_ax = 0, pk = 0, ci = 0;
-    const float2 * sb = P.m.sigma;                // this block's coefficients
+    const float * eb = P.m.ext;                   // this block's extinctions
     float  ptau = 0.0f;
     float  pG = 0.0f;                             // MODE 2: the ray's score
     int    n_dep = 0;                             // MODE 2: ... and its segments
@@ -826,7 +840,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
                     : __dmul_rn( __dsub_rn( __fma_rn( ( double ) ( c[ a ] + ( oa > 0.0f ? 1 : 0 ) ),
                                                       gd[ a ], g0[ a ] ), x0[ a ] ), P.inv_o[ a ] );
         }
-        sb = P.m.sigma + ( size_t ) b * P.m.cpb;
+        eb = P.m.ext + ( size_t ) b * P.m.cpb;
         ci = c[ 0 ] + nc0 * ( c[ 1 ] + nc1 * c[ 2 ] );
     };
     for( ;; )
@@ -953,7 +967,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
             if constexpr( MODE == 2 )
             {   // the measuring march counted the segments inside the cut:
                 // geometry only, no coefficients
-                add_grad< TALLY >( g_dep, ( size_t ) ( sb - P.m.sigma ) + ci,
+                add_grad< TALLY >( g_dep, ( size_t ) ( eb - P.m.ext ) + ci,
                                    __dmul_rn( -( double ) pG, t ), P.g_scale );
                 if( pk >= n_dep )
                 {
@@ -963,9 +977,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
             }
             else
             {
-                const float2 sg = sb[ ci ];
-                const float ext = __fadd_rn( sg.x, sg.y );
-                ptau = __fadd_rn( ptau, __fmul_rn( ext, ( float ) t ) );
+                ptau = __fadd_rn( ptau, __fmul_rn( eb[ ci ], ( float ) t ) );
                 if( ptau > P.tau_cut )
                 {
                     phase = PH_EMIT;
@@ -1087,6 +1099,7 @@ void fill_common_params( const kp_transport_cfg_t & c, const kp_tallies_t & t,
     // before it): the neighbour lookup and the new block's geometry are
     // dependent loads, paid once per batch.
     P.hop_batch = KP_HOP_BATCH;
+    P.emit_batch = KP_EMIT_BATCH;
     P.peel_batch = KP_PEEL_BATCH;
     P.mu_tally = t.mu;
     P.image = t.image;
@@ -1366,6 +1379,7 @@ extern "C" int kp_transport_forward( kp_mesh_t * mesh, const kp_transport_cfg_t 
     {
         kp::require( mesh && cfg && tallies, "null argument" );
         mesh->upload(  );
+        mesh->refresh_ext( ( cudaStream_t ) stream );
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = mesh->workspace(  );
@@ -1473,6 +1487,7 @@ extern "C" int kp_transport_forward_resume( kp_mesh_t * mesh, const kp_transport
                          "the in and out packet queues overlap" );
         }
         mesh->upload(  );
+        mesh->refresh_ext( ( cudaStream_t ) stream );
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = mesh->workspace(  );
@@ -1633,6 +1648,7 @@ extern "C" int kp_transport_forward_noalloc( kp_mesh_t * mesh, const kp_transpor
         static thread_local kp::fwd_params_t P;
         kp::make_fwd_params( mesh, * cfg, * tallies, P );
         P.work = static_cast< unsigned long long * >( kp::noalloc_scratch(  ) );
+        mesh->refresh_ext( ( cudaStream_t ) stream );    // a kernel into mesh memory
         kp::launch_forward( P, cfg->tally_mode, ( cudaStream_t ) stream, 256, 100 );
         if( kp::split_event ) KP_CUDA( cudaEventRecord( kp::split_event, ( cudaStream_t ) stream ) );
         kp::fold_carry( * cfg, * tallies, ( cudaStream_t ) stream );

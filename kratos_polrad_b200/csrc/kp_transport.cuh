@@ -71,6 +71,7 @@ struct fwd_params_t
     int         max_scatter;
     long long   max_steps;
     int         ev_batch;          // lanes that must wait for an event batch
+    int         emit_batch;        // lanes that must wait for an emission batch (0: ev_batch)
     int         hop_batch;         // lanes that must wait for a hand-off batch
     int         peel_batch;        // k_peel: lanes that must wait for a fetch batch
     double      lk_inv[ 3 ];       // lookup cells per unit length
@@ -644,8 +645,7 @@ __device__ __forceinline__ float oray_march( const fwd_params_t & P, int b, cons
     float tau = 0.0f;
     for( int k = 0; k < ( 1 << 20 ); ++ k )
     {
-        const float2 sg = P.m.sigma[ cell_index( P.m, b, c ) ];
-        const float ext = __fadd_rn( sg.x, sg.y );
+        const float ext = P.m.ext[ cell_index( P.m, b, c ) ];
         int ax;
         const double dt = oray_segment( tm, tc, ax );
         tau = __fadd_rn( tau, __fmul_rn( ext, ( float ) dt ) );
