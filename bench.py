@@ -47,7 +47,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="clump",
                    choices=["clump", "batched", "diff", "large", "decomp", "trace", "sph",
-                            "refine", "bio"])
+                            "refine", "bio", "resume"])
+    p.add_argument("--budget", type=int, default=256,
+                   help="resume workload: walk segments per packet and call")
     return p.parse_args()
 
 
@@ -812,6 +814,52 @@ def run_bio(args):
     print(json.dumps(line), flush=True)
 
 
+def run_resume(args):
+    """Resumable calls: the clump solve carried out in calls with a step budget
+    of `--budget` walk segments per packet and call (kp_transport_forward_resume;
+    the packets still walking are written out and resumed by the next call)
+    against one uninterrupted solve of the same packets: device time of all
+    the calls, their number, the packets carried between calls, and the
+    tallies compared."""
+    import torch
+    from kratos_polrad_b200 import scenes
+    from kratos_polrad_b200.transport import Tallies, forward, forward_resume
+    n_pk = int(args.packets)
+    mesh, sigma2, cfg = scenes.clump_amr(n_packets=n_pk)
+    mesh.set_sigma(sigma2)
+    rest = dataclasses.replace(cfg, n_packets=0)
+
+    def budgeted(tal):
+        tal, out = forward_resume(mesh, cfg, args.budget, tallies=tal)
+        calls, carried = 1, int(out.shape[0])
+        while out.shape[0] > 0 and calls < 10000:
+            tal, out = forward_resume(mesh, rest, args.budget, resumed=out, tallies=tal)
+            calls += 1
+            carried += int(out.shape[0])
+        return tal, calls, carried, int(out.shape[0])
+
+    full = Tallies(cfg)
+    forward(mesh, cfg, full)                     # warm-up of both forms
+    budgeted(Tallies(cfg))
+    torch.cuda.synchronize()
+    full.zero_()
+    _, t_full = _timed(lambda: forward(mesh, cfg, full))
+    (tal, calls, carried, left), t_res = _timed(lambda: budgeted(Tallies(cfg)))
+    assert mesh.status() == 0
+    same = all(torch.equal(getattr(tal, k), getattr(full, k))
+               for k in ("image", "image_batch", "mu", "counters"))
+    c = full.counts()
+    steps = c["steps"] + c["peel_steps"]
+    print(json.dumps({"metric": "packet-steps/s, clump solve in budgeted calls", "unit": UNIT,
+                      "value": steps / (t_res / 1e3), "higher_is_better": True, "n_gpus": 1,
+                      "config": {"workload": "clump_amr_2level_resumed", "packets": n_pk,
+                                 "step_budget": args.budget},
+                      "calls": calls, "packets_carried": carried, "packets_left": left,
+                      "ms_budgeted": t_res, "ms_one_solve": t_full,
+                      "cost_vs_one_solve": t_res / t_full,
+                      "tallies_equal_one_solve": same}), flush=True)
+
+
 def run_large(args):
     """Large workload: 256^3 root, 3 levels on a lognormal field (std of ln
     rho 1.5, seed 5; ~2e7 cells, 166 MB of coefficients: beyond L2), HG g=0.6
@@ -888,6 +936,8 @@ def main():
         return run_refine(args)
     if args.workload == "bio":
         return run_bio(args)
+    if args.workload == "resume":
+        return run_resume(args)
     if args.impl == "reference":     # host cores only: rank 0 runs, the others exit
         run_reference(args, int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)))
         return
