@@ -1165,7 +1165,9 @@ def main():
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
                "adjoint": adjoint_info, "flux_tally": flux_info, "batched": batched_info,
-               "gpu_launches": args.steps * (2 if cfg.image_n > 0 else 1),
+               # per solve: the extinction refresh, the walk and (with an
+               # image) the peel-off march
+               "gpu_launches": args.steps * (3 if cfg.image_n > 0 else 2),
                "clocks": clk.summary()}
         print(json.dumps(out), flush=True)
     if world > 1:
