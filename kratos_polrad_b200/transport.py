@@ -153,6 +153,11 @@ def forward_resume(mesh, cfg: TransportConfig, step_budget: int, resumed=None,
     if tallies is None:
         tallies = Tallies(cfg, n_cells=mesh.n_cells if cfg.flux else 0)
     dev = tallies.counters.device
+    if resumed is not None and not (resumed.dtype == torch.uint8 and resumed.dim() == 2
+                                    and resumed.shape[1] == PACKET_STATE_DTYPE.itemsize
+                                    and resumed.is_contiguous() and resumed.device == dev):
+        raise ValueError("resumed must be a contiguous uint8 [n, 128] tensor of packet states "
+                         "on the tallies' device")
     n_in = 0 if resumed is None else int(resumed.shape[0])
     cap = n_in + cfg.n_packets if capacity is None else int(capacity)
     out = torch.empty((max(cap, 1), PACKET_STATE_DTYPE.itemsize), dtype=torch.uint8, device=dev)

@@ -82,3 +82,20 @@ def test_resume_arguments_are_checked_before_device_work():
     assert st == _lib.KP_ERR_ARG and b"null queue" in msg
     st, msg = run(in_=base + 128 * 2, n_in=3)   # overlaps out[2:4]
     assert st == _lib.KP_ERR_ARG and b"overlap" in msg
+
+
+def test_resume_python_rejects_a_malformed_queue():
+    """forward_resume checks the resumed queue's type and shape before any
+    call (a CPU tensor of the wrong width here)."""
+    import pytest
+    import torch
+    from meshcases import AMR_BOX
+    from kratos_polrad_b200 import Mesh
+    from kratos_polrad_b200.transport import (EMIT_ISOTROPIC, SOURCE_POINT, Source, Tallies,
+                                              TransportConfig, forward_resume)
+    cfg = TransportConfig(n_packets=10, sources=[Source(SOURCE_POINT, EMIT_ISOTROPIC,
+                                                        (0.5, 0.5, 0.5))])
+    tal = Tallies(cfg, device="cpu")
+    with pytest.raises(ValueError, match="packet states"):
+        forward_resume(Mesh(AMR_BOX), cfg, 10, resumed=torch.zeros((4, 64), dtype=torch.uint8),
+                       tallies=tal)
