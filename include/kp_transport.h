@@ -575,7 +575,10 @@ int kp_mesh_tape_id( const kp_mesh_t * mesh, long long * tape_id );
  * int64 tallies are the same bit for bit, float tallies agree within float
  * rounding (another summation order; kp_tallies_t::carry, the caller's
  * memory, folds in their rounding errors), and the solve is slower.  A
- * kp_transport_split_event event is recorded after the walk.  Inputs and outputs are the
+ * kp_transport_split_event event is recorded after the walk.  Like every
+ * solve it first refreshes the mesh's per-cell extinction array from the
+ * coefficients, a kernel into memory the mesh allocated with its
+ * coefficients at upload.  Inputs and outputs are the
  * caller's: the mesh must already be on the current device (kp_mesh_upload,
  * or an earlier kp_mesh_set_sigma, at set-up time), else KP_ERR_CONFIG; a
  * solve whose scratch would not fit is rejected with KP_ERR_CAPACITY.  The
