@@ -671,6 +671,13 @@ typedef struct kp_particle_cfg
  * values override earlier ones, io/args/input.cpp:72-108). */
 int kp_particle_read( const char * ini_path, kp_particle_cfg_t * out );
 
+/* prob::cmd (user/probgen.cpp:8-16): reads the input files paths[0..n-1]
+ * in order with the reference's syntax, a later file's value of a key
+ * replacing an earlier one's (input::read, io/args/input.cpp:72-108,
+ * 162-167), and writes the merged keys to out_path as one INI file for
+ * kp_mesh_create_ini and kp_particle_read. */
+int kp_ini_merge( int n, const char * const * paths, const char * out_path );
+
 /* ------------------------------------------------------------------ */
 /* Binary container of the reference's binary_io (io/binary/            */
 /* binary_io.h:6-32; save/load in binary_io_base.cpp:89-131): a byte of */

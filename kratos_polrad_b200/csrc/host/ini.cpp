@@ -64,6 +64,28 @@ std::vector< std::string > ini_t::values( const std::string & sec,
     return out;
 }
 
+std::string ini_t::text(  ) const
+{
+    std::map< std::string, std::vector< std::pair< std::string, std::string > > > by_sec;
+    for( const auto & kv : map_ )
+    {
+        const auto bar = kv.first.find( '|' );
+        by_sec[ kv.first.substr( 0, bar ) ].emplace_back( kv.first.substr( bar + 1 ), kv.second );
+    }
+    for( const auto & s : secs_ )
+        by_sec[ s ];                                // sections without keys
+    std::ostringstream out;
+    for( const auto & [ sec, keys ] : by_sec )
+    {
+        if( ! sec.empty(  ) )
+            out << "[" << sec << "]\n";
+        for( const auto & [ k, v ] : keys )
+            out << k << " = " << v << "\n";
+        out << "\n";
+    }
+    return out.str(  );
+}
+
 void ini_t::set( const std::string & sec, const std::string & key,
                  const std::string & val )
 {

@@ -64,6 +64,9 @@ public:
     }
     void set( const std::string & sec, const std::string & key,
               const std::string & val );
+    // The keys as INI text: keys outside any section first, then one
+    // [section] block per section in name order, keys in name order.
+    std::string text(  ) const;
 
 private:
     std::map< std::string, std::string > map_;

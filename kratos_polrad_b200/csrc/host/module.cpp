@@ -4,6 +4,30 @@
 #include "../kp_common.cuh"
 #include "ini.h"
 
+#include <fstream>
+#include <string>
+
+extern "C" int kp_ini_merge( int n, const char * const * paths, const char * out_path )
+{
+    return kp::guarded( "kp_ini_merge", [ & ]
+    {
+        kp::require( n >= 1 && paths && out_path, "need at least one input file and an output path" );
+        kp::ini_t ini;
+        for( int k = 0; k < n; ++ k )
+        {
+            kp::require( paths[ k ] != nullptr, "null input file" );
+            kp::require( ini.read_file( paths[ k ] ),
+                         ( std::string( "cannot read the input file " ) + paths[ k ] ).c_str(  ),
+                         KP_ERR_CONFIG );
+        }
+        std::ofstream f( out_path );
+        kp::require( f.good(  ), "cannot write the merged input file", KP_ERR_CONFIG );
+        f << ini.text(  );
+        f.close(  );
+        kp::require( ! f.fail(  ), "cannot write the merged input file", KP_ERR_CONFIG );
+    } );
+}
+
 extern "C" int kp_particle_read( const char * ini_path, kp_particle_cfg_t * out )
 {
     return kp::guarded( "kp_particle_read", [ & ]
