@@ -13,8 +13,8 @@ x to the box boundary along o and mu = k.o the cosine of the scattering angle
     I(pixel) = integral over the pixel's column of
                sigma_s exp(-sigma_e (r + l(x))) f11(mu) / (4 pi r^2) dV,
 
-which in spherical coordinates about the source is a smooth integral over
-directions k and distances r (the 1 / r^2 cancels the volume element).  The
+which is integrated along the pixel's lines of sight (a change of variable
+removes the 1 / r^2 peak near the source).  The
 scattered light of unpolarized incident light is linearly polarized
 perpendicular to the scattering plane (the plane of k and o) with fraction
 p(mu): Rayleigh (Chandrasekhar 1960): f11 = 3 (1 + mu^2) / (16 pi),
@@ -74,55 +74,72 @@ def wall_distance(s, k, lo, hi):
     return t
 
 
+def _box_span(P, o, lo, hi):
+    """Entry and exit parameters (l_in, l_out) of the lines P + l o through the
+    box (l_in >= l_out where a line misses it)."""
+    l_in = np.full(P.shape[:-1], -np.inf)
+    l_out = np.full(P.shape[:-1], np.inf)
+    for a in range(3):
+        if o[a] != 0:
+            t1, t2 = (lo[a] - P[..., a]) / o[a], (hi[a] - P[..., a]) / o[a]
+            l_in = np.maximum(l_in, np.minimum(t1, t2))
+            l_out = np.minimum(l_out, np.maximum(t1, t2))
+        else:
+            inside = (P[..., a] >= lo[a]) & (P[..., a] <= hi[a])
+            l_out = np.where(inside, l_out, -np.inf)
+    return l_in, l_out
+
+
 def single_scatter_image(lo, hi, src, sigma_s, sigma_a, inclination_deg, azimuth_deg,
                          center, half_width, n_pix, kind="rayleigh", g=0.0, p_max=1.0,
-                         n_mu=160, n_phi=320, n_r=48):
+                         n_sub=24, n_theta=48):
     """Expected image [n_pix, n_pix, 4] (I, Q, U, V; row = vertical pixel) per
-    emitted packet of unit weight: first scatterings by quadrature, plus the
-    unscattered emission in the source's pixel."""
+    emitted packet of unit weight: first scatterings integrated pixel by
+    pixel along the lines of sight (n_sub x n_sub lines per pixel, midpoint
+    rule), plus the unscattered emission in the source's pixel.
+
+    Along a line x = P + l o with closest approach b to the source at l0,
+    r^2 = b^2 + (l - l0)^2 and l - l0 = b tan(theta) turns dl / r^2 into
+    dtheta / b; the path to the wall, l_exit - l, is linear in l, so the
+    integrand is smooth in theta (Gauss-Legendre, n_theta nodes)."""
     lo, hi, src, center = (np.asarray(v, float) for v in (lo, hi, src, center))
     sig_e = sigma_s + sigma_a
     o, ev, eh = observer_frame(inclination_deg, azimuth_deg)
     e2 = np.cross(o, ev)
-    mu_n, mu_w = np.polynomial.legendre.leggauss(n_mu)            # cos(theta) of k
-    phi = (np.arange(n_phi) + 0.5) * 2 * np.pi / n_phi
-    st = np.sqrt(1 - mu_n ** 2)
-    k = np.stack([st[:, None] * np.cos(phi)[None, :], st[:, None] * np.sin(phi)[None, :],
-                  np.broadcast_to(mu_n[:, None], (n_mu, n_phi))], -1)       # [mu, phi, 3]
-    w_dir = mu_w[:, None] * (2 * np.pi / n_phi) * np.ones((1, n_phi))    # dOmega
-    R = wall_distance(src, k, lo, hi)                               # [mu, phi]
-    r_n, r_w = np.polynomial.legendre.leggauss(n_r)
-    img = np.zeros((n_pix * n_pix, 4))
-    inv_pix = n_pix / (2 * half_width)
-    for j in range(n_mu):                                           # one cone at a time
-        kk = k[j]                                                   # [phi, 3]
-        Rj = R[j]
-        r = 0.5 * Rj[:, None] * (r_n[None, :] + 1)                  # [phi, r]
-        wr = 0.5 * Rj[:, None] * r_w[None, :]
-        x = src + r[..., None] * kk[:, None, :]                     # [phi, r, 3]
-        l_out = exit_length(x, o, lo, hi)
-        mu_s = kk @ o                                               # [phi]
-        f11, p = phase(kind, mu_s, g, p_max)
-        n = np.cross(kk, o)                                         # E-vector direction
+    pix = 2 * half_width / n_pix
+    th_n, th_w = np.polynomial.legendre.leggauss(n_theta)
+    sub = (np.arange(n_sub) + 0.5) / n_sub
+    dA = (pix / n_sub) ** 2
+    img = np.zeros((n_pix, n_pix, 4))
+    for fy in range(n_pix):
+        # the sub-lines of one row of pixels: [n_pix * n_sub, n_sub] lines
+        hs = (np.arange(n_pix)[:, None] + sub[None, :]).reshape(-1) * pix - half_width
+        vs = (fy + sub) * pix - half_width
+        P = center + hs[:, None, None] * eh + vs[None, :, None] * ev     # [H, V, 3]
+        l_in, l_out = _box_span(P, o, lo, hi)
+        hit = l_out > l_in                          # lines that miss add nothing
+        l_in, l_out = np.where(hit, l_in, 0.0), np.where(hit, l_out, 0.0)
+        l0 = np.einsum("hvk,k->hv", src - P, o)
+        b = np.maximum(np.linalg.norm(P + l0[..., None] * o - src, axis=-1), 1e-12)
+        t1, t2 = np.arctan((l_in - l0) / b), np.arctan((l_out - l0) / b)
+        th = 0.5 * (t2 - t1)[..., None] * (th_n + 1) + t1[..., None]      # [H, V, n]
+        wth = 0.5 * (t2 - t1)[..., None] * th_w
+        r = b[..., None] / np.cos(th)
+        along = l0[..., None] + b[..., None] * np.tan(th)                 # l of each node
+        k = (P[..., None, :] + along[..., None] * o - src) / r[..., None]
+        f11, p = phase(kind, np.sin(th), g, p_max)                         # k . o = sin(th)
+        n = np.cross(k, o)
         nn = np.linalg.norm(n, axis=-1)
         nn = np.where(nn > 0, nn, 1.0)
         c, s = (n @ ev) / nn, (n @ e2) / nn
-        cos2, sin2 = c * c - s * s, 2 * c * s
-        val = sigma_s * np.exp(-sig_e * (r + l_out)) * wr * (w_dir[j][:, None] / (4 * np.pi))
-        I = val * f11[:, None]
-        Q = I * (p * cos2)[:, None]
-        U = I * (p * sin2)[:, None]
-        d = x - center
-        fx = np.floor(d @ eh * inv_pix + 0.5 * n_pix).astype(np.int64)
-        fy = np.floor(d @ ev * inv_pix + 0.5 * n_pix).astype(np.int64)
-        ok = (fx >= 0) & (fy >= 0) & (fx < n_pix) & (fy < n_pix)
-        pix = (fy * n_pix + fx)[ok]
-        for q, v in enumerate((I, Q, U)):
-            img[:, q] += np.bincount(pix, weights=v[ok], minlength=n_pix * n_pix)
+        val = sigma_s * np.exp(-sig_e * (r + l_out[..., None] - along)) * f11 * wth
+        val = np.where(hit[..., None], val / (4 * np.pi * b[..., None]), 0.0) * dA
+        for q, w in enumerate((1.0, p * (c * c - s * s), p * 2 * c * s)):
+            img[fy, :, q] = (val * w).sum(-1).reshape(n_pix, n_sub, n_sub).sum((1, 2))
     # the unscattered emission toward the observer
     d = src - center
-    fx = int(np.floor(d @ eh * inv_pix + 0.5 * n_pix))
-    fy = int(np.floor(d @ ev * inv_pix + 0.5 * n_pix))
+    fx = int(np.floor(d @ eh / pix + 0.5 * n_pix))
+    fy = int(np.floor(d @ ev / pix + 0.5 * n_pix))
     if 0 <= fx < n_pix and 0 <= fy < n_pix:
-        img[fy * n_pix + fx, 0] += np.exp(-sig_e * exit_length(src[None], o, lo, hi)[0]) / (4 * np.pi)
-    return img.reshape(n_pix, n_pix, 4)
+        img[fy, fx, 0] += np.exp(-sig_e * exit_length(src[None], o, lo, hi)[0]) / (4 * np.pi)
+    return img
