@@ -705,7 +705,7 @@ k_forward( const __grid_constant__ fwd_params_t P )
         // scheduled here (all but the decomposed rounds) ----
         if( phase != PH_SEGMENT ) continue;
         #pragma unroll 1
-        for( int it = 0; it < ( ! DD ? KP_WALK_INNER : 1 ); ++ it )
+        for( int it = 0; it < ( DD ? 1 : ( FLUX ? KP_WALK_INNER_FLUX : KP_WALK_INNER ) ); ++ it )
         {
             // the active ray's direction is in p.d / p.inv (a peel-off ray
             // holds them while the walk's are parked)

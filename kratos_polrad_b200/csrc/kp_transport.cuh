@@ -39,10 +39,15 @@ struct scene_dev_t
     uint32_t  pad;
 };
 
-// Walk segments per scheduling round in the kernels whose peel-off rays are
-// marched by k_peel (k_forward<DEFER>, k_adj_walk).
+// Walk segments per scheduling round of k_forward (but its decomposed rounds)
+// and k_adj_walk: 3 (forward walk 58.5 -> 56.9 ms, gradient 252 -> 247 ms,
+// batched launch 154.6 -> 151.5 ms against 2); the walk with the flux tally
+// keeps 2 (119 against 134 ms with 3).
 #ifndef KP_WALK_INNER
-#define KP_WALK_INNER 2
+#define KP_WALK_INNER 3
+#endif
+#ifndef KP_WALK_INNER_FLUX
+#define KP_WALK_INNER_FLUX 2
 #endif
 
 // Everything a transport launch reads, passed by value.
