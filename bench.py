@@ -233,7 +233,7 @@ def measure_batched(steps, warmup, clocks=None):
     single-scene launches of the same packets (same tallies, bit for bit).
     Under torchrun each rank solves a contiguous range of the scenes (no
     collective in the data path); the per-scene tallies are gathered on rank
-    0.  Every rank returns the same dict."""
+    0 (the other ranks report gathered_scenes None)."""
     import contextlib
     import torch
     from kratos_polrad_b200 import scenes, shard
@@ -309,7 +309,9 @@ def measure_batched(steps, warmup, clocks=None):
                        "tallies": "int64 fixed point",
                        "launch": "one persistent launch replayed from a CUDA graph",
                        "split": "contiguous scene ranges per rank, tallies gathered on rank 0"},
-            "gathered_scenes": int(mu_all.shape[0]), "autotune": tune,
+            # rank 0 holds every scene's tallies, the others none
+            "gathered_scenes": None if mu_all is None else int(mu_all.shape[0]),
+            "autotune": tune,
             "sequential_ms": seq_ms, "sequential_value": n_steps / (seq_ms / 1e3),
             "batched_over_sequential": seq_ms / batched_ms,
             "tallies_identical_to_sequential": bool(differs.item() == 0)}
