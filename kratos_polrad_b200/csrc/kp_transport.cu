@@ -45,7 +45,11 @@ namespace cg = cooperative_groups;
 #define KP_EMIT_BATCH 0              // lanes that wait for an emission batch (0: the event batch)
 #endif
 #ifndef KP_PEEL_INNER
-#define KP_PEEL_INNER 8              // k_peel: segments per scheduling round
+#define KP_PEEL_INNER 16             // k_peel: segments per scheduling round
+#endif
+#ifndef KP_PEEL_INNER_ADJ
+#define KP_PEEL_INNER_ADJ 8          // ... in the adjoint's marches (modes 1, 2): 4
+                                     // and 16 are slower there
 #endif
 #ifndef KP_PEEL_MINB
 #define KP_PEEL_MINB 4               // k_peel: resident blocks of 256 the registers allow
@@ -958,7 +962,7 @@ k_peel( const __grid_constant__ fwd_params_t P )
 
         if( phase != PH_SEGMENT ) continue;
         #pragma unroll 1
-        for( int it = 0; it < KP_PEEL_INNER; ++ it )
+        for( int it = 0; it < ( MODE == 1 || MODE == 2 ? KP_PEEL_INNER_ADJ : KP_PEEL_INNER ); ++ it )
         {
             int ax;
             const double t = oray_segment( tm, tc, ax );
