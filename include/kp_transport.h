@@ -453,6 +453,22 @@ int kp_transport_forward_resume( kp_mesh_t * mesh, const kp_transport_cfg_t * cf
  * are refused (KP_ERR_CONFIG).  No counterpart in the reference. */
 int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays );
 
+/* The order in which kp_transport_forward marches the queued peel-off rays
+ * of this mesh.  KP_PEEL_ORDER_QUEUE: as queued.  KP_PEEL_ORDER_CELL: sorted
+ * by starting cell first (a counting sort over the mesh's cells, about 10 ms
+ * per 1e8 rays, and 4 B per ray plus 8 B per cell of device memory), so that
+ * a warp marches rays that cross nearly the same cells: this pays when the
+ * extinction field (4 B per cell) does not stay in L2.  KP_PEEL_ORDER_AUTO
+ * (the default): CELL when the field exceeds KP_PEEL_SORT_MIN_BYTES, else
+ * QUEUE.  Fixed-point tallies are the same bit for bit in either order;
+ * float tallies agree within rounding.  Other values are refused
+ * (KP_ERR_CONFIG).  No counterpart in the reference. */
+#define KP_PEEL_ORDER_AUTO  (-1)
+#define KP_PEEL_ORDER_QUEUE 0
+#define KP_PEEL_ORDER_CELL  1
+#define KP_PEEL_SORT_MIN_BYTES ( 32ll << 20 )
+int kp_mesh_peel_order( kp_mesh_t * mesh, int order );
+
 /* Profiling hook.  With an image, kp_transport_forward runs two kernels:
  * the walk (which queues the peel-off rays) and the peel-off march.  Later
  * kp_transport_forward calls of this host thread record `event` (a

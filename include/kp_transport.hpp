@@ -219,6 +219,7 @@ public:
     // Upper bound on the peel-off queue in rays (64 B each); larger solves
     // run in chunks of limit / 12 packets.
     void peel_queue_limit( long long max_rays ) { api( kp_mesh_peel_queue_limit( m_, max_rays ) ); }
+    void peel_order( int order ) { api( kp_mesh_peel_order( m_, order ) ); }
     // Device error bits of the last kernels (0: none); throws if any is set
     // when `raise` is true, as the reference's debug flag aborts a run.
     unsigned status( stream_t s = nullptr, bool raise = true )

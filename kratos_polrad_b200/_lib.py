@@ -85,6 +85,7 @@ _SIGS = {
     "kp_launch_host": [c_void_p, c_void_p, c_void_p],
     "kp_transport_split_event": [c_void_p],
     "kp_mesh_peel_queue_limit": [c_void_p, c_ll],
+    "kp_mesh_peel_order": [c_void_p, c_int],
     "kp_transport_forward_tape": [c_void_p, c_void_p, c_void_p, c_void_p, P(c_ll)],
     "kp_transport_adjoint_tape": [c_void_p, c_ll, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                   c_void_p, c_void_p],

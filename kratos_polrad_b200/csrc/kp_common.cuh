@@ -139,6 +139,14 @@ struct kp_mesh
     unsigned   * d_status = nullptr;
     void       * d_pq    = nullptr;  long long pq_cap = 0;        // deferred peel-off rays
     long long    pq_limit = 1ll << 27;                             // ... at most this many
+    // the order k_peel marches the queue in (KP_PEEL_ORDER_*) and the
+    // buffers of the sort by starting cell: per-cell counts and offsets,
+    // the scan's scratch, the permutation
+    int          peel_order = KP_PEEL_ORDER_AUTO;
+    unsigned   * d_sort_cnt = nullptr, * d_sort_off = nullptr;
+    int        * d_sort_perm = nullptr;
+    void       * d_sort_tmp = nullptr;
+    size_t       sort_cells = 0, sort_perm = 0, sort_tmp_bytes = 0;
     void       * d_adj   = nullptr;  size_t adj_bytes = 0;      // deferred adjoint
     // the taped forward solve whose rays the queue and d_adj hold (0: none)
     long long    tape_id = 0, tape_serial = 0;

@@ -189,6 +189,11 @@ void kp_mesh::release(  )
     cudaFree( d_status ); d_status = nullptr;
     cudaFree( d_work );   d_work   = nullptr;
     cudaFree( d_pq );     d_pq     = nullptr; pq_cap = 0;
+    cudaFree( d_sort_cnt );  d_sort_cnt  = nullptr;
+    cudaFree( d_sort_off );  d_sort_off  = nullptr;
+    cudaFree( d_sort_perm ); d_sort_perm = nullptr;
+    cudaFree( d_sort_tmp );  d_sort_tmp  = nullptr;
+    sort_cells = sort_perm = sort_tmp_bytes = 0;
     cudaFree( d_adj );    d_adj    = nullptr; adj_bytes = 0; tape_id = 0;
     cudaFree( d_rf_f );   d_rf_f   = nullptr;
     cudaFree( d_rf_d );   d_rf_d   = nullptr;

@@ -129,6 +129,7 @@ struct fwd_params_t
     struct peel_link_t * pq_link;       // [pq_cap] per-packet links (tape, adjoint)
     unsigned long long * pq_count;      // tasks written (may exceed pq_cap: those ran inline)
     unsigned long long * pq_next;       // k_peel's task counter
+    const int * pq_perm;                // k_peel: the tasks in march order (null: queue order)
     long long   pq_cap;
     // deferred adjoint (kp_transport_adjoint): the tasks are the vertices'
     // peel-off rays, linked in vertex order per packet of the launch
@@ -1071,8 +1072,10 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets );
 // for chunks of n_pk packets), with their own counters: P.work is set to
 // them, so launches that use the mesh's workspace do not touch a tape.
 void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk );
+// The walk of one chunk, then the march of its queue (in P.pq_perm's order
+// when set, sorted first with the mesh's buffers).
 template< int TALLY, bool TAPE, bool RESUME = false >
-void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s );
+void launch_deferred_chunk( fwd_params_t & P, cudaStream_t s, const kp_mesh_t * mesh = nullptr );
 // A forward solve with its peel-off rays queued for k_peel, in chunks (no tape).
 void launch_deferred_solve( kp_mesh_t * mesh, const fwd_params_t & P, int tally_mode,
                             cudaStream_t s );

@@ -17,6 +17,10 @@ from ._lib import call, ptr
 from .config import MeshConfig, RefineRegion  # noqa: F401  (re-exported)
 
 
+# kp_mesh_peel_order's orders
+PEEL_ORDER_AUTO, PEEL_ORDER_QUEUE, PEEL_ORDER_CELL = -1, 0, 1
+
+
 class Mesh:
     """Owns a ``kp_mesh_t``; building needs no GPU."""
 
@@ -165,6 +169,12 @@ class Mesh:
         tid = ctypes.c_longlong(0)
         call("kp_mesh_tape_id", self.handle, ctypes.byref(tid))
         return tid.value
+
+    def set_peel_order(self, order: int) -> None:
+        """The order the forward solve marches its queued peel-off rays in:
+        PEEL_ORDER_AUTO (default), PEEL_ORDER_QUEUE or PEEL_ORDER_CELL (sorted
+        by starting cell).  The fixed-point tallies do not depend on it."""
+        call("kp_mesh_peel_order", self.handle, int(order))
 
     def status(self, stream=None) -> int:
         flags = ctypes.c_uint()

@@ -30,6 +30,21 @@ def test_bad_mesh_config_is_refused():
     assert b"indivisible" in _lib.lib.kp_last_error()
 
 
+def test_peel_order_is_checked():
+    """kp_mesh_peel_order takes the three orders and refuses others
+    (KP_ERR_CONFIG); it only sets the mesh's choice."""
+    from meshcases import AMR_BOX
+    from kratos_polrad_b200 import Mesh
+    from kratos_polrad_b200.mesh import PEEL_ORDER_AUTO, PEEL_ORDER_CELL, PEEL_ORDER_QUEUE
+    m = Mesh(AMR_BOX)
+    for order in (PEEL_ORDER_QUEUE, PEEL_ORDER_CELL, PEEL_ORDER_AUTO):
+        assert _lib.lib.kp_mesh_peel_order(m.handle, order) == _lib.KP_OK
+    for bad in (2, -2):
+        assert _lib.lib.kp_mesh_peel_order(m.handle, bad) == _lib.KP_ERR_CONFIG
+        assert b"unknown peel-off order" in _lib.lib.kp_last_error()
+    assert _lib.lib.kp_mesh_peel_order(None, 0) == _lib.KP_ERR_ARG
+
+
 def test_tape_entry_points_refuse_without_a_taped_solve():
     """A mesh that never ran a taped solve has tape id 0, and the adjoint of
     tape 0 (or of any id) is refused before any device work."""
