@@ -911,6 +911,8 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
         kp::ensure_peel_queue( mesh, P.n_packets );
         const long long chunk = std::max< long long >( mesh->pq_cap / kp::PQ_PER_PACKET, 1 );
         kp::adjoint_buffers( mesh, P, std::min( chunk, P.n_packets ) );
+        // both marches read the queue in the forward solve's order
+        int * perm = kp::peel_sorted( mesh ) ? kp::ensure_task_sort( mesh, mesh->pq_cap ) : nullptr;
         const void * kw0 = fx ? ( const void * ) kp::k_adj_walk< KP_TALLY_FIXED, 0 >
                               : ( const void * ) kp::k_adj_walk< KP_TALLY_FLOAT, 0 >;
         const long long grid_w = kp::persistent_grid( kw0, threads );
@@ -918,6 +920,7 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
         for( long long done = 0; done < P.n_packets; done += chunk )
         {
             C = P;
+            C.pq_perm = perm;
             C.pid0 = P.pid0 + done;
             C.n_packets = std::min( chunk, P.n_packets - done );
             const unsigned gw = ( unsigned ) std::min< long long >( grid_w,
@@ -929,6 +932,7 @@ extern "C" int kp_transport_adjoint( kp_mesh_t * mesh, const kp_transport_cfg_t 
             if( fx ) kp::k_adj_walk< KP_TALLY_FIXED, 0 ><<< gw, threads, 0, s >>>( C );
             else     kp::k_adj_walk< KP_TALLY_FLOAT, 0 ><<< gw, threads, 0, s >>>( C );
             KP_CUDA( cudaGetLastError(  ) );
+            if( perm ) kp::task_sort( mesh, C, s );                     // by starting cell
             kp::launch_peel_adjoint( C, cfg->tally_mode, 1, s );       // scores G
             adjoint_second_half( C, cfg->tally_mode, s );
         }

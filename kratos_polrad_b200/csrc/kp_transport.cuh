@@ -1072,6 +1072,12 @@ void ensure_peel_queue( kp_mesh_t * mesh, long long n_packets );
 // for chunks of n_pk packets), with their own counters: P.work is set to
 // them, so launches that use the mesh's workspace do not touch a tape.
 void adjoint_buffers( kp_mesh_t * mesh, fwd_params_t & P, long long n_pk );
+// The march order of the mesh's queue (kp_mesh_peel_order): whether to
+// sort it by starting cell, the sort's buffers (returns the permutation),
+// and the sort of the queue P describes into P.pq_perm.
+bool peel_sorted( const kp_mesh_t * mesh );
+int * ensure_task_sort( kp_mesh_t * mesh, long long pq_cap );
+void task_sort( const kp_mesh_t * mesh, const fwd_params_t & P, cudaStream_t s );
 // The walk of one chunk, then the march of its queue (in P.pq_perm's order
 // when set, sorted first with the mesh's buffers).
 template< int TALLY, bool TAPE, bool RESUME = false >
