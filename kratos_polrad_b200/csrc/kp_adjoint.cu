@@ -964,19 +964,25 @@ extern "C" int kp_transport_forward_tape( kp_mesh_t * mesh, const kp_transport_c
             return;
         }
         kp::adjoint_buffers( mesh, P, P.n_packets );
+        // the march order; the gradient's depositing march reads the same
+        // permutation, which lives as long as the tape (every solve that
+        // overwrites the queue drops the tape)
+        const bool sorted = kp::peel_sorted( mesh );
+        P.pq_perm = sorted ? kp::ensure_task_sort( mesh, mesh->pq_cap ) : nullptr;
         auto s = ( cudaStream_t ) stream;
         KP_CUDA( cudaMemsetAsync( P.work, 0, 4 * sizeof( unsigned long long ), s ) );
         KP_CUDA( cudaMemsetAsync( P.adj_head, 0xff, P.n_packets * sizeof( int ), s ) );
         KP_CUDA( cudaMemsetAsync( P.adj_flag, 0, P.n_packets * sizeof( int ), s ) );
         if( cfg->tally_mode == KP_TALLY_FIXED )
-            kp::launch_deferred_chunk< KP_TALLY_FIXED, true >( P, s );
+            kp::launch_deferred_chunk< KP_TALLY_FIXED, true >( P, s, mesh );
         else
-            kp::launch_deferred_chunk< KP_TALLY_FLOAT, true >( P, s );
+            kp::launch_deferred_chunk< KP_TALLY_FLOAT, true >( P, s, mesh );
         kp::fold_carry( * cfg, * tallies, s );
         mesh->tape_cfg = * cfg;
         mesh->tape_cfg.sources = nullptr;
         for( int k = 0; k < cfg->n_sources; ++ k ) mesh->tape_src[ k ] = cfg->sources[ k ];
         mesh->tape_n = P.n_packets;
+        mesh->tape_sorted = sorted;
         mesh->tape_id = ++ mesh->tape_serial;
         * tape_id = mesh->tape_id;
     } );
@@ -998,6 +1004,7 @@ extern "C" int kp_transport_adjoint_tape( kp_mesh_t * mesh, long long tape_id,
         static thread_local kp::fwd_params_t P;
         adjoint_params( mesh, cfg, adj_image, grad_fx_shift, grad_len, grad_int, counters, P );
         kp::adjoint_buffers( mesh, P, mesh->tape_n );      // the taped solve's layout
+        P.pq_perm = mesh->tape_sorted ? mesh->d_sort_perm : nullptr;   // ... and order
         auto s = ( cudaStream_t ) stream;
         mesh->refresh_ext( s );
         const unsigned gs = 4 * 148;

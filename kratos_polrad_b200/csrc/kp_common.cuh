@@ -151,6 +151,7 @@ struct kp_mesh
     // the taped forward solve whose rays the queue and d_adj hold (0: none)
     long long    tape_id = 0, tape_serial = 0;
     long long    tape_n  = 0;                                      // its packets
+    bool         tape_sorted = false;   // its march read d_sort_perm (the tape's order)
     kp_transport_cfg_t tape_cfg {  };
     kp_source_t  tape_src[ KP_MAX_SOURCES ] {  };
     float      * d_rf_f  = nullptr;  double * d_rf_d  = nullptr;   // spherical tables

@@ -51,6 +51,34 @@ def test_tape_matches_plain_solve_and_full_adjoint(name):
         assert torch.equal(x, y)
 
 
+@pytest.mark.parametrize("name", ["amr_point", "hg_multi"])
+def test_tape_in_cell_order(name):
+    """A taped solve marched sorted by starting cell keeps that order for its
+    gradient, even after the mesh's order changed: tallies equal the plain
+    solve's and gradients the full adjoint's (queue order)."""
+    from kratos_polrad_b200.mesh import PEEL_ORDER_AUTO, PEEL_ORDER_CELL, PEEL_ORDER_QUEUE
+    mesh, sig, t = case(name)
+    mesh.set_sigma(sig)
+    plain = forward(mesh, t)
+    try:
+        mesh.set_peel_order(PEEL_ORDER_CELL)
+        taped = forward(mesh, t, Tallies(t), tape=True)
+        mesh.set_peel_order(PEEL_ORDER_QUEUE)
+        t0 = dataclasses.replace(t, n_record=0)
+        a1 = _adj(t, 1)
+        tape1 = adjoint(mesh, t0, a1, 24, tape_id=taped.tape_id)
+        torch.cuda.synchronize()
+        assert mesh.status() == 0
+        full1 = adjoint(mesh, t0, a1, 24)
+        torch.cuda.synchronize()
+    finally:
+        mesh.set_peel_order(PEEL_ORDER_AUTO)
+    for k in ("mu", "image", "image_batch", "counters", "records"):
+        assert torch.equal(getattr(taped, k), getattr(plain, k)), k
+    for x, y in zip(tape1, full1):
+        assert torch.equal(x, y)
+
+
 def test_tape_is_dropped_by_new_coefficients_and_later_solves():
     mesh, sig, t = case("amr_point")
     t = dataclasses.replace(t, n_record=0)
