@@ -455,8 +455,9 @@ int kp_mesh_peel_queue_limit( kp_mesh_t * mesh, long long max_rays );
 
 /* The order in which kp_transport_forward marches the queued peel-off rays
  * of this mesh.  KP_PEEL_ORDER_QUEUE: as queued.  KP_PEEL_ORDER_CELL: sorted
- * by starting cell first (a counting sort over the mesh's cells, about 10 ms
- * per 1e8 rays, and 4 B per ray plus 8 B per cell of device memory), so that
+ * by starting cell first (a counting sort over the mesh's cells: about 1.3 ms
+ * per 1e8 rays, up to 10 ms when one cell starts most of them, as a point
+ * source's does; 4 B per ray plus 8 B per cell of device memory), so that
  * a warp marches rays that cross nearly the same cells: this pays when the
  * extinction field (4 B per cell) does not stay in L2.  KP_PEEL_ORDER_AUTO
  * (the default): CELL when the field exceeds KP_PEEL_SORT_MIN_BYTES, else
