@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--packets", type=float, default=1e7)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--peel-order", default="auto", choices=["auto", "queue", "cell"],
+                   help="--workload large: the order the peel-off queue is marched in "
+                        "(kp_mesh_peel_order; auto sorts by starting cell on this scene)")
     p.add_argument("--workload", default="clump",
                    choices=["clump", "batched", "diff", "large", "decomp", "trace", "sph",
                             "refine", "bio", "resume"])
@@ -875,6 +878,9 @@ def run_large(args):
     n_pk = int(args.packets) if args.packets != 1e7 else 1_000_000_000
     mesh, sig, cfg = scenes.large_amr(n_packets=n_pk)
     mesh.set_sigma(sig)
+    from kratos_polrad_b200.mesh import PEEL_ORDER_AUTO, PEEL_ORDER_CELL, PEEL_ORDER_QUEUE
+    mesh.set_peel_order({"auto": PEEL_ORDER_AUTO, "queue": PEEL_ORDER_QUEUE,
+                         "cell": PEEL_ORDER_CELL}[args.peel_order])
     warm = dataclasses.replace(cfg, n_packets=min(n_pk, 2_000_000))
     forward(mesh, warm)
     torch.cuda.synchronize()
@@ -907,7 +913,8 @@ def run_large(args):
             "value": (c["steps"] + c["peel_steps"]) / (t_fwd / 1e3), "higher_is_better": True,
             "n_gpus": 1, "config": {"workload": "large_amr_3level", "packets": n_pk,
                                     "blocks": mesh.n_blocks, "cells": mesh.n_cells,
-                                    "sigma_MB": sig.nbytes / 1e6, "image": cfg.image_n},
+                                    "sigma_MB": sig.nbytes / 1e6, "image": cfg.image_n,
+                                    "peel_order": args.peel_order},
             "forward_ms": t_fwd, "counts": c, "pol_tangential": p_tan, "pol_rel_std_err": rel,
             "pol_tangential_about_sources": p_loc, "pol_tangential_about_sources_rel_std_err": rel_loc,
             # the std-error falls like packets^-1/2: packets (and forward time at
