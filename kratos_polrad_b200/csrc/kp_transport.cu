@@ -1610,6 +1610,7 @@ void launch_resume_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStrea
     mesh->tape_id = 0;                      // the queue is overwritten
     ensure_peel_queue( mesh, items );
     const long long chunk = std::max< long long >( mesh->pq_cap / PQ_PER_PACKET, 1 );
+    int * perm = peel_sorted( mesh ) ? ensure_task_sort( mesh, mesh->pq_cap ) : nullptr;
     static thread_local fwd_params_t C;
     for( long long lo = 0; lo < items; lo += chunk )
     {
@@ -1617,12 +1618,13 @@ void launch_resume_deferred( kp_mesh_t * mesh, const fwd_params_t & P, cudaStrea
         C = P;
         C.pq = static_cast< peel_task_t * >( mesh->d_pq );
         C.pq_cap = mesh->pq_cap;
+        C.pq_perm = perm;
         C.rs_in = P.rs_in + std::min( lo, n_in );
         C.rs_n_in = std::max< long long >( std::min( hi, n_in ) - lo, 0 );
         const long long first = std::max( lo, n_in );   // first new packet's item
         C.pid0 = P.pid0 + ( first - n_in );
         C.n_packets = std::max< long long >( hi - first, 0 );
-        launch_deferred_chunk< TALLY, false, true >( C, s );
+        launch_deferred_chunk< TALLY, false, true >( C, s, mesh );
     }
 }
 }   // namespace kp

@@ -75,6 +75,23 @@ def test_budgeted_calls_equal_one_solve(name, budget):
     _assert_same(tal, full, t)
 
 
+@pytest.mark.parametrize("name,budget", [("amr_point", 9), ("hg_multi", 13)])
+def test_budgeted_calls_in_cell_order(name, budget):
+    """Every call's queue marched sorted by starting cell: same as one
+    solve in queue order."""
+    from kratos_polrad_b200.mesh import PEEL_ORDER_AUTO, PEEL_ORDER_CELL
+    mesh, t = _setup(name)
+    full = forward(mesh, t, Tallies(t, n_cells=mesh.n_cells))
+    torch.cuda.synchronize()
+    mesh.set_peel_order(PEEL_ORDER_CELL)
+    try:
+        tal, calls, _ = _resumed_solve(mesh, t, budget)
+    finally:
+        mesh.set_peel_order(PEEL_ORDER_AUTO)
+    assert calls > 3
+    _assert_same(tal, full, t)
+
+
 def test_two_half_budget_calls():
     """The first call suspends every packet still walking after 150 of its
     300 segments; the second finishes them: same as one solve."""
